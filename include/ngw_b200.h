@@ -1,0 +1,148 @@
+/*
+ * ngw_b200 -- C ABI of the B200-native ISDF-Lanczos GW (Sigma_c) path.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (NGW_OK = 0; the Fortran shim calls die() on non-zero, as the reference's
+ * shared/die.F90:10 does) and leaves the human-readable reason in
+ * ngw_last_error().  Arrays are column-major with Fortran leading dimensions
+ * and band / pair indices are 1-based, exactly as the reference passes them.
+ * Energies are in Rydberg.  Host pointers are never kept after a call
+ * returns; the session owns its device-resident copies.  A session is used by
+ * one host thread at a time; calls are synchronous to the caller.
+ *
+ * Reference interfaces replaced (file:line in the NanoGW tree):
+ *   ngw_set_isdf / ngw_set_pairs  -- the isdf_in%Psi_intp / Mmtrx / cvpair /
+ *        sqrtR arguments of shared/apply_matvec.f90:25 and
+ *        shared/apply_matvec_BLOCK.F90:25 (type ISDF, shared/typedefs.F90:24-72)
+ *   ngw_matvec_isdf               -- matvec_isdf            shared/apply_matvec.f90:25
+ *                                    matvec_isdf_BLOCK      shared/apply_matvec_BLOCK.F90:25
+ *                                    matvec_isdf_lowcomsym  shared/apply_matvec_lowcomsym.F90:31
+ *   ngw_polynomial_matvec_isdf    -- polynomial_matvec_isdf shared/apply_matvec.f90:142
+ *                                    (_BLOCK :210, _lowcomsym :419)
+ *   ngw_lanczos_spectra_isdf      -- lanczos_spectra_isdf   shared/lanczos_spectra.f90:7
+ *                                    (_BLOCK shared/lanczos_spectra_BLOCK.F90:7,
+ *                                     _lowcomsym shared/lanczos_spectra_lowcomsym.F90:7)
+ *   ngw_k_integrate_isdf          -- Zk_integrate_isdf      shared/k_integrate_isdf.F90z:12
+ *   ngw_sigma_lanczos             -- Zcalculate_sigma_lanczos(_lowcomsym)
+ *                                    SIGMA/calculate_sigma_lanczos_lowcomsym.F90z:9
+ *   ngw_qp_newton                 -- QP part of printsigma  SIGMA/printsigma.F90:97-125
+ *                                    (newtonr SIGMA/newtonr.f90:18)
+ *   ngw_cvt / ngw_dedup_points    -- cvt shared/cvt.F90:8 and SIGMA/sigma.F90:377-461
+ *   ngw_shell_sort                -- quicksort shared/quicksort.f90:19
+ *   ngw_build_coulomb_kernel      -- Mmtrx build, shared/isdf_parallel_sym_UltraLowMem.F90:687-889
+ *                                    (dpoisson shared/fft_module.F90z:122,
+ *                                     dcreate_coul_0D shared/fft_module.F90z:628)
+ */
+#ifndef NGW_B200_H
+#define NGW_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define NGW_OK 0
+#define NGW_ERR_ARG 1        /* bad shape / argument */
+#define NGW_ERR_OOM 2        /* device allocation failed */
+#define NGW_ERR_CUDA 3       /* CUDA runtime / library error */
+#define NGW_ERR_TIMEOUT 4    /* a bounded device wait gave up */
+#define NGW_ERR_NONFINITE 5  /* NaN / Inf in an input */
+#define NGW_ERR_BUDGET 6     /* over the memory budget */
+#define NGW_ERR_STATE 7      /* call order (e.g. no operator set) */
+#define NGW_ERR_NOCONV 8     /* QP Newton did not converge */
+
+/* precision modes of the matvec */
+#define NGW_PREC_FP64 0      /* FP64 GEMMs + Horner: the reference's arithmetic */
+#define NGW_PREC_MIXED 1     /* split-BF16 tcgen05 GEMMs (FP32 accumulate),
+                                Chebyshev-Clenshaw form of the same polynomial,
+                                FP64 Lanczos recurrence / continued fraction */
+
+typedef struct ngw_session ngw_session;
+
+int ngw_version(void);
+const char *ngw_last_error(void);
+
+int ngw_session_create(int device, ngw_session **out);
+void ngw_session_destroy(ngw_session *s);
+/* cudaStream_t of the session, as an opaque pointer (for event timing) */
+void *ngw_session_stream(ngw_session *s);
+int ngw_set_precision(ngw_session *s, int mode);
+/* bytes of device memory the session holds now */
+long long ngw_session_bytes(ngw_session *s);
+
+/* ISDF operator: psi_intp (n_isdf x nmem), mmtrx (n_isdf x n_isdf) Coulomb
+ * block, mxc optional (n_isdf x n_isdf) f_xc block or NULL. */
+int ngw_set_isdf(ngw_session *s, int n_isdf, int nmem, const double *psi_intp,
+                 const double *mmtrx, const double *mxc);
+/* valence-conduction pairs: cvpair (2 x ncv) 1-based (v, c); sqrtR (ncv) */
+int ngw_set_pairs(ngw_session *s, int ncv, const int *cvpair, const double *sqrtR);
+
+/* Hvec = H vec for blksz columns (ld >= ncv).  tamm_d != 0: A = R + 2 C^T M C */
+int ngw_matvec_isdf(ngw_session *s, const double *vec, double *hvec, int ld,
+                    int blksz, int tamm_d);
+/* Hvec = p(H) vec, polynomial (npoly+1) stored high -> low */
+int ngw_polynomial_matvec_isdf(ngw_session *s, const double *polynomial, int npoly,
+                               const double *vec, double *hvec, int ld, int blksz);
+/* spectra(iz, j) = <v_j|(zz(iz,j) - p(H))^-1|v_j>, v_j = v0(:,j)/v0_norm(j).
+ * zz / spectra: complex128 interleaved (nz x blksz).  alpha / beta (niter x
+ * blksz) may be NULL.  tamm_d != 0 uses H = A and ignores the polynomial. */
+int ngw_lanczos_spectra_isdf(ngw_session *s, const double *v0, const double *v0_norm,
+                             int ld, const double *zz, int nz, int niter,
+                             const double *polynomial, int npoly, int blksz, int tamm_d,
+                             double *spectra, double *alpha, double *beta);
+/* kmat(i, j) = (psi_r1 psi_r2)^T M (psi_c1 psi_c2) for row pairs rows(2, nrow)
+ * and column pairs cols(2, ncol) (1-based bands);
+ * M = [kflag < 2] M_C + [kflag > 0] M_xc.  kmat: nrow x ncol column-major. */
+int ngw_k_integrate_isdf(ngw_session *s, int kflag, const int *rows, int nrow,
+                         const int *cols, int ncol, double *kmat);
+
+typedef struct {
+  int nen;                 /* energy points per QP state */
+  double deltae;           /* energy range (Ry) of the grid centred on e1(m) */
+  double ecuts;            /* broadening eta (Ry) */
+  int niter;               /* Lanczos steps */
+  int npoly;               /* polynomial degree (ignored with tamm_d) */
+  const double *polynomial;/* npoly+1 coefficients high -> low */
+  int tamm_d;              /* Tamm-Dancoff */
+  int nval;                /* occupied bands (eta_n = +1 for n <= nval) */
+  int nqp;                 /* number of QP states */
+  const int *qp_bands;     /* nqp 1-based band indices m */
+  int nbands_sum;          /* bands n summed over: 1..nbands_sum (0 = nmem) */
+  int block_chains;        /* chains per device block (0 = all that fit) */
+  double cheb_lo, cheb_hi; /* mixed mode: Chebyshev interval (0,0 = auto) */
+} ngw_sigma_params;
+
+/* Sigma_c(omega) for every QP state: sigma_c complex128 interleaved,
+ * (nen x nqp) column-major, in Ry.  e1: KS energies (nmem), Ry.
+ * alpha/beta (niter x nchains, chain = iq*nbands_sum + n) optional. */
+int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e1,
+                      double *sigma_c, double *alpha, double *beta);
+
+/* QP Newton solve on the device (eV in, eV out), one state per column:
+ * sigma_c (nen x nqp complex, eV), e1/e0/sigx/vxc (nqp) eV.
+ * Grid: x_i = e1 - deltae/2 + deltae/(nen-1)*(i-1).  Tolerance xacc (eV). */
+int ngw_qp_newton(ngw_session *s, int nqp, int nen, const double *sigma_c_ev,
+                  const double *e1_ev, const double *e0_ev, double deltae_ev,
+                  const double *sigx_ev, const double *vxc_ev, double xacc_ev,
+                  double *eqp_ev, double *zfac, int *ierr);
+
+/* ---- setup path ---- */
+/* Shell sort (ascending) returning a 1-based permutation. Host code. */
+int ngw_shell_sort(int n, const double *arr, int *idx);
+/* CVT interpolation points; grid (3 x ngrid), pts (3 x n_intp) in/out,
+ * intp (n_intp) 1-based grid indices.  Bit-exact with the reference loops. */
+int ngw_cvt(int ngrid, const double *grid, const double *rho, int n_intp, double *pts,
+            int max_iter, int *intp, int *iters);
+/* de-duplicate CVT points by density (C1): returns the kept count in *nout */
+int ngw_dedup_points(int n, const int *intp, const double *rho, int *out, int *nout);
+/* Coulomb ISDF kernel: M = ntrans/hcub * zeta^T (v_c zeta) on the device.
+ * zeta (ngrid x n_isdf) column-major, grid_idx (3 x ngrid) integer coords,
+ * nfft box edge, h spacing, trunc = 2*rmax.  mmtrx out (n_isdf x n_isdf). */
+int ngw_build_coulomb_kernel(ngw_session *s, int ngrid, int n_isdf, const double *zeta,
+                             const int *grid_idx, int nfft, double h, double trunc,
+                             double *mmtrx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,761 @@
+// C ABI of ngw_b200: sessions, the ISDF operator, matvec / polynomial matvec,
+// Lanczos spectra, Sigma_c driver, k_integrate and the QP Newton solve.
+// FP64 GEMMs of the plain path go through cuBLAS (library GEMMs); every other
+// step is a kernel of this library.
+#include <cstdarg>
+#include <cstring>
+#include <cmath>
+#include <vector>
+
+#include "ngw_internal.h"
+
+namespace ngw {
+
+int mixed_build_operator(ngw_session *s);
+int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1);
+int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const double *g, int n,
+                     double c0, double c1, int tda, double *out64);
+void mixed_free(ngw_session *s);
+void monomial_to_chebyshev(const double *poly_hl, int n, double lo, double hi, double *g);
+
+static thread_local char g_err[1024] = {0};
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int dalloc(ngw_session *s, void **p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    *p = nullptr;
+    return NGW_ERR_OOM;
+  }
+  s->bytes += bytes;
+  return NGW_OK;
+}
+
+void dfree(ngw_session *s, void *p, size_t bytes) {
+  if (!p) return;
+  cudaFree(p);
+  s->bytes -= bytes;
+}
+
+// Named scratch slots, grown on demand and kept for the session's lifetime.
+int scratch(ngw_session *s, int slot, size_t bytes, void **p) {
+  if ((int)s->scratch.size() <= slot) s->scratch.resize(slot + 1);
+  DBuf &b = s->scratch[slot];
+  if (b.bytes < bytes) {
+    if (b.p) {
+      NGW_CUDA(cudaStreamSynchronize(s->stream));
+      dfree(s, b.p, b.bytes);
+      b.p = nullptr;
+      b.bytes = 0;
+    }
+    NGW_TRY(dalloc(s, &b.p, bytes));
+    b.bytes = bytes;
+  }
+  *p = b.p;
+  return NGW_OK;
+}
+
+int check_status(ngw_session *s) {
+  int h = 0;
+  NGW_CUDA(cudaMemcpyAsync(&h, s->d_status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  if (h != DEV_OK) {
+    int z = 0;
+    cudaMemcpy(s->d_status, &z, sizeof(int), cudaMemcpyHostToDevice);
+    set_error("device status %d (%s)", h, h == DEV_TIMEOUT ? "bounded wait timed out" : "index check");
+    return h == DEV_TIMEOUT ? NGW_ERR_TIMEOUT : NGW_ERR_CUDA;
+  }
+  return NGW_OK;
+}
+
+static bool all_finite(const double *x, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(x[i])) return false;
+  return true;
+}
+
+// slots of session scratch
+enum {
+  SL_IN = 0, SL_OUT, SL_HS, SL_T1, SL_T2, SL_Z, SL_VEC, SL_WVEC, SL_TMP, SL_A, SL_B, SL_ZZ,
+  SL_SPEC, SL_CMN, SL_CM, SL_P, SL_P2, SL_PN2, SL_PN, SL_CHB, SL_CHQ, SL_E1, SL_ZZ0, SL_SIG,
+  SL_KR, SL_KC, SL_KM, SL_B1, SL_B2, SL_QPW, SL_QPIO, SL_SPECS, SL_NUM
+};
+
+// ---------------------------------------------------------------------------
+// FP64 matvec on device buffers.  hs = (R^1/2 or 1) * x must already be in
+// place; y = H x; optional Horner step against vec; optional next hs.
+static int matvec_f64_dev(ngw_session *s, int nb, double *hs, double *y, const double *vec,
+                          int tamm_d, int horner_k, double pk, double pk1, double *hs_next) {
+  double *t1, *t2, *z;
+  NGW_TRY(scratch(s, SL_T1, (size_t)s->n_isdf * nb * 8, (void **)&t1));
+  NGW_TRY(scratch(s, SL_T2, (size_t)s->n_isdf * nb * 8, (void **)&t2));
+  NGW_TRY(scratch(s, SL_Z, (size_t)s->ncv * nb * 8, (void **)&z));
+  const double one = 1.0, zero = 0.0;
+  // tmp_vec = Cmtrx * Hvec          (apply_matvec_lowcomsym.F90:228-229)
+  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, s->n_isdf, nb, s->ncv, &one, s->d_C,
+                         s->n_isdf, hs, s->ncv, &zero, t1, s->n_isdf));
+  // MC_vec = Mmtrx * tmp_vec         (:283-284)
+  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, s->n_isdf, nb, s->n_isdf, &one,
+                         s->d_M, s->n_isdf, t1, s->n_isdf, &zero, t2, s->n_isdf));
+  // CMC_vec = Cmtrx^T * MC_vec       (:365-366)
+  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, s->ncv, nb, s->n_isdf, &one, s->d_C,
+                         s->n_isdf, t2, s->n_isdf, &zero, z, s->ncv));
+  launch_matvec_combine(s->d_sqrtR, hs, z, y, vec, s->ncv, nb, tamm_d, horner_k, pk, pk1, hs_next,
+                        s->stream);
+  NGW_CUDA(cudaGetLastError());
+  return NGW_OK;
+}
+
+// out = p(H) vec by Horner (FP64), vec/out: (ncv, nb); hs scratch holds
+// (R^1/2) vec on entry and is clobbered.
+static int poly_f64_dev(ngw_session *s, int nb, const double *poly, int npoly, const double *vec,
+                        double *hs, double *out) {
+  for (int k = 1; k <= npoly; ++k) {
+    double *hn = (k < npoly) ? hs : nullptr;
+    NGW_TRY(matvec_f64_dev(s, nb, hs, out, vec, 0, k, poly[k - 1], poly[k], hn));
+  }
+  return NGW_OK;
+}
+
+struct PolyPlan {
+  int tamm_d = 0;
+  int npoly = 0;
+  std::vector<double> poly;   // high -> low
+  std::vector<double> cheb;   // Chebyshev coefficients (mixed)
+  double c0 = 0, c1 = 1;
+};
+
+// t = p(H) vec  (or A vec with TDA) on device, in the session's precision.
+static int apply_poly(ngw_session *s, const PolyPlan &pp, int nb, const double *vec, double *hs,
+                      double *t) {
+  if (s->precision == NGW_PREC_MIXED) {
+    if (pp.tamm_d) {
+      // A = R + 2 C^T M C as the degree-1 Chebyshev series x on [c0-c1, c0+c1]
+      const double g[2] = {pp.c0, pp.c1};
+      return mixed_poly_apply(s, nb, vec, s->ncv, g, 1, pp.c0, pp.c1, 1, t);
+    }
+    return mixed_poly_apply(s, nb, vec, s->ncv, pp.cheb.data(), pp.npoly, pp.c0, pp.c1, 0, t);
+  }
+  if (pp.tamm_d) return matvec_f64_dev(s, nb, hs, t, vec, 1, 0, 0.0, 0.0, nullptr);
+  return poly_f64_dev(s, nb, pp.poly.data(), pp.npoly, vec, hs, t);
+}
+
+// Lanczos recurrence for nb chains whose normalised start vectors are set up
+// by launch_lanczos_init.  Leaves a, b (niter x nb).
+static int lanczos_dev(ngw_session *s, const PolyPlan &pp, int nb, int niter, double *V,
+                       double *W, double *hs, double *tmp, double *a, double *b) {
+  // wvec = p(H) vec
+  NGW_TRY(apply_poly(s, pp, nb, V, hs, W));
+  launch_lanczos_first(W, V, s->ncv, nb, a, b, niter, s->stream);
+  if (niter >= 2)
+    launch_lanczos_prescale(W, V, s->ncv, nb, 1, b, niter, s->d_sqrtR, hs, pp.tamm_d, s->stream);
+  double *vec = W, *wvec = V;   // roles after the swap
+  for (int k = 1; k < niter; ++k) {
+    NGW_TRY(apply_poly(s, pp, nb, vec, hs, tmp));
+    launch_lanczos_step(wvec, vec, tmp, s->ncv, nb, k, a, b, niter, s->d_sqrtR, hs, pp.tamm_d,
+                        (k + 1 < niter) ? 1 : 0, s->stream);
+    if (k + 1 < niter) {
+      double *t = vec;
+      vec = wvec;
+      wvec = t;
+    }
+  }
+  NGW_CUDA(cudaGetLastError());
+  return NGW_OK;
+}
+
+static int need_op(ngw_session *s) {
+  if (!s) {
+    set_error("null session");
+    return NGW_ERR_ARG;
+  }
+  if (!s->have_isdf || !s->have_pairs) {
+    set_error("ISDF operator or pair list not set");
+    return NGW_ERR_STATE;
+  }
+  if (!s->have_C) {
+    launch_pair_gather_f64(s->d_psi, s->n_isdf, s->d_cvpair, s->ncv, s->d_C, s->stream);
+    NGW_CUDA(cudaGetLastError());
+    s->have_C = true;
+  }
+  if (s->precision == NGW_PREC_MIXED && !s->mixed) NGW_TRY(mixed_build_operator(s));
+  return NGW_OK;
+}
+
+// Largest eigenvalue of C (or of A with TDA) from a 40-step FP64 Lanczos
+// run on one deterministic start vector: the Ritz value converges from
+// below, and the Chebyshev interval of the mixed path adds a margin.
+static double tridiag_max_eig(const std::vector<double> &a, const std::vector<double> &b, int k) {
+  // Sturm-count bisection on T = tridiag(b[1..k-1], a[0..k-1], b[1..k-1])
+  double lo = a[0], hi = a[0];
+  for (int i = 0; i < k; ++i) {
+    const double r = (i > 0 ? std::fabs(b[i]) : 0.0) + (i + 1 < k ? std::fabs(b[i + 1]) : 0.0);
+    lo = std::min(lo, a[i] - r);
+    hi = std::max(hi, a[i] + r);
+  }
+  auto count_below = [&](double x) {
+    int c = 0;
+    double d = 1.0;
+    for (int i = 0; i < k; ++i) {
+      const double bb = (i > 0) ? b[i] * b[i] : 0.0;
+      d = a[i] - x - (i > 0 ? bb / d : 0.0);
+      if (d == 0.0) d = -1e-300;
+      if (d < 0) ++c;
+    }
+    return c;
+  };
+  for (int it = 0; it < 200 && hi - lo > 1e-14 * std::max(1.0, std::fabs(hi)); ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (count_below(mid) >= k) hi = mid;
+    else lo = mid;
+  }
+  return hi;
+}
+
+static int estimate_lambda_max(ngw_session *s, int tamm_d, double *out) {
+  const int ncv = s->ncv;
+  const int k = std::min(40, ncv);
+  std::vector<double> v(ncv);
+  uint64_t st = 0x9E3779B97F4A7C15ull;
+  double nrm = 0.0;
+  for (int i = 0; i < ncv; ++i) {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    v[i] = (double)((st >> 11) & ((1ull << 53) - 1)) / 9007199254740992.0 - 0.5;
+    nrm += v[i] * v[i];
+  }
+  nrm = std::sqrt(nrm);
+  double *d0, *V, *W, *hs, *tmp, *a, *b, *dn;
+  NGW_TRY(scratch(s, SL_IN, (size_t)ncv * 8, (void **)&d0));
+  NGW_TRY(scratch(s, SL_VEC, (size_t)ncv * 8, (void **)&V));
+  NGW_TRY(scratch(s, SL_WVEC, (size_t)ncv * 8, (void **)&W));
+  NGW_TRY(scratch(s, SL_HS, (size_t)ncv * 8, (void **)&hs));
+  NGW_TRY(scratch(s, SL_TMP, (size_t)ncv * 8, (void **)&tmp));
+  NGW_TRY(scratch(s, SL_A, (size_t)k * 8, (void **)&a));
+  NGW_TRY(scratch(s, SL_B, (size_t)k * 8, (void **)&b));
+  NGW_TRY(scratch(s, SL_PN, 8, (void **)&dn));
+  NGW_CUDA(cudaMemcpyAsync(d0, v.data(), (size_t)ncv * 8, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(dn, &nrm, 8, cudaMemcpyHostToDevice, s->stream));
+  PolyPlan pp;
+  pp.tamm_d = tamm_d;
+  pp.npoly = 1;
+  pp.poly = {1.0, 0.0};
+  const int prec = s->precision;
+  s->precision = NGW_PREC_FP64;
+  launch_lanczos_init(d0, ncv, dn, V, hs, s->d_sqrtR, ncv, 1, tamm_d, b, k, s->stream);
+  int rc = lanczos_dev(s, pp, 1, k, V, W, hs, tmp, a, b);
+  s->precision = prec;
+  NGW_TRY(rc);
+  std::vector<double> ha(k), hb(k);
+  NGW_CUDA(cudaMemcpyAsync(ha.data(), a, (size_t)k * 8, cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(hb.data(), b, (size_t)k * 8, cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  // stop at a (numerically) invariant subspace
+  int kk = k;
+  for (int i = 1; i < k; ++i)
+    if (!(hb[i] > 1e-12 * std::fabs(ha[0]))) {
+      kk = i;
+      break;
+    }
+  *out = tridiag_max_eig(ha, hb, kk);
+  return NGW_OK;
+}
+
+// cached spectral interval of the session's operator for the Chebyshev form
+static int spectral_interval(ngw_session *s, int tamm_d, double *lo, double *hi) {
+  double &cache = tamm_d ? s->lmax_tda : s->lmax;
+  if (!(cache > 0.0)) NGW_TRY(estimate_lambda_max(s, tamm_d, &cache));
+  *lo = 0.0;
+  *hi = cache * 1.02;
+  return NGW_OK;
+}
+
+static int make_plan(ngw_session *s, PolyPlan &pp, const double *poly, int npoly, int tamm_d,
+                     double lo, double hi) {
+  pp.tamm_d = tamm_d;
+  if (!tamm_d) {
+    if (!poly || npoly < 1) {
+      set_error("polynomial of degree >= 1 required");
+      return NGW_ERR_ARG;
+    }
+    pp.npoly = npoly;
+    pp.poly.assign(poly, poly + npoly + 1);
+    if (!all_finite(poly, npoly + 1)) {
+      set_error("non-finite polynomial coefficient");
+      return NGW_ERR_NONFINITE;
+    }
+  } else {
+    pp.npoly = 1;
+  }
+  if (s->precision == NGW_PREC_MIXED) {
+    if (!(hi > lo)) {
+      set_error("mixed precision needs a spectral interval hi > lo (got %g, %g)", lo, hi);
+      return NGW_ERR_ARG;
+    }
+    pp.c0 = 0.5 * (hi + lo);
+    pp.c1 = 0.5 * (hi - lo);
+    if (!tamm_d) {
+      pp.cheb.resize(npoly + 1);
+      monomial_to_chebyshev(poly, npoly, lo, hi, pp.cheb.data());
+    }
+  }
+  return NGW_OK;
+}
+
+}  // namespace ngw
+
+using namespace ngw;
+
+extern "C" {
+
+int ngw_version(void) { return 100; }
+
+const char *ngw_last_error(void) { return g_err; }
+
+int ngw_session_create(int device, ngw_session **out) {
+  if (!out) {
+    set_error("null out pointer");
+    return NGW_ERR_ARG;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  NGW_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) {
+    set_error("device %d out of range (%d devices)", device, ndev);
+    return NGW_ERR_ARG;
+  }
+  NGW_CUDA(cudaSetDevice(device));
+  ngw_session *s = new ngw_session();
+  s->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    set_error("cudaStreamCreate: %s", cudaGetErrorString(e));
+    delete s;
+    return NGW_ERR_CUDA;
+  }
+  if (cublasCreate(&s->cublas) != CUBLAS_STATUS_SUCCESS) {
+    set_error("cublasCreate failed");
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return NGW_ERR_CUDA;
+  }
+  cublasSetStream(s->cublas, s->stream);
+  cublasSetMathMode(s->cublas, CUBLAS_DEFAULT_MATH);
+  if (dalloc(s, (void **)&s->d_status, sizeof(int)) != NGW_OK) {
+    ngw_session_destroy(s);
+    return NGW_ERR_OOM;
+  }
+  cudaMemset(s->d_status, 0, sizeof(int));
+  *out = s;
+  return NGW_OK;
+}
+
+void ngw_session_destroy(ngw_session *s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  mixed_free(s);
+  for (auto &b : s->scratch)
+    if (b.p) cudaFree(b.p);
+  void *ptrs[] = {s->d_psi, s->d_M, s->d_Mxc, s->d_cvpair, s->d_sqrtR, s->d_C, s->d_status};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (s->cublas) cublasDestroy(s->cublas);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+void *ngw_session_stream(ngw_session *s) { return s ? (void *)s->stream : nullptr; }
+
+long long ngw_session_bytes(ngw_session *s) { return s ? (long long)s->bytes : 0; }
+
+int ngw_set_precision(ngw_session *s, int mode) {
+  if (!s || (mode != NGW_PREC_FP64 && mode != NGW_PREC_MIXED)) {
+    set_error("bad precision mode %d", mode);
+    return NGW_ERR_ARG;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  s->precision = mode;
+  if (mode == NGW_PREC_MIXED && s->have_isdf && s->have_pairs) {
+    NGW_TRY(need_op(s));
+  }
+  return NGW_OK;
+}
+
+int ngw_set_isdf(ngw_session *s, int n_isdf, int nmem, const double *psi_intp, const double *mmtrx,
+                 const double *mxc) {
+  if (!s || n_isdf <= 0 || nmem <= 0 || !psi_intp || !mmtrx) {
+    set_error("ngw_set_isdf: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  if (!all_finite(psi_intp, (size_t)n_isdf * nmem) || !all_finite(mmtrx, (size_t)n_isdf * n_isdf) ||
+      (mxc && !all_finite(mxc, (size_t)n_isdf * n_isdf))) {
+    set_error("ngw_set_isdf: non-finite input");
+    return NGW_ERR_NONFINITE;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  mixed_free(s);
+  if (s->d_psi) dfree(s, s->d_psi, (size_t)s->n_isdf * s->nmem * 8);
+  if (s->d_M) dfree(s, s->d_M, (size_t)s->n_isdf * s->n_isdf * 8);
+  if (s->d_Mxc) dfree(s, s->d_Mxc, (size_t)s->n_isdf * s->n_isdf * 8);
+  if (s->d_C) dfree(s, s->d_C, (size_t)s->n_isdf * s->ncv * 8);
+  s->d_psi = s->d_M = s->d_Mxc = s->d_C = nullptr;
+  s->have_C = false;
+  s->lmax = s->lmax_tda = 0.0;
+  s->n_isdf = n_isdf;
+  s->nmem = nmem;
+  NGW_TRY(dalloc(s, (void **)&s->d_psi, (size_t)n_isdf * nmem * 8));
+  NGW_TRY(dalloc(s, (void **)&s->d_M, (size_t)n_isdf * n_isdf * 8));
+  NGW_CUDA(cudaMemcpyAsync(s->d_psi, psi_intp, (size_t)n_isdf * nmem * 8, cudaMemcpyHostToDevice,
+                           s->stream));
+  NGW_CUDA(cudaMemcpyAsync(s->d_M, mmtrx, (size_t)n_isdf * n_isdf * 8, cudaMemcpyHostToDevice,
+                           s->stream));
+  if (mxc) {
+    NGW_TRY(dalloc(s, (void **)&s->d_Mxc, (size_t)n_isdf * n_isdf * 8));
+    NGW_CUDA(cudaMemcpyAsync(s->d_Mxc, mxc, (size_t)n_isdf * n_isdf * 8, cudaMemcpyHostToDevice,
+                             s->stream));
+  }
+  if (s->have_pairs) NGW_TRY(dalloc(s, (void **)&s->d_C, (size_t)n_isdf * s->ncv * 8));
+  s->have_isdf = true;
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return NGW_OK;
+}
+
+int ngw_set_pairs(ngw_session *s, int ncv, const int *cvpair, const double *sqrtR) {
+  if (!s || ncv <= 0 || !cvpair || !sqrtR) {
+    set_error("ngw_set_pairs: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  if (s->have_isdf) {
+    for (int i = 0; i < 2 * ncv; ++i) {
+      if (cvpair[i] < 1 || cvpair[i] > s->nmem) {
+        set_error("ngw_set_pairs: band index %d out of 1..%d", cvpair[i], s->nmem);
+        return NGW_ERR_ARG;
+      }
+    }
+  }
+  if (!all_finite(sqrtR, ncv)) {
+    set_error("ngw_set_pairs: non-finite sqrtR");
+    return NGW_ERR_NONFINITE;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  mixed_free(s);
+  if (s->d_cvpair) dfree(s, s->d_cvpair, (size_t)2 * s->ncv * 4);
+  if (s->d_sqrtR) dfree(s, s->d_sqrtR, (size_t)s->ncv * 8);
+  if (s->d_C) dfree(s, s->d_C, (size_t)s->n_isdf * s->ncv * 8);
+  s->d_C = nullptr;
+  s->have_C = false;
+  s->lmax = s->lmax_tda = 0.0;
+  s->ncv = ncv;
+  NGW_TRY(dalloc(s, (void **)&s->d_cvpair, (size_t)2 * ncv * 4));
+  NGW_TRY(dalloc(s, (void **)&s->d_sqrtR, (size_t)ncv * 8));
+  NGW_CUDA(cudaMemcpyAsync(s->d_cvpair, cvpair, (size_t)2 * ncv * 4, cudaMemcpyHostToDevice,
+                           s->stream));
+  NGW_CUDA(cudaMemcpyAsync(s->d_sqrtR, sqrtR, (size_t)ncv * 8, cudaMemcpyHostToDevice, s->stream));
+  if (s->have_isdf) NGW_TRY(dalloc(s, (void **)&s->d_C, (size_t)s->n_isdf * ncv * 8));
+  s->have_pairs = true;
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return NGW_OK;
+}
+
+int ngw_matvec_isdf(ngw_session *s, const double *vec, double *hvec, int ld, int blksz,
+                    int tamm_d) {
+  NGW_TRY(need_op(s));
+  if (!vec || !hvec || blksz <= 0 || ld < s->ncv) {
+    set_error("ngw_matvec_isdf: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  const int ncv = s->ncv, nb = blksz;
+  double *din, *dout, *hs;
+  NGW_TRY(scratch(s, SL_IN, (size_t)ncv * nb * 8, (void **)&din));
+  NGW_TRY(scratch(s, SL_OUT, (size_t)ncv * nb * 8, (void **)&dout));
+  NGW_TRY(scratch(s, SL_HS, (size_t)ncv * nb * 8, (void **)&hs));
+  NGW_CUDA(cudaMemcpy2DAsync(din, (size_t)ncv * 8, vec, (size_t)ld * 8, (size_t)ncv * 8, nb,
+                             cudaMemcpyHostToDevice, s->stream));
+  if (s->precision == NGW_PREC_MIXED) {
+    // a single matvec in mixed precision: Chebyshev series "x" on [0, 2]
+    NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
+    const double g[2] = {1.0, 1.0};
+    NGW_TRY(mixed_poly_apply(s, nb, din, ncv, g, 1, 1.0, 1.0, tamm_d ? 1 : 0, dout));
+  } else {
+    launch_scale_rows(s->d_sqrtR, din, ncv, hs, ncv, ncv, nb, tamm_d, s->stream);
+    NGW_TRY(matvec_f64_dev(s, nb, hs, dout, din, tamm_d, 0, 0.0, 0.0, nullptr));
+  }
+  NGW_CUDA(cudaMemcpy2DAsync(hvec, (size_t)ld * 8, dout, (size_t)ncv * 8, (size_t)ncv * 8, nb,
+                             cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return check_status(s);
+}
+
+int ngw_polynomial_matvec_isdf(ngw_session *s, const double *polynomial, int npoly,
+                               const double *vec, double *hvec, int ld, int blksz) {
+  NGW_TRY(need_op(s));
+  if (!vec || !hvec || blksz <= 0 || ld < s->ncv || !polynomial || npoly < 1) {
+    set_error("ngw_polynomial_matvec_isdf: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  const int ncv = s->ncv, nb = blksz;
+  double *din, *dout, *hs;
+  NGW_TRY(scratch(s, SL_IN, (size_t)ncv * nb * 8, (void **)&din));
+  NGW_TRY(scratch(s, SL_OUT, (size_t)ncv * nb * 8, (void **)&dout));
+  NGW_TRY(scratch(s, SL_HS, (size_t)ncv * nb * 8, (void **)&hs));
+  NGW_CUDA(cudaMemcpy2DAsync(din, (size_t)ncv * 8, vec, (size_t)ld * 8, (size_t)ncv * 8, nb,
+                             cudaMemcpyHostToDevice, s->stream));
+  // the explicit Horner form of the reference, always in FP64
+  launch_scale_rows(s->d_sqrtR, din, ncv, hs, ncv, ncv, nb, 0, s->stream);
+  NGW_TRY(poly_f64_dev(s, nb, polynomial, npoly, din, hs, dout));
+  NGW_CUDA(cudaMemcpy2DAsync(hvec, (size_t)ld * 8, dout, (size_t)ncv * 8, (size_t)ncv * 8, nb,
+                             cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return check_status(s);
+}
+
+int ngw_lanczos_spectra_isdf(ngw_session *s, const double *v0, const double *v0_norm, int ld,
+                             const double *zz, int nz, int niter, const double *polynomial,
+                             int npoly, int blksz, int tamm_d, double *spectra, double *alpha,
+                             double *beta) {
+  NGW_TRY(need_op(s));
+  if (!v0 || !v0_norm || !zz || !spectra || nz <= 0 || niter <= 0 || blksz <= 0 || ld < s->ncv) {
+    set_error("ngw_lanczos_spectra_isdf: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  const int ncv = s->ncv, nb = blksz;
+  PolyPlan pp;
+  // mixed precision: Chebyshev interval [0, 1.02 lambda_max] of the operator
+  double lo = 0.0, hi = 0.0;
+  if (s->precision == NGW_PREC_MIXED) NGW_TRY(spectral_interval(s, tamm_d, &lo, &hi));
+  NGW_TRY(make_plan(s, pp, polynomial, npoly, tamm_d, lo, hi));
+  double *dv0, *V, *W, *hs, *tmp, *a, *b, *dzz, *dspec, *dnorm;
+  NGW_TRY(scratch(s, SL_IN, (size_t)ncv * nb * 8, (void **)&dv0));
+  NGW_TRY(scratch(s, SL_VEC, (size_t)ncv * nb * 8, (void **)&V));
+  NGW_TRY(scratch(s, SL_WVEC, (size_t)ncv * nb * 8, (void **)&W));
+  NGW_TRY(scratch(s, SL_HS, (size_t)ncv * nb * 8, (void **)&hs));
+  NGW_TRY(scratch(s, SL_TMP, (size_t)ncv * nb * 8, (void **)&tmp));
+  NGW_TRY(scratch(s, SL_A, (size_t)niter * nb * 8, (void **)&a));
+  NGW_TRY(scratch(s, SL_B, (size_t)niter * nb * 8, (void **)&b));
+  NGW_TRY(scratch(s, SL_ZZ, (size_t)nz * nb * 16, (void **)&dzz));
+  NGW_TRY(scratch(s, SL_SPEC, (size_t)nz * nb * 16, (void **)&dspec));
+  NGW_TRY(scratch(s, SL_PN, (size_t)nb * 8, (void **)&dnorm));
+  if (s->precision == NGW_PREC_MIXED) NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
+  NGW_CUDA(cudaMemcpy2DAsync(dv0, (size_t)ncv * 8, v0, (size_t)ld * 8, (size_t)ncv * 8, nb,
+                             cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(dnorm, v0_norm, (size_t)nb * 8, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(dzz, zz, (size_t)nz * nb * 16, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemsetAsync(b, 0, (size_t)niter * nb * 8, s->stream));
+  NGW_CUDA(cudaMemsetAsync(a, 0, (size_t)niter * nb * 8, s->stream));
+  launch_lanczos_init(dv0, ncv, dnorm, V, hs, s->d_sqrtR, ncv, nb, tamm_d, b, niter, s->stream);
+  NGW_TRY(lanczos_dev(s, pp, nb, niter, V, W, hs, tmp, a, b));
+  launch_contfrac(a, b, niter, nb, dzz, nz, dspec, s->stream);
+  NGW_CUDA(cudaGetLastError());
+  NGW_CUDA(cudaMemcpyAsync(spectra, dspec, (size_t)nz * nb * 16, cudaMemcpyDeviceToHost, s->stream));
+  if (alpha)
+    NGW_CUDA(cudaMemcpyAsync(alpha, a, (size_t)niter * nb * 8, cudaMemcpyDeviceToHost, s->stream));
+  if (beta)
+    NGW_CUDA(cudaMemcpyAsync(beta, b, (size_t)niter * nb * 8, cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return check_status(s);
+}
+
+int ngw_k_integrate_isdf(ngw_session *s, int kflag, const int *rows, int nrow, const int *cols,
+                         int ncol, double *kmat) {
+  if (!s || !s->have_isdf) {
+    set_error("ISDF operator not set");
+    return NGW_ERR_STATE;
+  }
+  if (!rows || !cols || !kmat || nrow <= 0 || ncol <= 0 || kflag < 0 || kflag > 2) {
+    set_error("ngw_k_integrate_isdf: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  if (kflag > 0 && !s->d_Mxc) {
+    set_error("kflag > 0 needs the f_xc kernel block");
+    return NGW_ERR_STATE;
+  }
+  for (int i = 0; i < 2 * nrow; ++i)
+    if (rows[i] < 1 || rows[i] > s->nmem) { set_error("row band out of range"); return NGW_ERR_ARG; }
+  for (int i = 0; i < 2 * ncol; ++i)
+    if (cols[i] < 1 || cols[i] > s->nmem) { set_error("col band out of range"); return NGW_ERR_ARG; }
+  NGW_CUDA(cudaSetDevice(s->device));
+  const int n = s->n_isdf;
+  std::vector<int> r1(nrow), r2(nrow), c1(ncol), c2(ncol);
+  for (int i = 0; i < nrow; ++i) { r1[i] = rows[2 * i]; r2[i] = rows[2 * i + 1]; }
+  for (int i = 0; i < ncol; ++i) { c1[i] = cols[2 * i]; c2[i] = cols[2 * i + 1]; }
+  int *db;
+  double *cr, *cc, *km, *tmp, *out;
+  NGW_TRY(scratch(s, SL_B1, (size_t)2 * (nrow + ncol) * 4, (void **)&db));
+  NGW_TRY(scratch(s, SL_KR, (size_t)n * nrow * 8, (void **)&cr));
+  NGW_TRY(scratch(s, SL_KC, (size_t)n * ncol * 8, (void **)&cc));
+  NGW_TRY(scratch(s, SL_KM, (size_t)n * n * 8, (void **)&km));
+  NGW_TRY(scratch(s, SL_T1, (size_t)n * nrow * 8, (void **)&tmp));
+  NGW_TRY(scratch(s, SL_OUT, (size_t)nrow * ncol * 8, (void **)&out));
+  NGW_CUDA(cudaMemcpyAsync(db, r1.data(), nrow * 4, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(db + nrow, r2.data(), nrow * 4, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(db + 2 * nrow, c1.data(), ncol * 4, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(db + 2 * nrow + ncol, c2.data(), ncol * 4, cudaMemcpyHostToDevice, s->stream));
+  launch_pair_gather_cols(s->d_psi, n, db, db + nrow, nrow, cr, s->stream);
+  launch_pair_gather_cols(s->d_psi, n, db + 2 * nrow, db + 2 * nrow + ncol, ncol, cc, s->stream);
+  launch_k_combine(s->d_M, s->d_Mxc, n, kflag, km, s->stream);
+  const double one = 1.0, zero = 0.0;
+  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrow, n, &one, km, n, cr, n, &zero,
+                         tmp, n));
+  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, nrow, ncol, n, &one, tmp, n, cc, n,
+                         &zero, out, nrow));
+  NGW_CUDA(cudaMemcpyAsync(kmat, out, (size_t)nrow * ncol * 8, cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return check_status(s);
+}
+
+int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e1,
+                      double *sigma_c, double *alpha, double *beta) {
+  NGW_TRY(need_op(s));
+  if (!p || !e1 || !sigma_c || p->nen < 2 || p->niter < 1 || p->nqp < 1 || !p->qp_bands ||
+      p->nval < 1 || p->nval >= s->nmem) {
+    set_error("ngw_sigma_lanczos: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  const int nbsum = p->nbands_sum > 0 ? p->nbands_sum : s->nmem;
+  if (nbsum > s->nmem) {
+    set_error("nbands_sum > nmem");
+    return NGW_ERR_ARG;
+  }
+  for (int i = 0; i < p->nqp; ++i)
+    if (p->qp_bands[i] < 1 || p->qp_bands[i] > s->nmem) {
+      set_error("qp band %d out of range", p->qp_bands[i]);
+      return NGW_ERR_ARG;
+    }
+  if (!all_finite(e1, s->nmem)) {
+    set_error("non-finite energies");
+    return NGW_ERR_NONFINITE;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  const int ncv = s->ncv, n = s->n_isdf, nen = p->nen, niter = p->niter;
+  const int tamm_d = p->tamm_d ? 1 : 0;
+  // Chebyshev interval (mixed): [0, 1.02 lambda_max(C)] unless given; C is
+  // positive definite, and the interval must contain its whole spectrum for the
+  // Clenshaw recurrence to be stable (the reference's fit range need not).
+  double lo = p->cheb_lo, hi = p->cheb_hi;
+  if (s->precision == NGW_PREC_MIXED && !(hi > lo)) NGW_TRY(spectral_interval(s, tamm_d, &lo, &hi));
+  PolyPlan pp;
+  NGW_TRY(make_plan(s, pp, p->polynomial, p->npoly, tamm_d, lo, hi));
+  // chain blocking: whole QP states per block
+  int nq_blk = p->nqp;
+  if (p->block_chains > 0) nq_blk = std::max(1, std::min(p->nqp, p->block_chains / nbsum));
+  const int nb_max = nq_blk * nbsum;
+  double *de1, *zz0, *sig, *cmn, *cm, *P, *P2, *pn2, *pn, *V, *W, *hs, *tmp, *a, *b, *S;
+  int *chb, *chq;
+  NGW_TRY(scratch(s, SL_E1, (size_t)s->nmem * 8, (void **)&de1));
+  NGW_TRY(scratch(s, SL_ZZ0, (size_t)p->nqp * 8, (void **)&zz0));
+  NGW_TRY(scratch(s, SL_SIG, (size_t)p->nqp * nen * 16, (void **)&sig));
+  NGW_TRY(scratch(s, SL_CMN, (size_t)n * nb_max * 8, (void **)&cmn));
+  NGW_TRY(scratch(s, SL_CM, (size_t)n * nb_max * 8, (void **)&cm));
+  NGW_TRY(scratch(s, SL_P, (size_t)ncv * nb_max * 8, (void **)&P));
+  NGW_TRY(scratch(s, SL_P2, (size_t)ncv * nb_max * 8, (void **)&P2));
+  NGW_TRY(scratch(s, SL_PN2, (size_t)nb_max * 8, (void **)&pn2));
+  NGW_TRY(scratch(s, SL_PN, (size_t)nb_max * 8, (void **)&pn));
+  NGW_TRY(scratch(s, SL_WVEC, (size_t)ncv * nb_max * 8, (void **)&W));
+  NGW_TRY(scratch(s, SL_HS, (size_t)ncv * nb_max * 8, (void **)&hs));
+  NGW_TRY(scratch(s, SL_TMP, (size_t)ncv * nb_max * 8, (void **)&tmp));
+  NGW_TRY(scratch(s, SL_A, (size_t)niter * nb_max * 8, (void **)&a));
+  NGW_TRY(scratch(s, SL_B, (size_t)niter * nb_max * 8, (void **)&b));
+  NGW_TRY(scratch(s, SL_SPECS, (size_t)(nen + 1) * nb_max * 16, (void **)&S));
+  NGW_TRY(scratch(s, SL_CHB, (size_t)2 * nb_max * 4, (void **)&chb));
+  NGW_TRY(scratch(s, SL_CHQ, (size_t)2 * nb_max * 4, (void **)&chq));
+  NGW_TRY(scratch(s, SL_VEC, (size_t)ncv * nb_max * 8, (void **)&V));
+  if (s->precision == NGW_PREC_MIXED) NGW_TRY(mixed_prepare_chains(s, nb_max, 0, 0, 0));
+  NGW_CUDA(cudaMemcpyAsync(de1, e1, (size_t)s->nmem * 8, cudaMemcpyHostToDevice, s->stream));
+  // energy grid origin per QP state: en0 = e1(m) - deltae/2, step deltae/(nen-1)
+  std::vector<double> hz0(p->nqp);
+  for (int i = 0; i < p->nqp; ++i) hz0[i] = e1[p->qp_bands[i] - 1] - p->deltae * 0.5;
+  const double de = p->deltae / (double)(nen - 1);
+  NGW_CUDA(cudaMemcpyAsync(zz0, hz0.data(), (size_t)p->nqp * 8, cudaMemcpyHostToDevice, s->stream));
+  const double one = 1.0, zero = 0.0;
+  std::vector<int> hb(2 * nb_max), hq(2 * nb_max);
+  for (int q0 = 0; q0 < p->nqp; q0 += nq_blk) {
+    const int nq = std::min(nq_blk, p->nqp - q0);
+    const int nb = nq * nbsum;
+    // chain (iq, n): band1 = m (QP band), band2 = n; chain_qp = block-local QP index
+    for (int iq = 0; iq < nq; ++iq)
+      for (int jn = 0; jn < nbsum; ++jn) {
+        const int j = iq * nbsum + jn;
+        hb[j] = p->qp_bands[q0 + iq];
+        hb[nb + j] = jn + 1;
+        hq[j] = q0 + iq;
+      }
+    NGW_CUDA(cudaMemcpyAsync(chb, hb.data(), (size_t)2 * nb * 4, cudaMemcpyHostToDevice, s->stream));
+    NGW_CUDA(cudaMemcpyAsync(chq, hq.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
+    NGW_CUDA(cudaStreamSynchronize(s->stream));
+    // start vectors  P = sqrtR * C^T M (psi_m psi_n)   (F90z:578-709), FP64
+    launch_pair_gather_cols(s->d_psi, n, chb, chb + nb, nb, cmn, s->stream);
+    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, n, nb, n, &one, s->d_M, n, cmn, n,
+                           &zero, cm, n));
+    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, ncv, nb, n, &one, s->d_C, n, cm, n,
+                           &zero, P, ncv));
+    launch_norms(P, ncv, nb, s->d_sqrtR, tamm_d, P2, pn2, s->stream);
+    NGW_CUDA(cudaMemsetAsync(a, 0, (size_t)niter * nb * 8, s->stream));
+    NGW_CUDA(cudaMemsetAsync(b, 0, (size_t)niter * nb * 8, s->stream));
+    // pnorm = sqrt(pnorm2), v0 = P / pnorm   (F90z:707-709, lanczos_spectra_lowcomsym.F90:68-70)
+    launch_sqrt_vec(pn2, pn, nb, s->stream);
+    launch_lanczos_init(P2, ncv, pn, V, hs, s->d_sqrtR, ncv, nb, tamm_d, b, niter, s->stream);
+    NGW_TRY(lanczos_dev(s, pp, nb, niter, V, W, hs, tmp, a, b));
+    launch_sigma_spectra(a, b, niter, nb, de1, chb + nb, chq, zz0, de, nen, p->ecuts, p->nval, S,
+                         s->stream);
+    launch_sigma_reduce(S, pn2, de1, chb + nb, zz0 + q0, de, nen, p->ecuts, p->nval, nbsum, nq,
+                        tamm_d, sig + (size_t)2 * q0 * nen, 0, s->stream);
+    NGW_CUDA(cudaGetLastError());
+    if (alpha)
+      NGW_CUDA(cudaMemcpyAsync(alpha + (size_t)q0 * nbsum * niter, a, (size_t)niter * nb * 8,
+                               cudaMemcpyDeviceToHost, s->stream));
+    if (beta)
+      NGW_CUDA(cudaMemcpyAsync(beta + (size_t)q0 * nbsum * niter, b, (size_t)niter * nb * 8,
+                               cudaMemcpyDeviceToHost, s->stream));
+  }
+  NGW_CUDA(cudaMemcpyAsync(sigma_c, sig, (size_t)p->nqp * nen * 16, cudaMemcpyDeviceToHost,
+                           s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return check_status(s);
+}
+
+int ngw_qp_newton(ngw_session *s, int nqp, int nen, const double *sigma_c_ev, const double *e1_ev,
+                  const double *e0_ev, double deltae_ev, const double *sigx_ev,
+                  const double *vxc_ev, double xacc_ev, double *eqp_ev, double *zfac, int *ierr) {
+  if (!s || nqp <= 0 || nen < 4 || !sigma_c_ev || !e1_ev || !e0_ev || !sigx_ev || !vxc_ev ||
+      !eqp_ev || !zfac || !ierr) {
+    set_error("ngw_qp_newton: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  double *dsig, *io, *w;
+  NGW_TRY(scratch(s, SL_SIG, (size_t)nqp * nen * 16, (void **)&dsig));
+  NGW_TRY(scratch(s, SL_QPIO, (size_t)nqp * 6 * 8 + (size_t)nqp * 4, (void **)&io));
+  NGW_TRY(scratch(s, SL_QPW, (size_t)nqp * 4 * nen * 8, (void **)&w));
+  double *d_e1 = io, *d_e0 = io + nqp, *d_sx = io + 2 * nqp, *d_vx = io + 3 * nqp;
+  double *d_eq = io + 4 * nqp, *d_z = io + 5 * nqp;
+  int *d_err = reinterpret_cast<int *>(io + 6 * nqp);
+  NGW_CUDA(cudaMemcpyAsync(dsig, sigma_c_ev, (size_t)nqp * nen * 16, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(d_e1, e1_ev, nqp * 8, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(d_e0, e0_ev, nqp * 8, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(d_sx, sigx_ev, nqp * 8, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(d_vx, vxc_ev, nqp * 8, cudaMemcpyHostToDevice, s->stream));
+  launch_qp_newton_ws(nqp, nen, dsig, d_e1, d_e0, deltae_ev, d_sx, d_vx, xacc_ev, d_eq, d_z, d_err,
+                      w, s->stream);
+  NGW_CUDA(cudaGetLastError());
+  NGW_CUDA(cudaMemcpyAsync(eqp_ev, d_eq, nqp * 8, cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(zfac, d_z, nqp * 8, cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(ierr, d_err, nqp * 4, cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return check_status(s);
+}
+
+}  // extern "C"

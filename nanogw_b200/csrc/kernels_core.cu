@@ -1,0 +1,585 @@
+// FP64 kernels of the ISDF-Lanczos GW path: pair gather, the matvec's
+// diagonal combine + Horner step, the Lanczos recurrence (one CTA per chain,
+// warp-shuffle reductions), the continued fraction, the Sigma_c accumulation
+// and the QP Newton solve.  All vectors are column blocks (ncv, nb) with the
+// pair index fastest, i.e. one chain's vector is contiguous.
+#include "ngw_internal.h"
+
+#include <cmath>
+
+namespace ngw {
+
+static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// pair products C(mu, icv) = psi(mu, c) * psi(mu, v)
+// (shared/apply_matvec_lowcomsym.F90:209-210, hadamard_prod_mat_sym.cpp:3-17)
+// 128-bit loads along mu when n_isdf is even (columns stay 16-byte aligned).
+__global__ void k_pair_gather_f64(const double *__restrict__ psi, int n_isdf,
+                                  const int *__restrict__ cvpair, int ncv,
+                                  double *__restrict__ C) {
+  const int cv = blockIdx.y;
+  if (cv >= ncv) return;
+  const int v = cvpair[2 * cv] - 1, c = cvpair[2 * cv + 1] - 1;
+  const double *pv = psi + (size_t)v * n_isdf;
+  const double *pc = psi + (size_t)c * n_isdf;
+  double *out = C + (size_t)cv * n_isdf;
+  if ((n_isdf & 1) == 0) {
+    const int n2 = n_isdf >> 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+      double2 a = reinterpret_cast<const double2 *>(pc)[i];
+      double2 b = reinterpret_cast<const double2 *>(pv)[i];
+      reinterpret_cast<double2 *>(out)[i] = make_double2(a.x * b.x, a.y * b.y);
+    }
+  } else {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_isdf; i += gridDim.x * blockDim.x)
+      out[i] = pc[i] * pv[i];
+  }
+}
+
+void launch_pair_gather_f64(const double *psi, int n_isdf, const int *cvpair, int ncv,
+                            double *C, cudaStream_t st) {
+  if (ncv <= 0) return;
+  int threads = 128;
+  int bx = cdiv((n_isdf + 1) / 2, threads);
+  if (bx > 8) bx = 8;
+  dim3 grid(bx, ncv);
+  k_pair_gather_f64<<<grid, threads, 0, st>>>(psi, n_isdf, cvpair, ncv, C);
+}
+
+// out(:, j) = psi(:, b1(j)) * psi(:, b2(j))  (start vectors C_mn, k_integrate)
+__global__ void k_pair_gather_cols(const double *__restrict__ psi, int n_isdf,
+                                   const int *__restrict__ b1, const int *__restrict__ b2, int n,
+                                   double *__restrict__ out) {
+  const int j = blockIdx.y;
+  if (j >= n) return;
+  const double *p1 = psi + (size_t)(b1[j] - 1) * n_isdf;
+  const double *p2 = psi + (size_t)(b2[j] - 1) * n_isdf;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_isdf; i += gridDim.x * blockDim.x)
+    out[(size_t)j * n_isdf + i] = p1[i] * p2[i];
+}
+
+void launch_pair_gather_cols(const double *psi, int n_isdf, const int *b1, const int *b2, int n,
+                             double *out, cudaStream_t st) {
+  if (n <= 0) return;
+  int bx = cdiv(n_isdf, 128);
+  if (bx > 8) bx = 8;
+  k_pair_gather_cols<<<dim3(bx, n), 128, 0, st>>>(psi, n_isdf, b1, b2, n, out);
+}
+
+// ---------------------------------------------------------------------------
+// y = sqrtR * x  (or a copy with TDA)   apply_matvec_lowcomsym.F90:112-128
+__global__ void k_scale_rows(const double *__restrict__ s, const double *__restrict__ x, int ldx,
+                             double *__restrict__ y, int ldy, int ncv, int nb, int tamm_d) {
+  const int j = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
+    double v = x[(size_t)j * ldx + i];
+    y[(size_t)j * ldy + i] = tamm_d ? v : s[i] * v;
+  }
+}
+
+void launch_scale_rows(const double *s, const double *x, int ldx, double *y, int ldy, int ncv,
+                       int nb, int tamm_d, cudaStream_t st) {
+  if (nb <= 0) return;
+  int bx = cdiv(ncv, 256);
+  if (bx > 16) bx = 16;
+  k_scale_rows<<<dim3(bx, nb), 256, 0, st>>>(s, x, ldx, y, ldy, ncv, nb, tamm_d);
+}
+
+__global__ void k_copy_cols(const double *__restrict__ x, int ldx, double *__restrict__ y, int ldy,
+                            int n, int nb) {
+  const int j = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[(size_t)j * ldy + i] = x[(size_t)j * ldx + i];
+}
+
+void launch_copy_cols(const double *x, int ldx, double *y, int ldy, int n, int nb,
+                      cudaStream_t st) {
+  if (nb <= 0) return;
+  int bx = cdiv(n, 256);
+  if (bx > 16) bx = 16;
+  k_copy_cols<<<dim3(bx, nb), 256, 0, st>>>(x, ldx, y, ldy, n, nb);
+}
+
+// Diagonal combine of the ISDF matvec (apply_matvec_lowcomsym.F90:396-412)
+//   non-TDA: y = sqrtR^3 * h + 4 sqrtR * z      (h = sqrtR * x)
+//   TDA:     y = sqrtR^2 * h + 2 z              (h = x)
+// followed by the Horner step (apply_matvec_lowcomsym.F90:504-511)
+//   k == 1: y = p_k * y + p_{k+1} * vec ;  k > 1: y = y + p_{k+1} * vec
+// and, for the next Horner matvec, hs = sqrtR * y (TDA: y).
+__global__ void k_matvec_combine(const double *__restrict__ s, const double *__restrict__ h,
+                                 const double *__restrict__ z, double *__restrict__ y,
+                                 const double *__restrict__ vec, int ncv, int nb, int tamm_d,
+                                 int horner_k, double pk, double pk1, double *__restrict__ hs) {
+  const int j = blockIdx.y;
+  const size_t base = (size_t)j * ncv;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
+    const double si = s[i];
+    double r;
+    if (tamm_d) {
+      r = (si * si) * h[base + i];
+      r = r + 2.0 * z[base + i];
+    } else {
+      r = (si * si * si) * h[base + i];
+      r = r + 4.0 * si * z[base + i];
+    }
+    if (horner_k == 1) {
+      r = pk * r + pk1 * vec[base + i];
+    } else if (horner_k > 1) {
+      r = r + pk1 * vec[base + i];
+    }
+    y[base + i] = r;
+    if (hs) hs[base + i] = tamm_d ? r : si * r;
+  }
+}
+
+void launch_matvec_combine(const double *s, const double *h, const double *z, double *y,
+                           const double *vec, int ncv, int nb, int tamm_d, int horner_k,
+                           double pk, double pk1, double *hs_next, cudaStream_t st) {
+  if (nb <= 0) return;
+  int bx = cdiv(ncv, 256);
+  if (bx > 16) bx = 16;
+  k_matvec_combine<<<dim3(bx, nb), 256, 0, st>>>(s, h, z, y, vec, ncv, nb, tamm_d, horner_k,
+                                                 pk, pk1, hs_next);
+}
+
+// ---------------------------------------------------------------------------
+// block reduction helper (sum of one double per thread; result to all threads)
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = (l < NT / 32) ? sh[l] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (l == 0) sh[32] = t;
+  }
+  __syncthreads();
+  return sh[32];
+}
+
+constexpr int LNT = 256;
+
+// vec = v0 / v0_norm ; b(1) = 1 ; hs = sqrtR * vec (TDA: vec)
+// (lanczos_spectra_lowcomsym.F90:68-72)
+__global__ void k_lanczos_init(const double *__restrict__ v0, int ld,
+                               const double *__restrict__ v0_norm, double *__restrict__ vec,
+                               double *__restrict__ hs, const double *__restrict__ s, int ncv,
+                               int tamm_d, double *__restrict__ b_elmt, int niter) {
+  const int j = blockIdx.x;
+  const double nrm = v0_norm[j];
+  for (int i = threadIdx.x; i < ncv; i += blockDim.x) {
+    double v = v0[(size_t)j * ld + i] / nrm;
+    vec[(size_t)j * ncv + i] = v;
+    hs[(size_t)j * ncv + i] = tamm_d ? v : s[i] * v;
+  }
+  if (threadIdx.x == 0) b_elmt[(size_t)j * niter] = 1.0;
+}
+
+void launch_lanczos_init(const double *v0, int ld, const double *v0_norm, double *vec, double *hs,
+                         const double *s, int ncv, int nb, int tamm_d, double *b_elmt, int niter,
+                         cudaStream_t st) {
+  if (nb <= 0) return;
+  k_lanczos_init<<<nb, LNT, 0, st>>>(v0, ld, v0_norm, vec, hs, s, ncv, tamm_d, b_elmt, niter);
+}
+
+// Rescale for the next step and hand the next matvec its input:
+//   w = w / b_k ; v = -v * b_k ; (swap: the caller exchanges the roles)
+//   hs = sqrtR * w  (w is the next "vec")          lanczos_spectra_lowcomsym.F90:121-128
+__device__ __forceinline__ void prescale_chain(double *w, double *v, int ncv, double bk,
+                                               const double *s, double *hs, int tamm_d) {
+  for (int i = threadIdx.x; i < ncv; i += blockDim.x) {
+    double wi = w[i] / bk;
+    w[i] = wi;
+    v[i] = -v[i] * bk;
+    hs[i] = tamm_d ? wi : s[i] * wi;
+  }
+}
+
+// a(1) = <w, v> ; w = w - a(1) v ; b(2) = ||w||   (lanczos_spectra_lowcomsym.F90:104-116)
+__global__ void k_lanczos_first(double *__restrict__ w, const double *__restrict__ v, int ncv,
+                                double *__restrict__ a, double *__restrict__ b, int niter) {
+  __shared__ double sh[33];
+  const int j = blockIdx.x;
+  double *wj = w + (size_t)j * ncv;
+  const double *vj = v + (size_t)j * ncv;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < ncv; i += blockDim.x) acc += wj[i] * vj[i];
+  const double a1 = block_sum<LNT>(acc, sh);
+  acc = 0.0;
+  for (int i = threadIdx.x; i < ncv; i += blockDim.x) {
+    double wi = wj[i] - a1 * vj[i];
+    wj[i] = wi;
+    acc += wi * wi;
+  }
+  const double bb = block_sum<LNT>(acc, sh);
+  if (threadIdx.x == 0) {
+    a[(size_t)j * niter] = a1;
+    if (niter >= 2) b[(size_t)j * niter + 1] = sqrt(bb);
+  }
+}
+
+void launch_lanczos_first(double *w, const double *v, int ncv, int nb, double *a, double *b,
+                          int niter, cudaStream_t st) {
+  if (nb <= 0) return;
+  k_lanczos_first<<<nb, LNT, 0, st>>>(w, v, ncv, a, b, niter);
+}
+
+__global__ void k_lanczos_prescale(double *__restrict__ w, double *__restrict__ v, int ncv, int k,
+                                   const double *__restrict__ b, int niter,
+                                   const double *__restrict__ s, double *__restrict__ hs,
+                                   int tamm_d) {
+  const int j = blockIdx.x;
+  const double bk = b[(size_t)j * niter + k];
+  prescale_chain(w + (size_t)j * ncv, v + (size_t)j * ncv, ncv, bk, s, hs + (size_t)j * ncv,
+                 tamm_d);
+}
+
+void launch_lanczos_prescale(double *w, double *v, int ncv, int nb, int k, const double *b,
+                             int niter, const double *s, double *hs, int tamm_d,
+                             cudaStream_t st) {
+  if (nb <= 0) return;
+  k_lanczos_prescale<<<nb, LNT, 0, st>>>(w, v, ncv, k, b, niter, s, hs, tamm_d);
+}
+
+// Step k (0-based, k >= 1):  w = w + t ; a(k) = <w, v> ;
+//   if k+1 < niter: w = w - a(k) v ; b(k+1) = ||w||    (lanczos_spectra_lowcomsym.F90:153-164)
+// and, when prescale_next, the next step's rescale (w /= b(k+1), v = -v b(k+1), hs).
+__global__ void k_lanczos_step(double *__restrict__ w, double *__restrict__ v,
+                               const double *__restrict__ t, int ncv, int k,
+                               double *__restrict__ a, double *__restrict__ b, int niter,
+                               const double *__restrict__ s, double *__restrict__ hs, int tamm_d,
+                               int prescale_next) {
+  __shared__ double sh[33];
+  const int j = blockIdx.x;
+  double *wj = w + (size_t)j * ncv;
+  double *vj = v + (size_t)j * ncv;
+  const double *tj = t + (size_t)j * ncv;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < ncv; i += blockDim.x) {
+    double wi = wj[i] + tj[i];
+    wj[i] = wi;
+    acc += wi * vj[i];
+  }
+  const double ak = block_sum<LNT>(acc, sh);
+  if (threadIdx.x == 0) a[(size_t)j * niter + k] = ak;
+  if (k + 1 < niter) {
+    acc = 0.0;
+    for (int i = threadIdx.x; i < ncv; i += blockDim.x) {
+      double wi = wj[i] - ak * vj[i];
+      wj[i] = wi;
+      acc += wi * wi;
+    }
+    const double bk1 = sqrt(block_sum<LNT>(acc, sh));
+    if (threadIdx.x == 0) b[(size_t)j * niter + k + 1] = bk1;
+    if (prescale_next) prescale_chain(wj, vj, ncv, bk1, s, hs + (size_t)j * ncv, tamm_d);
+  }
+}
+
+void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb, int k, double *a,
+                         double *b, int niter, const double *s, double *hs, int tamm_d,
+                         int prescale_next, cudaStream_t st) {
+  if (nb <= 0) return;
+  k_lanczos_step<<<nb, LNT, 0, st>>>(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next);
+}
+
+// ---------------------------------------------------------------------------
+// complex helpers (Smith's division)
+struct cplx {
+  double re, im;
+};
+__device__ __forceinline__ cplx cdivd(cplx a, cplx b) {
+  cplx r;
+  if (fabs(b.re) >= fabs(b.im)) {
+    double q = b.im / b.re, d = b.re + b.im * q;
+    r.re = (a.re + a.im * q) / d;
+    r.im = (a.im - a.re * q) / d;
+  } else {
+    double q = b.re / b.im, d = b.im + b.re * q;
+    r.re = (a.re * q + a.im) / d;
+    r.im = (a.im * q - a.re) / d;
+  }
+  return r;
+}
+
+// S = 0; for j = niter..1: S = (j == 1 ? 1 : b_j^2) / (z - a_j - S)
+// (lanczos_spectra_lowcomsym.F90:175-188)
+__device__ __forceinline__ cplx contfrac_eval(const double *a, const double *b, int niter, cplx z) {
+  cplx sacc = {0.0, 0.0};
+  for (int jj = niter - 1; jj >= 0; --jj) {
+    cplx num = {jj == 0 ? 1.0 : b[jj] * b[jj], 0.0};
+    cplx den = {z.re - a[jj] - sacc.re, z.im - sacc.im};
+    sacc = cdivd(num, den);
+  }
+  return sacc;
+}
+
+__global__ void k_contfrac(const double *__restrict__ a, const double *__restrict__ b, int niter,
+                           int nb, const double *__restrict__ zz, int nz,
+                           double *__restrict__ spectra) {
+  const int j = blockIdx.y;
+  const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iz >= nz || j >= nb) return;
+  const size_t o = (size_t)j * nz + iz;
+  cplx z = {zz[2 * o], zz[2 * o + 1]};
+  cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, niter, z);
+  spectra[2 * o] = r.re;
+  spectra[2 * o + 1] = r.im;
+}
+
+void launch_contfrac(const double *a, const double *b, int niter, int nb, const double *zz, int nz,
+                     double *spectra, cudaStream_t st) {
+  if (nb <= 0 || nz <= 0) return;
+  k_contfrac<<<dim3(cdiv(nz, 128), nb), 128, 0, st>>>(a, b, niter, nb, zz, nz, spectra);
+}
+
+// Per-chain spectra on the Sigma energy grid:
+//   zz_i = zz0 + de * i ; ezz_i = (E_n - zz_i) * eta_n + i*ecuts ; ezz_nen = 0
+// (calculate_sigma_lanczos_lowcomsym.F90:527-530,713-720).  S: (nen+1, nchain).
+__global__ void k_sigma_spectra(const double *__restrict__ a, const double *__restrict__ b,
+                                int niter, int nchain, const double *__restrict__ e1,
+                                const int *__restrict__ chain_band,
+                                const int *__restrict__ chain_qp, const double *__restrict__ zz0,
+                                double de, int nen, double ecuts, int nval,
+                                double *__restrict__ S) {
+  const int j = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nchain || i > nen) return;
+  const int n = chain_band[j];
+  const double eta = (n <= nval) ? 1.0 : -1.0;
+  cplx z;
+  if (i == nen) {
+    z.re = 0.0;
+    z.im = 0.0;
+  } else {
+    const double zz = de * (double)i + zz0[chain_qp[j]];
+    z.re = (-zz + e1[n - 1]) * eta;
+    z.im = ecuts;
+  }
+  cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, niter, z);
+  const size_t o = (size_t)j * (nen + 1) + i;
+  S[2 * o] = r.re;
+  S[2 * o + 1] = r.im;
+}
+
+void launch_sigma_spectra(const double *a, const double *b, int niter, int nchain,
+                          const double *e1, const int *chain_band, const int *chain_qp,
+                          const double *zz0, double de, int nen, double ecuts, int nval,
+                          double *S, cudaStream_t st) {
+  if (nchain <= 0) return;
+  k_sigma_spectra<<<dim3(cdiv(nen + 1, 128), nchain), 128, 0, st>>>(
+      a, b, niter, nchain, e1, chain_band, chain_qp, zz0, de, nen, ecuts, nval, S);
+}
+
+// Sigma_c(i, iq) (+)= sum_n in band order of
+//   non-TDA: (S_n(0) - S_n(ezz)) * eta_n * 2 * pnorm2_n / ezz
+//   TDA:     -S_n(ezz) * eta_n * sqrt(2) * pnorm2_n   (sqrt(2) in single precision, as 2.0**0.5)
+// (calculate_sigma_lanczos_lowcomsym.F90:736-745).  Chains of QP iq are
+// iq*nbsum .. iq*nbsum + nbsum-1 of this block.
+__global__ void k_sigma_reduce(const double *__restrict__ S, const double *__restrict__ pnorm2,
+                               const double *__restrict__ e1, const int *__restrict__ chain_band,
+                               const double *__restrict__ zz0, double de, int nen, double ecuts,
+                               int nval, int nbsum, int nqp, int tamm_d,
+                               double *__restrict__ sigma, int accumulate) {
+  const int iq = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iq >= nqp || i >= nen) return;
+  const double zz = de * (double)i + zz0[iq];
+  const double sqrt2f = (double)sqrtf(2.0f);
+  cplx acc = {0.0, 0.0};
+  if (accumulate) {
+    acc.re = sigma[2 * ((size_t)iq * nen + i)];
+    acc.im = sigma[2 * ((size_t)iq * nen + i) + 1];
+  }
+  for (int nn = 0; nn < nbsum; ++nn) {
+    const int j = iq * nbsum + nn;
+    const int n = chain_band[j];
+    const double eta = (n <= nval) ? 1.0 : -1.0;
+    const size_t o = (size_t)j * (nen + 1);
+    cplx s = {S[2 * (o + i)], S[2 * (o + i) + 1]};
+    cplx t;
+    if (tamm_d) {
+      t.re = -s.re * eta * sqrt2f * pnorm2[j];
+      t.im = -s.im * eta * sqrt2f * pnorm2[j];
+    } else {
+      cplx s0 = {S[2 * (o + nen)], S[2 * (o + nen) + 1]};
+      cplx d = {(s0.re - s.re) * eta * 2.0 * pnorm2[j], (s0.im - s.im) * eta * 2.0 * pnorm2[j]};
+      cplx ez = {(-zz + e1[n - 1]) * eta, ecuts};
+      t = cdivd(d, ez);
+    }
+    acc.re += t.re;
+    acc.im += t.im;
+  }
+  sigma[2 * ((size_t)iq * nen + i)] = acc.re;
+  sigma[2 * ((size_t)iq * nen + i) + 1] = acc.im;
+}
+
+void launch_sigma_reduce(const double *S, const double *pnorm2, const double *e1,
+                         const int *chain_band, const double *zz0, double de, int nen,
+                         double ecuts, int nval, int nbsum, int nqp, int tamm_d, double *sigma,
+                         int accumulate, cudaStream_t st) {
+  if (nqp <= 0) return;
+  k_sigma_reduce<<<dim3(cdiv(nen, 128), nqp), 128, 0, st>>>(S, pnorm2, e1, chain_band, zz0, de,
+                                                            nen, ecuts, nval, nbsum, nqp, tamm_d,
+                                                            sigma, accumulate);
+}
+
+// P = P * sqrtR (non-TDA) ; pnorm2 = <P, P>   (calculate_sigma_lanczos_lowcomsym.F90:696-705)
+__global__ void k_norms(const double *__restrict__ P, int ncv, const double *__restrict__ s,
+                        int tamm_d, double *__restrict__ Pout, double *__restrict__ pnorm2) {
+  __shared__ double sh[33];
+  const int j = blockIdx.x;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < ncv; i += blockDim.x) {
+    double p = P[(size_t)j * ncv + i];
+    if (!tamm_d) p = p * s[i];
+    Pout[(size_t)j * ncv + i] = p;
+    acc += p * p;
+  }
+  double t = block_sum<LNT>(acc, sh);
+  if (threadIdx.x == 0) pnorm2[j] = t;
+}
+
+void launch_norms(const double *P, int ncv, int nb, const double *s, int tamm_d, double *P_out,
+                  double *pnorm2, cudaStream_t st) {
+  if (nb <= 0) return;
+  k_norms<<<nb, LNT, 0, st>>>(P, ncv, s, tamm_d, P_out, pnorm2);
+}
+
+// ---------------------------------------------------------------------------
+// QP Newton solve: one thread per state.  spline / splint / spline_evaluate /
+// newtonr restate SIGMA/spline.f90, splint.f90, spline_evaluate.f90:37-48,
+// newtonr.f90:43-55; printsigma.F90:100-125 builds the table.
+// Workspace per state: 4 * nen doubles.
+__device__ void d_spline(const double *xx, const double *yy, int nn, double yp1, double ypn,
+                         double *y2, double *uu) {
+  const double HUGEV = 1.0e10;
+  if (fabs(yp1) > HUGEV) {
+    y2[0] = 0.0;
+    uu[0] = 0.0;
+  } else {
+    y2[0] = -0.5;
+    uu[0] = (3.0 / (xx[1] - xx[0])) * ((yy[1] - yy[0]) / (xx[1] - xx[0]) - yp1);
+  }
+  for (int i = 1; i < nn - 1; ++i) {
+    double sig = (xx[i] - xx[i - 1]) / (xx[i + 1] - xx[i - 1]);
+    double p = sig * y2[i - 1] + 2.0;
+    y2[i] = (sig - 1.0) / p;
+    uu[i] = (6.0 * ((yy[i + 1] - yy[i]) / (xx[i + 1] - xx[i]) - (yy[i] - yy[i - 1]) / (xx[i] - xx[i - 1])) /
+                 (xx[i + 1] - xx[i - 1]) -
+             sig * uu[i - 1]) /
+            p;
+  }
+  double qn, un;
+  if (ypn > HUGEV) {
+    qn = 0.0;
+    un = 0.0;
+  } else {
+    qn = 0.5;
+    un = (3.0 / (xx[nn - 1] - xx[nn - 2])) * (ypn - (yy[nn - 1] - yy[nn - 2]) / (xx[nn - 1] - xx[nn - 2]));
+  }
+  y2[nn - 1] = (un - qn * uu[nn - 2]) / (qn * y2[nn - 2] + 1.0);
+  for (int k = nn - 2; k >= 0; --k) y2[k] = y2[k] * y2[k + 1] + uu[k];
+}
+
+__device__ double d_splint(const double *xx, const double *yy, const double *y2a, int nn, double x0) {
+  int klo = 0, khi = nn - 1;
+  while (khi - klo > 1) {
+    int k = (khi + klo + 2) / 2 - 1;
+    if (xx[k] > x0) khi = k;
+    else klo = k;
+  }
+  double hh = xx[khi] - xx[klo];
+  double aa = (xx[khi] - x0) / hh, bb = (x0 - xx[klo]) / hh;
+  return aa * yy[klo] + bb * yy[khi] + ((aa * aa * aa - aa) * y2a[klo] + (bb * bb * bb - bb) * y2a[khi]) * (hh * hh) / 6.0;
+}
+
+// real part only is needed for the root and the derivative
+__device__ void d_spline_eval_re(const double *xt, const double *ft, int nt, double *y2, double *uu,
+                                 double x, double *fx, double *df) {
+  // spline through interior points 2..nt-1 with end slopes from the outer points
+  const double yp1 = (ft[1] - ft[0]) / (xt[1] - xt[0]);
+  const double ypn = (ft[nt - 1] - ft[nt - 2]) / (xt[nt - 1] - xt[nt - 2]);
+  d_spline(xt + 1, ft + 1, nt - 2, yp1, ypn, y2, uu);
+  *fx = d_splint(xt + 1, ft + 1, y2, nt - 2, x);
+  const double ym = d_splint(xt + 1, ft + 1, y2, nt - 2, x - 1.0e-2);
+  const double yp = d_splint(xt + 1, ft + 1, y2, nt - 2, x + 1.0e-2);
+  *df = (yp - ym) / 1.0e-2 * 0.5;
+}
+
+__global__ void k_qp_newton(int nqp, int nen, const double *__restrict__ sig,
+                            const double *__restrict__ e1, const double *__restrict__ e0,
+                            double deltae, const double *__restrict__ sigx,
+                            const double *__restrict__ vxc, double xacc, double *__restrict__ eqp,
+                            double *__restrict__ zfac, int *__restrict__ ierr,
+                            double *__restrict__ work) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nqp) return;
+  double *xt = work + (size_t)q * 4 * nen;
+  double *ft = xt + nen;
+  double *y2 = ft + nen;
+  double *uu = y2 + nen;
+  for (int i = 0; i < nen; ++i) {
+    xt[i] = e1[q] - deltae * 0.5 + deltae / (double)(nen - 1) * (double)i;
+    ft[i] = sigx[q] + sig[2 * ((size_t)q * nen + i)] - vxc[q] + e0[q] - xt[i];
+  }
+  double x = e1[q], fx = 0.0, df = 1.0;
+  int err = 21;   // Fortran loop counter after MAX_IT = 20 iterations
+  for (int it = 1; it <= 20; ++it) {
+    d_spline_eval_re(xt, ft, nen, y2, uu, x, &fx, &df);
+    const double dx = fx / df;
+    x = x - dx;
+    if (fabs(dx) < xacc) {
+      err = 0;
+      break;
+    }
+  }
+  d_spline_eval_re(xt, ft, nen, y2, uu, x, &fx, &df);
+  eqp[q] = x;
+  zfac[q] = -1.0 / df;
+  ierr[q] = err;
+}
+
+void launch_qp_newton_ws(int nqp, int nen, const double *sig, const double *e1, const double *e0,
+                         double deltae, const double *sigx, const double *vxc, double xacc,
+                         double *eqp, double *zfac, int *ierr, double *work, cudaStream_t st) {
+  if (nqp <= 0) return;
+  k_qp_newton<<<cdiv(nqp, 32), 32, 0, st>>>(nqp, nen, sig, e1, e0, deltae, sigx, vxc, xacc, eqp,
+                                            zfac, ierr, work);
+}
+
+__global__ void k_sqrt_vec(const double *__restrict__ x, double *__restrict__ y, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = sqrt(x[i]);
+}
+
+void launch_sqrt_vec(const double *x, double *y, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  k_sqrt_vec<<<cdiv(n, 256), 256, 0, st>>>(x, y, n);
+}
+
+__global__ void k_k_combine(const double *__restrict__ M, const double *__restrict__ Mxc, size_t n,
+                            int kflag, double *__restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (kflag < 2) v = M[i];
+    if (kflag > 0) v = v + Mxc[i];
+    out[i] = v;
+  }
+}
+
+void launch_k_combine(const double *M, const double *Mxc, int n, int kflag, double *out,
+                      cudaStream_t st) {
+  size_t nn = (size_t)n * n;
+  int blocks = cdiv((long long)nn, 256);
+  if (blocks > 4096) blocks = 4096;
+  k_k_combine<<<blocks, 256, 0, st>>>(M, Mxc, nn, kflag, out);
+}
+
+}  // namespace ngw

@@ -1,0 +1,130 @@
+// Internal declarations shared by the ngw_b200 translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cublas_v2.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/ngw_b200.h"
+
+namespace ngw {
+
+void set_error(const char *fmt, ...);
+
+#define NGW_CUDA(call)                                                           \
+  do {                                                                           \
+    cudaError_t e_ = (call);                                                     \
+    if (e_ != cudaSuccess) {                                                     \
+      ::ngw::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,               \
+                       cudaGetErrorString(e_));                                  \
+      return (e_ == cudaErrorMemoryAllocation) ? NGW_ERR_OOM : NGW_ERR_CUDA;     \
+    }                                                                            \
+  } while (0)
+
+#define NGW_CUBLAS(call)                                                         \
+  do {                                                                           \
+    cublasStatus_t st_ = (call);                                                 \
+    if (st_ != CUBLAS_STATUS_SUCCESS) {                                          \
+      ::ngw::set_error("%s:%d %s: cublas status %d", __FILE__, __LINE__, #call,  \
+                       (int)st_);                                                \
+      return NGW_ERR_CUDA;                                                       \
+    }                                                                            \
+  } while (0)
+
+#define NGW_TRY(call)                                                            \
+  do {                                                                           \
+    int r_ = (call);                                                             \
+    if (r_ != NGW_OK) return r_;                                                 \
+  } while (0)
+
+// Device buffer owned by a session (bytes tracked for admission / reporting).
+struct DBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+// Status word the kernels write when a bounded wait gives up or an index
+// check fails; read back after every synchronising call.
+enum DevStatus : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BOUNDS = 2 };
+
+struct MixedOperator;   // tcgen05 operand set (gemm_tc.cu)
+
+}  // namespace ngw
+
+struct ngw_session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  int precision = NGW_PREC_FP64;
+  size_t bytes = 0;
+  // operator
+  int n_isdf = 0, nmem = 0, ncv = 0;
+  double *d_psi = nullptr;     // (n_isdf, nmem) column-major
+  double *d_M = nullptr;       // (n_isdf, n_isdf)
+  double *d_Mxc = nullptr;     // optional
+  int *d_cvpair = nullptr;     // (2, ncv) 1-based
+  double *d_sqrtR = nullptr;   // (ncv)
+  double *d_C = nullptr;       // (n_isdf, ncv) pair products (FP64)
+  bool have_isdf = false, have_pairs = false, have_C = false;
+  ngw::MixedOperator *mixed = nullptr;
+  int *d_status = nullptr;     // device status word
+  double lmax = 0.0, lmax_tda = 0.0;   // cached spectral upper bounds (C, A)
+  // scratch (grown on demand)
+  std::vector<ngw::DBuf> scratch;
+  std::vector<void *> owned;
+};
+
+namespace ngw {
+
+// allocation helpers (track session bytes)
+int dalloc(ngw_session *s, void **p, size_t bytes);
+void dfree(ngw_session *s, void *p, size_t bytes);
+int scratch(ngw_session *s, int slot, size_t bytes, void **p);
+int check_status(ngw_session *s);
+
+// ---- FP64 path kernels (kernels_core.cu) ----
+void launch_pair_gather_f64(const double *psi, int n_isdf, const int *cvpair, int ncv,
+                            double *C, cudaStream_t st);
+void launch_pair_gather_cols(const double *psi, int n_isdf, const int *b1, const int *b2,
+                             int n, double *out, cudaStream_t st);
+void launch_scale_rows(const double *s, const double *x, int ldx, double *y, int ldy,
+                       int ncv, int nb, int tamm_d, cudaStream_t st);
+void launch_matvec_combine(const double *s, const double *h, const double *z, double *y,
+                           const double *vec, int ncv, int nb, int tamm_d, int horner_k,
+                           double pk, double pk1, double *hs_next, cudaStream_t st);
+void launch_copy_cols(const double *x, int ldx, double *y, int ldy, int n, int nb,
+                      cudaStream_t st);
+void launch_lanczos_init(const double *v0, int ld, const double *v0_norm, double *vec,
+                         double *hs, const double *s, int ncv, int nb, int tamm_d,
+                         double *b_elmt, int niter, cudaStream_t st);
+void launch_lanczos_first(double *w, const double *v, int ncv, int nb, double *a, double *b,
+                          int niter, cudaStream_t st);
+void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb, int k,
+                         double *a, double *b, int niter, const double *s, double *hs,
+                         int tamm_d, int prescale_next, cudaStream_t st);
+void launch_lanczos_prescale(double *w, double *v, int ncv, int nb, int k, const double *b,
+                             int niter, const double *s, double *hs, int tamm_d,
+                             cudaStream_t st);
+void launch_contfrac(const double *a, const double *b, int niter, int nb, const double *zz,
+                     int nz, double *spectra, cudaStream_t st);
+void launch_sigma_spectra(const double *a, const double *b, int niter, int nchain,
+                          const double *e1, const int *chain_band, const int *chain_qp,
+                          const double *zz0, double de, int nen, double ecuts, int nval,
+                          double *S, cudaStream_t st);
+void launch_sigma_reduce(const double *S, const double *pnorm2, const double *e1,
+                         const int *chain_band, const double *zz0, double de, int nen,
+                         double ecuts, int nval, int nbsum, int nqp, int tamm_d,
+                         double *sigma, int accumulate, cudaStream_t st);
+void launch_norms(const double *P, int ncv, int nb, const double *s, int tamm_d, double *P_out,
+                  double *pnorm2, cudaStream_t st);
+void launch_qp_newton_ws(int nqp, int nen, const double *sig, const double *e1, const double *e0,
+                         double deltae, const double *sigx, const double *vxc, double xacc,
+                         double *eqp, double *zfac, int *ierr, double *work, cudaStream_t st);
+void launch_sqrt_vec(const double *x, double *y, int n, cudaStream_t st);
+void launch_k_combine(const double *M, const double *Mxc, int n, int kflag, double *out,
+                      cudaStream_t st);
+
+}  // namespace ngw

@@ -1,0 +1,198 @@
+// Coulomb block of the ISDF kernel:  M_C = ntrans/hcub * zeta^T (v_c zeta).
+//
+// v_c zeta_mu is the FFT-Poisson solve of shared/fft_module.F90z:122-177: each
+// zeta column is packed into the (zero-padded) FFT box, transformed, multiplied
+// by the truncated Coulomb kernel 8 pi (1 - cos(R_t |G|)) / |G|^2
+// (8 pi R_t^2 / 2 at G = 0; shared/fft_module.F90z:628-691, R_t = 2 rmax), and
+// transformed back.  The box edge is nfft = even(nint(4 rmax / h))
+// (shared/parsec_wfn.F90:365-381), the scale 1/nfft^3 (fft_module.F90z:403),
+// and the kernel matrix is the GEMM of shared/isdf_parallel_sym_UltraLowMem.F90:865-867.
+// Columns are processed in batches: pack / multiply / unpack are kernels of
+// this library, the 3-D transforms are batched cuFFT D2Z / Z2D.
+#include <cufft.h>
+
+#include <cmath>
+#include <vector>
+
+#include "ngw_internal.h"
+
+namespace ngw {
+
+__global__ void k_coulomb_table(double *__restrict__ v, int n, double b, double trunc) {
+  const int nh = n / 2 + 1;
+  const size_t total = (size_t)n * n * nh;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(idx % nh);
+    const int bb = (int)((idx / nh) % n);
+    const int a = (int)(idx / ((size_t)nh * n));
+    const int ja = a < n / 2 ? a : a - n;
+    const int jb = bb < n / 2 ? bb : bb - n;
+    const int jc = c;
+    const double g2 = b * b * ((double)ja * ja + (double)jb * jb + (double)jc * jc);
+    double r;
+    if (ja == 0 && jb == 0 && jc == 0)
+      r = trunc * trunc / 2.0;
+    else
+      r = (1.0 - cos(trunc * sqrt(g2))) / g2;
+    v[idx] = 8.0 * M_PI * r;
+  }
+}
+
+// box[col][a][b][c] = zeta[col][g] at the grid point's (wrapped) coordinates
+__global__ void k_pack(const double *__restrict__ zeta, int ngrid, int ldz,
+                       const int *__restrict__ gidx, int n, double *__restrict__ box, int ncol) {
+  const int col = blockIdx.y;
+  const size_t bsz = (size_t)n * n * n;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngrid; g += gridDim.x * blockDim.x) {
+    int a = gidx[3 * g], b = gidx[3 * g + 1], c = gidx[3 * g + 2];
+    a = ((a % n) + n) % n;
+    b = ((b % n) + n) % n;
+    c = ((c % n) + n) % n;
+    box[(size_t)col * bsz + ((size_t)a * n + b) * n + c] = zeta[(size_t)col * ldz + g];
+  }
+  (void)ncol;
+}
+
+__global__ void k_unpack(const double *__restrict__ box, int ngrid, const int *__restrict__ gidx,
+                         int n, double scale, double *__restrict__ out, int ldo) {
+  const int col = blockIdx.y;
+  const size_t bsz = (size_t)n * n * n;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngrid; g += gridDim.x * blockDim.x) {
+    int a = gidx[3 * g], b = gidx[3 * g + 1], c = gidx[3 * g + 2];
+    a = ((a % n) + n) % n;
+    b = ((b % n) + n) % n;
+    c = ((c % n) + n) % n;
+    out[(size_t)col * ldo + g] = box[(size_t)col * bsz + ((size_t)a * n + b) * n + c] * scale;
+  }
+}
+
+__global__ void k_mul_coulomb(cufftDoubleComplex *__restrict__ f, const double *__restrict__ v,
+                              size_t per, int ncol) {
+  const size_t total = per * (size_t)ncol;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double w = v[i % per];
+    f[i].x *= w;
+    f[i].y *= w;
+  }
+}
+
+}  // namespace ngw
+
+using namespace ngw;
+
+extern "C" int ngw_build_coulomb_kernel(ngw_session *s, int ngrid, int n_isdf, const double *zeta,
+                                        const int *grid_idx, int nfft, double h, double trunc,
+                                        double *mmtrx) {
+  if (!s || ngrid <= 0 || n_isdf <= 0 || !zeta || !grid_idx || nfft < 4 || (nfft & 1) || h <= 0 ||
+      !mmtrx) {
+    set_error("ngw_build_coulomb_kernel: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  const int n = nfft;
+  const size_t bsz = (size_t)n * n * n;
+  const size_t csz = (size_t)n * n * (n / 2 + 1);
+  // batch so that the boxes stay under ~2 GB
+  int batch = (int)std::max<size_t>(1, (size_t)(2ull << 30) / (bsz * 8 + csz * 16));
+  if (batch > n_isdf) batch = n_isdf;
+  double *dz = nullptr, *dvz = nullptr, *box = nullptr, *vtab = nullptr, *dm = nullptr;
+  cufftDoubleComplex *spec = nullptr;
+  int *dg = nullptr;
+  int rc = NGW_OK;
+  cufftHandle pf = 0, pb = 0;
+  bool have_pf = false, have_pb = false;
+  auto fail = [&](int code) {
+    rc = code;
+    return code;
+  };
+  do {
+    if (dalloc(s, (void **)&dz, (size_t)ngrid * n_isdf * 8) ||
+        dalloc(s, (void **)&dvz, (size_t)ngrid * n_isdf * 8) ||
+        dalloc(s, (void **)&box, bsz * batch * 8) ||
+        dalloc(s, (void **)&spec, csz * batch * 16) || dalloc(s, (void **)&vtab, csz * 8) ||
+        dalloc(s, (void **)&dm, (size_t)n_isdf * n_isdf * 8) ||
+        dalloc(s, (void **)&dg, (size_t)3 * ngrid * 4)) {
+      fail(NGW_ERR_OOM);
+      break;
+    }
+    if (cudaMemcpyAsync(dz, zeta, (size_t)ngrid * n_isdf * 8, cudaMemcpyHostToDevice, s->stream) ||
+        cudaMemcpyAsync(dg, grid_idx, (size_t)3 * ngrid * 4, cudaMemcpyHostToDevice, s->stream)) {
+      set_error("copy to device failed");
+      fail(NGW_ERR_CUDA);
+      break;
+    }
+    const double b = 2.0 * M_PI / ((double)n * h);
+    k_coulomb_table<<<1024, 256, 0, s->stream>>>(vtab, n, b, trunc);
+    int dims[3] = {n, n, n};
+    if (cufftPlanMany(&pf, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, batch) != CUFFT_SUCCESS) {
+      set_error("cufftPlanMany D2Z failed");
+      fail(NGW_ERR_CUDA);
+      break;
+    }
+    have_pf = true;
+    if (cufftPlanMany(&pb, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, batch) != CUFFT_SUCCESS) {
+      set_error("cufftPlanMany Z2D failed");
+      fail(NGW_ERR_CUDA);
+      break;
+    }
+    have_pb = true;
+    cufftSetStream(pf, s->stream);
+    cufftSetStream(pb, s->stream);
+    const double scale = 1.0 / ((double)n * (double)n * (double)n);
+    for (int c0 = 0; c0 < n_isdf && rc == NGW_OK; c0 += batch) {
+      const int nc = std::min(batch, n_isdf - c0);
+      cudaMemsetAsync(box, 0, bsz * batch * 8, s->stream);
+      int bx = (ngrid + 255) / 256;
+      if (bx > 256) bx = 256;
+      k_pack<<<dim3(bx, nc), 256, 0, s->stream>>>(dz + (size_t)c0 * ngrid, ngrid, ngrid, dg, n, box,
+                                                  nc);
+      if (cufftExecD2Z(pf, box, spec) != CUFFT_SUCCESS) {
+        set_error("cufftExecD2Z failed");
+        fail(NGW_ERR_CUDA);
+        break;
+      }
+      k_mul_coulomb<<<2048, 256, 0, s->stream>>>(spec, vtab, csz, batch);
+      if (cufftExecZ2D(pb, spec, box) != CUFFT_SUCCESS) {
+        set_error("cufftExecZ2D failed");
+        fail(NGW_ERR_CUDA);
+        break;
+      }
+      k_unpack<<<dim3(bx, nc), 256, 0, s->stream>>>(box, ngrid, dg, n, scale,
+                                                    dvz + (size_t)c0 * ngrid, ngrid);
+    }
+    if (rc != NGW_OK) break;
+    if (cudaGetLastError() != cudaSuccess) {
+      set_error("Poisson kernels failed to launch");
+      fail(NGW_ERR_CUDA);
+      break;
+    }
+    // M = (ntrans / hcub) zeta^T (v_c zeta)
+    const double nf = 1.0 / (h * h * h);
+    const double zero = 0.0;
+    if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n_isdf, n_isdf, ngrid, &nf, dz, ngrid, dvz,
+                    ngrid, &zero, dm, n_isdf) != CUBLAS_STATUS_SUCCESS) {
+      set_error("cublasDgemm (zeta^T v zeta) failed");
+      fail(NGW_ERR_CUDA);
+      break;
+    }
+    if (cudaMemcpyAsync(mmtrx, dm, (size_t)n_isdf * n_isdf * 8, cudaMemcpyDeviceToHost, s->stream) ||
+        cudaStreamSynchronize(s->stream)) {
+      set_error("copy back failed");
+      fail(NGW_ERR_CUDA);
+      break;
+    }
+  } while (0);
+  cudaStreamSynchronize(s->stream);
+  if (have_pf) cufftDestroy(pf);
+  if (have_pb) cufftDestroy(pb);
+  dfree(s, dz, (size_t)ngrid * n_isdf * 8);
+  dfree(s, dvz, (size_t)ngrid * n_isdf * 8);
+  dfree(s, box, bsz * batch * 8);
+  dfree(s, spec, csz * batch * 16);
+  dfree(s, vtab, csz * 8);
+  dfree(s, dm, (size_t)n_isdf * n_isdf * 8);
+  dfree(s, dg, (size_t)3 * ngrid * 4);
+  return rc;
+}

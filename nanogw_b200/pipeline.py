@@ -1,0 +1,82 @@
+"""Setup pipeline: molecule -> ISDF points -> Psi_intp, zeta -> Coulomb kernel M.
+
+Order follows ``SIGMA/sigma.F90:318-738``: CVT point selection on the
+density (``shared/cvt.F90``), density de-duplication (``sigma.F90:377-461``),
+the ISDF fit of the interpolation vectors zeta
+(``shared/isdf_parallel_sym_UltraLowMem.F90:439-667``) and the Coulomb block
+``M = ntrans/hcub zeta^T v_c zeta`` built on the device
+(``:687-889``; library entry ``ngw_build_coulomb_kernel``).
+The fit (P, Q products and the A zeta^T = B solve) runs on the host with
+LAPACK in this version.
+"""
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import host, synth
+from .api import lowcomsym_pairs, sqrt_r
+
+
+@dataclass
+class IsdfOperator:
+    psi_intp: np.ndarray     # (n_isdf, nmem)
+    mmtrx: np.ndarray        # (n_isdf, n_isdf) Coulomb block, Ry
+    intp: np.ndarray         # 1-based grid indices of the points
+    e1: np.ndarray           # (nmem,) Ry
+    nval: int
+    cvt_iters: int
+    zeta: np.ndarray = None
+
+    @property
+    def nmem(self):
+        return self.psi_intp.shape[1]
+
+    @property
+    def n_isdf(self):
+        return self.psi_intp.shape[0]
+
+    def pairs(self):
+        cv = lowcomsym_pairs(self.nval, self.nmem)
+        return cv, sqrt_r(self.e1, cv)
+
+
+def fft_box_size(rmax, h):
+    """nfft = even(nint(4 rmax / h)) (``shared/parsec_wfn.F90:365-381``)."""
+    n = int(np.rint(4.0 * rmax / h))
+    return n + (n % 2)
+
+
+def isdf_fit(psi, psi_intp, mv, nmem):
+    """zeta (ngrid, n_isdf): P = sum_{v<=mv} psi_v(r_mu) psi_v(r),
+    Q = sum_{c<=nmem} psi_c(r_mu) psi_c(r), A = P_intp*Q_intp, B = P*Q, A Z = B."""
+    pv = psi_intp[:, :mv]
+    pc = psi_intp[:, :nmem]
+    P = pv @ psi[:, :mv].T
+    Q = pc @ psi[:, :nmem].T
+    A = (pv @ pv.T) * (pc @ pc.T)
+    B = P * Q
+    del P, Q
+    Z = np.linalg.solve(A, B)
+    return np.ascontiguousarray(Z.T)
+
+
+def build_operator(mol, n_isdf, session, qp_bands=(), seed=0, max_cvt_iter=100000,
+                   keep_zeta=False):
+    grid = mol.grid
+    init = synth.cvt_initial_points(grid, n_isdf, seed if seed else mol.seed)
+    intp, _, iters = host.cvt(grid, mol.rho, init, max_cvt_iter)
+    intp = host.dedup_points(intp, mol.rho)
+    psi_intp = np.asfortranarray(mol.psi[intp - 1, :])
+    mv = max([mol.nval] + [int(b) for b in qp_bands])
+    zeta = isdf_fit(mol.psi, psi_intp, mv, mol.nmem)
+    nfft = fft_box_size(mol.rmax, mol.h)
+    M = session.build_coulomb_kernel(zeta, mol.grid_idx, nfft, mol.h, 2.0 * mol.rmax)
+    return IsdfOperator(psi_intp=psi_intp, mmtrx=np.asfortranarray(M), intp=intp, e1=mol.e1.copy(),
+                        nval=mol.nval, cvt_iters=iters, zeta=zeta if keep_zeta else None)
+
+
+def qp_bands_near_gap(nval, nqp):
+    """The nqp bands nearest the gap: nqp/2 highest occupied, the rest lowest empty."""
+    nocc = nqp // 2
+    return np.array(list(range(nval - nocc + 1, nval + 1)) +
+                    list(range(nval + 1, nval + 1 + nqp - nocc)), dtype=np.int32)

@@ -1,0 +1,143 @@
+"""Oracle: ISDF Casida matvec, Horner polynomial matvec, Lanczos recurrence and
+continued fraction (FP64 numpy).  Test infrastructure only.
+
+Vectors are stored Fortran-style column blocks ``vec(ncv, blksz)``: numpy arrays
+of shape ``(ncv, blksz)``.
+"""
+import numpy as np
+
+
+def matvec_isdf(vec, cmtrx, mmtrx, sqrtR, tamm_d=False):
+    """H x for a block of columns.
+
+    Follows ``shared/apply_matvec_lowcomsym.F90:112-128`` (R^1/2 scaling),
+    ``:228-229`` (C x), ``:283-284`` (M (C x)), ``:365-366`` (C^T ...) and
+    ``:396-412`` (diagonal combine):
+        non-TDA: H x = R^{3/2} (R^{1/2} x) + 4 R^{1/2} C^T M C R^{1/2} x
+        TDA:     A x = R x + 2 C^T M C x
+    cmtrx: (n_isdf, ncv) pair products, mmtrx: (n_isdf, n_isdf), sqrtR: (ncv,).
+    """
+    vec = np.asarray(vec, dtype=np.float64)
+    one_d = vec.ndim == 1
+    if one_d:
+        vec = vec[:, None]
+    s = sqrtR[:, None]
+    if tamm_d:
+        h = vec.copy()
+    else:
+        h = s * vec
+    tmp = cmtrx @ h                      # (n_isdf, blksz)
+    mc = mmtrx @ tmp                     # (n_isdf, blksz)
+    cmc = cmtrx.T @ mc                   # (ncv, blksz)
+    if tamm_d:
+        h = (s * s) * h
+        h = h + 2.0 * cmc
+    else:
+        h = (s * s * s) * h
+        h = h + 4.0 * s * cmc
+    return h[:, 0] if one_d else h
+
+
+def polynomial_matvec_isdf(vec, polynomial, cmtrx, mmtrx, sqrtR):
+    """p(H) x by Horner's rule, coefficients stored high->low
+    (``polynomial(1) = a_n``).  Follows
+    ``shared/apply_matvec_lowcomsym.F90:490-514`` (and ``shared/apply_matvec.f90:169-184``).
+    """
+    npoly = len(polynomial) - 1
+    hold = np.array(vec, dtype=np.float64, copy=True)
+    hvec = None
+    for k in range(1, npoly + 1):
+        hvec = matvec_isdf(hold, cmtrx, mmtrx, sqrtR)
+        if k == 1:
+            hvec = polynomial[0] * hvec + polynomial[1] * vec
+        else:
+            hvec = hvec + polynomial[k] * vec
+        hold = hvec
+    return hvec
+
+
+def lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=None):
+    """Lanczos alpha/beta for a block of independent chains.
+
+    Follows ``shared/lanczos_spectra_lowcomsym.F90:67-166`` exactly (no
+    reorthogonalisation; ``b(1) = 1``; the ``k+1 <= niter`` guard).  With
+    ``early_exit_eps`` the chain stops when ``|b_k| < eps`` as in
+    ``shared/lanczos_spectra.f90:57-58`` (single chain only); the unset
+    tail is returned as zeros (the reference leaves it uninitialised).
+    Returns (a, b) with shape (niter, blksz).
+    """
+    v0 = np.asarray(v0, dtype=np.float64)
+    if v0.ndim == 1:
+        v0 = v0[:, None]
+    blksz = v0.shape[1]
+    v0_norm = np.broadcast_to(np.asarray(v0_norm, dtype=np.float64), (blksz,))
+    a = np.zeros((niter, blksz))
+    b = np.zeros((niter, blksz))
+    vec = v0 / v0_norm[None, :]
+    b[0, :] = 1.0
+    wvec = apply_h(vec)
+    a[0] = np.einsum("ij,ij->j", wvec, vec)
+    wvec = wvec - a[0][None, :] * vec
+    if niter >= 2:
+        b[1] = np.sqrt(np.einsum("ij,ij->j", wvec, wvec))
+    for k in range(1, niter):
+        if early_exit_eps is not None and np.all(np.abs(b[k]) < early_exit_eps):
+            break
+        wvec = wvec / b[k][None, :]
+        vec = -vec * b[k][None, :]
+        vec, wvec = wvec, vec
+        tmp = apply_h(vec)
+        wvec = wvec + tmp
+        a[k] = np.einsum("ij,ij->j", wvec, vec)
+        if k + 1 < niter:
+            wvec = wvec - a[k][None, :] * vec
+            b[k + 1] = np.sqrt(np.einsum("ij,ij->j", wvec, wvec))
+    return a, b
+
+
+def continued_fraction(a, b, zz):
+    """S(z) = <v|(z-H)^-1|v> from the Lanczos coefficients.
+
+    Follows ``shared/lanczos_spectra_lowcomsym.F90:175-188``:
+    S = 0; for j = niter..1: S = (j==1 ? 1 : b_j^2) / (z - a_j - S).
+    a, b: (niter, blksz); zz: (nz, blksz) complex.  Returns (nz, blksz).
+    """
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.ndim == 1:
+        a = a[:, None]
+        b = b[:, None]
+    zz = np.asarray(zz, dtype=np.complex128)
+    if zz.ndim == 1:
+        zz = zz[:, None]
+    niter = a.shape[0]
+    s = np.zeros(np.broadcast_shapes(zz.shape, (1, a.shape[1])), dtype=np.complex128)
+    for j in range(niter - 1, -1, -1):
+        num = 1.0 if j == 0 else b[j] * b[j]
+        s = num / (zz - a[j][None, :] - s)
+    return s
+
+
+def lanczos_spectra_isdf(v0, v0_norm, zz, niter, polynomial, cmtrx, mmtrx, sqrtR,
+                         tamm_d=False):
+    """``lanczos_spectra_isdf_lowcomsym`` (``shared/lanczos_spectra_lowcomsym.F90:7-190``):
+    the spectra <P|1/(zz-p(H))|P> for a block of start vectors.
+    Returns (spectra (nz, blksz), a, b)."""
+    if tamm_d:
+        def apply_h(x):
+            return matvec_isdf(x, cmtrx, mmtrx, sqrtR, tamm_d=True)
+    else:
+        def apply_h(x):
+            return polynomial_matvec_isdf(x, polynomial, cmtrx, mmtrx, sqrtR)
+    a, b = lanczos_recurrence(apply_h, v0, v0_norm, niter)
+    return continued_fraction(a, b, zz), a, b
+
+
+def dense_lanczos_spectra(H, v0, zz, niter):
+    """The dense-matrix test driver of ``shared/test_lanczos/test_lanczos.f90``
+    with the production recurrence (``niter`` Lanczos levels) -- used to pin the
+    oracle against the reference's golden table ``H_aux_v0.txt``."""
+    v0 = np.asarray(v0, dtype=np.float64)
+    nrm = np.sqrt(v0 @ v0)
+    a, b = lanczos_recurrence(lambda x: H @ x, v0[:, None], nrm, niter)
+    return continued_fraction(a, b, np.asarray(zz)[:, None])[:, 0], a[:, 0], b[:, 0]

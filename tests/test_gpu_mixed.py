@@ -1,0 +1,47 @@
+"""Mixed-precision path (split-BF16 tcgen05 GEMMs, FP64 recurrence) against
+the FP64 oracle: QP energies within 1 meV."""
+import numpy as np
+import pytest
+
+import nanogw_b200 as ngw
+from oracle import lanczos as L
+from oracle import sigma as OS
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def msess(small_system):
+    s = ngw.Session(0, "mixed")
+    s.set_isdf(small_system.psi_intp, small_system.M)
+    s.set_pairs(small_system.cvpair, small_system.sqrtR)
+    yield s
+    s.close()
+
+
+def test_mixed_matvec_close(msess, small_system):
+    S = small_system
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((len(S.sqrtR), 16))
+    ref = L.matvec_isdf(x, S.Cmtrx, S.M, S.sqrtR)
+    got = msess.matvec_isdf(x)
+    rel = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+    assert rel < 1e-4, rel
+
+
+def test_mixed_sigma_qp_within_1mev(msess, small_system):
+    S = small_system
+    qp = np.array([S.nval - 1, S.nval, S.nval + 1, S.nval + 2], dtype=np.int32)
+    nen, deltae, ecuts, niter = 81, 2.0, 0.02, 24
+    got = msess.calculate_sigma_lanczos(S.e1, S.nval, qp, nen, deltae, ecuts, niter, S.poly)
+    ryd = OS.RYD
+    sigx = np.full(len(qp), -0.4)
+    vxc = np.full(len(qp), -0.6)
+    refs = np.stack([OS.sigma_c_state(S.psi_intp, S.M, S.e1, S.nval, int(m), nen, deltae, ecuts,
+                                      niter, S.poly) for m in qp], axis=1)
+    e_ref = OS.qp_energies(refs.T, S.e1, S.e1, qp, deltae, sigx, vxc, xacc_ev=1e-7)
+    e_got = OS.qp_energies(got.T, S.e1, S.e1, qp, deltae, sigx, vxc, xacc_ev=1e-7)
+    err_mev = np.array([abs(a[0] - b[0]) * 1e3 for a, b in zip(e_got, e_ref)])
+    print("QP error (meV):", err_mev)
+    assert np.all(err_mev < 1.0)
+    assert np.max(np.abs(got - refs)) * ryd < 5e-3

@@ -1,0 +1,169 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle on the same
+seeded inputs (small synthetic molecule, 96 ISDF points, 192 pairs).
+
+Tolerances (FP64 path): matvec 1e-12 relative to the largest element; the
+Horner polynomial amplifies rounding by up to ~1e5-1e6 (monomial basis), so
+p(H) x and alpha/beta are held to 1e-9 / 1e-10 relative; Sigma_c to 1e-8."""
+import numpy as np
+import pytest
+
+import nanogw_b200 as ngw
+from nanogw_b200 import NGWError
+from oracle import isdf as OI
+from oracle import lanczos as L
+from oracle import qp as OQ
+from oracle import sigma as OS
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sess(small_system):
+    s = ngw.Session(0, "fp64")
+    s.set_isdf(small_system.psi_intp, small_system.M)
+    s.set_pairs(small_system.cvpair, small_system.sqrtR)
+    yield s
+    s.close()
+
+
+def _rel(a, b):
+    return np.max(np.abs(a - b)) / np.max(np.abs(b))
+
+
+def test_matvec_fp64(sess, small_system):
+    S = small_system
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((len(S.sqrtR), 7))
+    ref = L.matvec_isdf(x, S.Cmtrx, S.M, S.sqrtR)
+    got = sess.matvec_isdf(x)
+    assert _rel(got, ref) < 1e-12
+    ref_t = L.matvec_isdf(x, S.Cmtrx, S.M, S.sqrtR, tamm_d=True)
+    got_t = sess.matvec_isdf(x, tamm_d=True)
+    assert _rel(got_t, ref_t) < 1e-12
+
+
+def test_polynomial_matvec_fp64(sess, small_system):
+    S = small_system
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((len(S.sqrtR), 3))
+    ref = L.polynomial_matvec_isdf(x, S.poly, S.Cmtrx, S.M, S.sqrtR)
+    got = sess.polynomial_matvec_isdf(x, S.poly)
+    assert _rel(got, ref) < 1e-9
+
+
+def test_lanczos_alpha_beta_fp64(sess, small_system):
+    """alpha/beta of the plain FP64 form within 1e-10 relative (reference
+    default lanczos_niter = 9)."""
+    S = small_system
+    p, pn2 = OS.start_vectors(S.psi_intp, S.M, S.Cmtrx, S.sqrtR, S.nval, np.arange(1, 9))
+    zz = np.linspace(-1.0, 1.0, 11) + 0.02j
+    spec_r, a_r, b_r = L.lanczos_spectra_isdf(p, np.sqrt(pn2), np.repeat(zz[:, None], 8, 1), 9,
+                                              S.poly, S.Cmtrx, S.M, S.sqrtR)
+    spec, a, b = sess.lanczos_spectra_isdf(p, np.sqrt(pn2), np.repeat(zz[:, None], 8, 1), 9, S.poly)
+    assert np.max(np.abs(a - a_r) / np.abs(a_r)) < 1e-10
+    assert np.max(np.abs(b[1:] - b_r[1:]) / np.abs(b_r[1:])) < 1e-10
+    assert _rel(spec, spec_r) < 1e-10
+
+
+def test_lanczos_tda_fp64(sess, small_system):
+    S = small_system
+    p, pn2 = OS.start_vectors(S.psi_intp, S.M, S.Cmtrx, S.sqrtR, S.nval, np.arange(1, 5),
+                              tamm_d=True)
+    zz = np.linspace(-1.0, 1.0, 5) + 0.02j
+    spec_r, a_r, b_r = L.lanczos_spectra_isdf(p, np.sqrt(pn2), np.repeat(zz[:, None], 4, 1), 12,
+                                              None, S.Cmtrx, S.M, S.sqrtR, tamm_d=True)
+    spec, a, b = sess.lanczos_spectra_isdf(p, np.sqrt(pn2), np.repeat(zz[:, None], 4, 1), 12,
+                                           None, tamm_d=True)
+    assert np.max(np.abs(a - a_r) / np.abs(a_r)) < 1e-10
+    assert _rel(spec, spec_r) < 1e-9
+
+
+@pytest.mark.parametrize("tamm_d", [False, True])
+def test_sigma_lanczos_fp64(sess, small_system, tamm_d):
+    S = small_system
+    qp = np.array([S.nval - 1, S.nval, S.nval + 1, S.nval + 2], dtype=np.int32)
+    nen, deltae, ecuts, niter = 41, 2.0, 0.02, 16
+    got, a, b = sess.calculate_sigma_lanczos(S.e1, S.nval, qp, nen, deltae, ecuts, niter, S.poly,
+                                             tamm_d=tamm_d, return_ab=True)
+    for i, m in enumerate(qp):
+        ref, ar, br, _, _ = OS.sigma_c_state(S.psi_intp, S.M, S.e1, S.nval, int(m), nen, deltae,
+                                             ecuts, niter, S.poly, tamm_d=tamm_d, return_ab=True)
+        assert _rel(got[:, i], ref) < 1e-8, (i, _rel(got[:, i], ref))
+        nb = S.nmem
+        ai = a[:, i * nb:(i + 1) * nb]
+        # first 9 steps: reference-default depth, 1e-10
+        assert np.max(np.abs(ai[:9] - ar[:9]) / np.abs(ar[:9])) < 1e-10
+
+
+def test_sigma_chain_blocking_is_invisible(sess, small_system):
+    S = small_system
+    qp = np.array([S.nval, S.nval + 1, S.nval + 2], dtype=np.int32)
+    a = sess.calculate_sigma_lanczos(S.e1, S.nval, qp, 21, 2.0, 0.02, 8, S.poly)
+    b = sess.calculate_sigma_lanczos(S.e1, S.nval, qp, 21, 2.0, 0.02, 8, S.poly,
+                                     block_chains=S.nmem)
+    assert _rel(b, a) < 1e-13
+
+
+def test_k_integrate(small_system):
+    S = small_system
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal(S.M.shape) * 0.01
+    Mxc = X + X.T
+    rows = np.array([[1, 9], [2, 10], [8, 8], [3, 30]], dtype=np.int32)
+    cols = np.array([[1, 9], [4, 12], [8, 20]], dtype=np.int32)
+    with ngw.Session(0) as s:
+        s.set_isdf(S.psi_intp, S.M, Mxc)
+        for kflag in (0, 1, 2):
+            ref = OI.k_integrate(S.psi_intp, S.M, Mxc, rows, cols, kflag)
+            got = s.k_integrate_isdf(kflag, rows, cols)
+            assert _rel(got, ref) < 1e-12
+
+
+def test_qp_newton(sess):
+    rng = np.random.default_rng(7)
+    nen, nqp = 101, 5
+    e1 = rng.uniform(-10, 5, nqp)
+    deltae = 10.0
+    x = e1[None, :] - deltae / 2 + deltae / (nen - 1) * np.arange(nen)[:, None]
+    # smooth model self-energy with a pole outside the window
+    sig = (0.8 / (x - e1[None, :] - 12.0) - 0.3 * (x - e1[None, :])) + 0.01j
+    sx = rng.uniform(-3, -1, nqp)
+    vx = rng.uniform(-4, -2, nqp)
+    eqp, z, ierr = sess.qp_newton(sig, e1, e1, deltae, sx, vx, 1e-6)
+    for i in range(nqp):
+        er, zr, ie = OQ.qp_solve(sig[:, i], e1[i], e1[i], deltae, sx[i], vx[i], xacc=1e-6)
+        assert ierr[i] == ie == 0
+        assert abs(eqp[i] - er) < 1e-9
+        assert abs(z[i] - zr) < 1e-7
+
+
+def test_coulomb_kernel_build(small_system):
+    S = small_system
+    mol = S.mol
+    vc = OI.coulomb_0d(S.nfft, mol.h, 2.0 * mol.rmax)
+    vz = OI.poisson(S.zeta, mol.grid_idx, S.nfft, vc)
+    ref, _ = OI.kernel_mmtrx(S.zeta, vz, mol.hcub)
+    with ngw.Session(0) as s:
+        got = s.build_coulomb_kernel(S.zeta, mol.grid_idx, S.nfft, mol.h, 2.0 * mol.rmax)
+    assert _rel(got, ref) < 1e-11
+
+
+def test_errors_are_codes(small_system):
+    S = small_system
+    with ngw.Session(0) as s:
+        with pytest.raises(NGWError) as e:
+            s.matvec_isdf(np.zeros((4, 1)))
+        assert e.value.code == ngw._lib.NGW_ERR_STATE
+        bad = S.M.copy()
+        bad[3, 4] = np.nan
+        with pytest.raises(NGWError) as e:
+            s.set_isdf(S.psi_intp, bad)
+        assert e.value.code == ngw._lib.NGW_ERR_NONFINITE
+        s.set_isdf(S.psi_intp, S.M)
+        cv = S.cvpair.copy()
+        cv[0, 1] = S.nmem + 5
+        with pytest.raises(NGWError) as e:
+            s.set_pairs(cv, S.sqrtR)
+        assert e.value.code == ngw._lib.NGW_ERR_ARG
+    with pytest.raises(NGWError):
+        ngw.Session(device=999)
