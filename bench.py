@@ -1,0 +1,317 @@
+"""Benchmark: Sigma_c solves/s of the ISDF-Lanczos GW path on B200.
+
+Workload (default): the 12-atom synthetic molecule -- 12 atoms in a 4-bohr
+sphere, grid radius 9 bohr at h = 0.35 (~71k points), 30 occupied + 90 empty
+orbitals, 600 CVT-selected ISDF points, 150 Lanczos steps, degree-12
+polynomial, 6 QP states nearest the gap, 400 energies over a 2 Ha window
+centred on each QP energy, eta = 0.01 Ha -- in the mixed-precision form
+(split-BF16 tcgen05 GEMMs, FP64 recurrence).  One step = one Sigma_c request:
+all 6 QP states (720 band chains) solved through Sigma_c(omega) and the QP
+Newton solve.  A solve = one QP state.  Inputs are seeded synthetic data.
+
+Timing: W warm-up steps, then K steps timed with CUDA events on the session's
+stream (barrier + synchronize around the timed region, max over ranks);
+between timed steps L2 is flushed by writing a 256 MB buffer (outside the
+per-step events).  ``e2e`` times the same request through the public API from
+pinned host buffers: upload of Psi_intp / M / pairs, operator build, solve,
+Newton, download.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="12-atom molecule, 30 occ + 90 empty, 600 ISDF points, 150 Lanczos steps, "
+                     "6 QP states x 400 energies", n_atoms=12, atom_radius=4.0, grid_radius=9.0,
+                h=0.35, n_occ=30, n_empty=90, n_isdf=600, niter=150, n_qp=6, nen=400,
+                deltae=4.0, ecuts=0.02, npoly=12, seed=11)
+METRIC = "Sigma_c solves/s"
+RYD = 13.60569193
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], d["bf16_tflops"], d.get("bf16_tflops_sustained"), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, device=0):
+        self.samples = []
+        self.proc = None
+        self.device = device
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[3 + i]
+                          and "Not" not in s[3 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
+
+
+def build_workload(sess, wl, seed_offset=0):
+    """Untimed setup: molecule, CVT points, ISDF fit, Coulomb kernel (device)."""
+    from nanogw_b200 import pipeline, synth
+    from nanogw_b200.polyfit import sigma_polynomial
+    mol = synth.make_molecule(wl["n_atoms"], wl["atom_radius"], wl["grid_radius"], wl["h"],
+                              wl["n_occ"], wl["n_empty"], wl["seed"] + seed_offset)
+    qp = pipeline.qp_bands_near_gap(mol.nval, wl["n_qp"])
+    op = pipeline.build_operator(mol, wl["n_isdf"], sess, qp_bands=qp, seed=wl["seed"] + seed_offset)
+    poly, emin, emax = sigma_polynomial(op.e1, op.nval, op.nmem, wl["npoly"])
+    return op, qp, poly
+
+
+def solve_once(sess, op, qp, poly, wl, sigx, vxc):
+    sig = sess.calculate_sigma_lanczos(op.e1, op.nval, qp, wl["nen"], wl["deltae"], wl["ecuts"],
+                                       wl["niter"], poly)
+    e1 = op.e1[qp - 1] * RYD
+    eqp, z, ierr = sess.qp_newton(sig * RYD, e1, e1, wl["deltae"] * RYD, sigx, vxc)
+    return sig, eqp
+
+
+def cpu_reference(op, qp, poly, wl, niter_sample):
+    """The oracle (CPU restatement of the reference path, numpy/OpenBLAS on all
+    host threads) on a bounded sample: one QP state, all band chains,
+    ``niter_sample`` Lanczos steps.  Returns seconds per full solve (scaled
+    linearly to the workload's Lanczos depth)."""
+    from oracle import sigma as OS
+    t = time.perf_counter()
+    OS.sigma_c_state(op.psi_intp, op.mmtrx, op.e1, op.nval, int(qp[0]), wl["nen"], wl["deltae"],
+                     wl["ecuts"], niter_sample, poly)
+    dt = time.perf_counter() - t
+    return dt * wl["niter"] / niter_sample
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--cpu-niter", type=int, default=15)
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    W = max(3, args.warmup)
+    K = args.steps
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    wl = dict(WORKLOAD)
+    import nanogw_b200 as ngw
+
+    if args.impl == "reference":
+        if rank != 0:
+            if dist:
+                dist.destroy_process_group()
+            return
+        # inputs built with the library's setup pipeline (untimed), then the
+        # oracle (restatement of the reference's CPU path) is timed
+        with ngw.Session(local, "fp64") as sess:
+            op, qp, poly = build_workload(sess, wl)
+        nthreads = os.cpu_count()
+        times = []
+        for i in range(W + K):
+            t = cpu_reference(op, qp, poly, wl, args.cpu_niter)
+            if i >= W:
+                times.append(t)
+        v = 1.0 / float(np.mean(times))
+        sample = (f"1 QP state x {op.nmem} band chains x {args.cpu_niter} Lanczos steps per step, "
+                  f"scaled x{wl['niter'] / args.cpu_niter:.0f} to {wl['niter']} steps")
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
+                "n_gpus": args.gpus, "steps": K, "warmup": W, "ms_per_step": 1e3 * float(np.mean(times)),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": wl["name"], "parallelism": "cpu"},
+                "cpu_baseline": {"value": v, "unit": "solves/s", "cores": nthreads, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    sess = ngw.Session(local, "fp64")
+    op, qp, poly = build_workload(sess, wl, seed_offset=rank)
+    cv, sr = op.pairs()
+    sess.set_isdf(op.psi_intp, op.mmtrx)
+    sess.set_pairs(cv, sr)
+    nq = len(qp)
+    sigx = np.full(nq, -12.0)
+    vxc = np.full(nq, -10.0)
+
+    # ---- plain FP64 GPU path (comparison point of the metric) ----
+    t = time.perf_counter()
+    sig64, eqp64 = solve_once(sess, op, qp, poly, wl, sigx, vxc)
+    torch.cuda.synchronize()
+    fp64_times = []
+    for _ in range(args.fp64_steps):
+        t = time.perf_counter()
+        sig64, eqp64 = solve_once(sess, op, qp, poly, wl, sigx, vxc)
+        fp64_times.append(time.perf_counter() - t)
+    fp64_sps = nq / float(np.mean(fp64_times))
+
+    # ---- mixed-precision path ----
+    sess.set_precision(args.precision)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    ext = torch.cuda.ExternalStream(sess.stream_ptr, device=f"cuda:{local}")
+    for _ in range(W):
+        sigm, eqpm = solve_once(sess, op, qp, poly, wl, sigx, vxc)
+    qp_err_mev = float(np.max(np.abs(eqpm - eqp64)) * 1e3)
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    step_ms = []
+    lat = []
+    for _ in range(K):
+        with torch.cuda.stream(ext):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        t = time.perf_counter()
+        solve_once(sess, op, qp, poly, wl, sigx, vxc)
+        with torch.cuda.stream(ext):
+            e1.record()
+        e1.synchronize()
+        lat.append(time.perf_counter() - t)
+        step_ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    tot_ms = float(np.sum(step_ms))
+    if dist:
+        tt = torch.tensor([tot_ms], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot_ms = float(tt.item())
+    value = world * K * nq / (tot_ms / 1e3)
+
+    # ---- roofline of the dominant kernel (the two tcgen05 GEMMs) ----
+    nb = nq * op.nmem
+    roof = None
+    if args.precision == "mixed":
+        us1, us2 = sess.profile_mixed_gemms(nb, reps=50)
+        M1, N1, K1, BN1, sp1, M2, N2, K2, BN2 = sess.mixed_gemm_shapes(nb)
+        flops = 2.0 * M1 * N1 * K1 + 2.0 * M2 * N2 * K2
+        achieved = flops / ((us1 + us2) * 1e-6) / 1e12
+        hbm, bf16, bf16s, src = load_peaks()
+        roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+                "frac": achieved / bf16, "traffic": None,
+                "kernel": "k_tc_gemm (GEMM1 + GEMM2 of one matvec)",
+                "us_per_launch": [us1, us2], "shapes": [[M1, N1, K1, BN1, sp1], [M2, N2, K2, BN2]],
+                "peak_source": f"{src} (bf16 dense, burst)",
+                "executed_bf16_frac": 3.0 * achieved / bf16}
+
+    # ---- e2e through the public API from pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(np.asfortranarray(a)).pin_memory().numpy()  # noqa: E731
+        psi_h = torch.empty(op.psi_intp.shape[::-1], dtype=torch.float64).pin_memory().numpy().T
+        psi_h[...] = op.psi_intp
+        m_h = torch.empty(op.mmtrx.shape[::-1], dtype=torch.float64).pin_memory().numpy().T
+        m_h[...] = op.mmtrx
+        cv_h = pin(cv)
+        sr_h = pin(sr)
+        e2e_t = []
+        for i in range(2 + max(2, K // 2)):
+            t = time.perf_counter()
+            sess.set_isdf(psi_h, m_h)
+            sess.set_pairs(cv_h, sr_h)
+            solve_once(sess, op, qp, poly, wl, sigx, vxc)
+            if i >= 2:
+                e2e_t.append(time.perf_counter() - t)
+        h2d = psi_h.nbytes + m_h.nbytes + cv_h.nbytes + sr_h.nbytes + op.e1.nbytes + 4 * nq * 8
+        d2h = wl["nen"] * nq * 16 + nq * (8 + 8 + 4)
+        e2e = {"value": world * nq / float(np.mean(e2e_t)), "unit": "solves/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    # ---- CPU baseline (rank 0, N=1 only) ----
+    cpu = None
+    if rank == 0 and world == 1:
+        tcpu = cpu_reference(op, qp, poly, wl, args.cpu_niter)
+        cpu = {"value": 1.0 / tcpu, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"1 QP state x {op.nmem} chains x {args.cpu_niter} Lanczos steps, scaled to "
+                         f"{wl['niter']} steps (oracle: numpy/OpenBLAS FP64)"}
+
+    launches_per_step = wl["niter"] * (wl["npoly"] * 3 + 1) + 8
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": K,
+                "warmup": W, "ms_per_step": tot_ms / K, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16x3/f32 GEMM + f64 recurrence"
+                if args.precision == "mixed" else "f64",
+                "data": "synthetic (seeded molecule per rank)",
+                "config": {"workload": wl["name"], "chains_per_step": nb, "precision": args.precision,
+                           "l2": "flushed between timed steps (256 MB write)",
+                           "parallelism": f"replicas x{world}"},
+                "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
+                               "p99": 1e3 * float(np.percentile(lat, 99))},
+                "fp64_gpu": {"value": fp64_sps, "unit": "solves/s",
+                             "ms_per_step": 1e3 * float(np.mean(fp64_times))},
+                "speedup_vs_fp64_gpu": value / world / fp64_sps,
+                "qp_err_mev_vs_fp64": qp_err_mev,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "gpu_launches": K * launches_per_step}
+        print(json.dumps(line), flush=True)
+    sess.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

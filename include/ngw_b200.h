@@ -126,6 +126,15 @@ int ngw_qp_newton(ngw_session *s, int nqp, int nen, const double *sigma_c_ev,
                   const double *sigx_ev, const double *vxc_ev, double xacc_ev,
                   double *eqp_ev, double *zfac, int *ierr);
 
+/* ---- measurement ---- */
+/* Average device time (us) of one launch of each mixed-precision GEMM for nb
+ * chains (GEMM1: T = C_isdf S, GEMM2: Z = (M C_isdf)^T T with its Clenshaw
+ * epilogue), from CUDA events around `reps` back-to-back launches on the
+ * session stream.  No reference counterpart: used by the benchmark. */
+int ngw_profile_mixed_gemms(ngw_session *s, int nb, int reps, double *us_gemm1, double *us_gemm2);
+/* shape[9] = {M1, N1, K1, BN1, splitK1, M2, N2, K2, BN2} of the two GEMMs. */
+int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape);
+
 /* ---- setup path ---- */
 /* Shell sort (ascending) returning a 1-based permutation. Host code. */
 int ngw_shell_sort(int n, const double *arr, int *idx);

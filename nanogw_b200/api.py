@@ -177,6 +177,18 @@ class Session:
                                   _p(vx), float(xacc_ev), _p(eqp), _p(z), _p(ierr)))
         return eqp, z, ierr
 
+    def profile_mixed_gemms(self, nb, reps=20):
+        """(us_gemm1, us_gemm2): mean device time of one launch of each GEMM."""
+        t1 = np.zeros(1)
+        t2 = np.zeros(1)
+        check(lib().ngw_profile_mixed_gemms(self._h, int(nb), int(reps), _p(t1), _p(t2)))
+        return float(t1[0]), float(t2[0])
+
+    def mixed_gemm_shapes(self, nb):
+        sh = np.zeros(9, dtype=np.int32)
+        check(lib().ngw_mixed_gemm_shapes(self._h, int(nb), _p(sh)))
+        return [int(x) for x in sh]
+
     def build_coulomb_kernel(self, zeta, grid_idx, nfft, h, trunc):
         zt = _f64(zeta)
         g = np.ascontiguousarray(grid_idx, dtype=np.int32)

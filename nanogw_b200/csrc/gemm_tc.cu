@@ -693,3 +693,61 @@ void monomial_to_chebyshev(const double *poly_hl, int n, double lo, double hi, d
 }
 
 }  // namespace ngw
+
+// ---------------------------------------------------------------------------
+// Per-kernel timing of the two mixed-precision GEMMs on the session stream
+// (CUDA events around `reps` back-to-back launches of each), used by the
+// benchmark's roofline report.  Operates on the session's own chain buffers.
+extern "C" int ngw_profile_mixed_gemms(ngw_session *s, int nb, int reps, double *us_gemm1,
+                                       double *us_gemm2) {
+  using namespace ngw;
+  if (!s || nb <= 0 || reps <= 0 || !us_gemm1 || !us_gemm2) {
+    set_error("ngw_profile_mixed_gemms: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  if (!s->mixed) {
+    set_error("mixed operator not built (set precision to mixed and set the operator)");
+    return NGW_ERR_STATE;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
+  MixedOperator *op = s->mixed;
+  cudaEvent_t e0, e1, e2;
+  NGW_CUDA(cudaEventCreate(&e0));
+  NGW_CUDA(cudaEventCreate(&e1));
+  NGW_CUDA(cudaEventCreate(&e2));
+  NGW_TRY(run_gemm1(s, nb));   // warm
+  NGW_TRY(run_gemm2(s, nb, op->bb[0], nullptr, nullptr, 0, 0.0, 1.0, 0.0, 0.0, 0, op->bb[1],
+                    nullptr, true));
+  NGW_CUDA(cudaEventRecord(e0, s->stream));
+  for (int i = 0; i < reps; ++i) NGW_TRY(run_gemm1(s, nb));
+  NGW_CUDA(cudaEventRecord(e1, s->stream));
+  for (int i = 0; i < reps; ++i)
+    NGW_TRY(run_gemm2(s, nb, op->bb[0], nullptr, nullptr, 0, 0.0, 1.0, 0.0, 0.0, 0, op->bb[1],
+                      nullptr, true));
+  NGW_CUDA(cudaEventRecord(e2, s->stream));
+  NGW_CUDA(cudaEventSynchronize(e2));
+  float t1 = 0, t2 = 0;
+  NGW_CUDA(cudaEventElapsedTime(&t1, e0, e1));
+  NGW_CUDA(cudaEventElapsedTime(&t2, e1, e2));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  *us_gemm1 = 1e3 * t1 / reps;
+  *us_gemm2 = 1e3 * t2 / reps;
+  return check_status(s);
+}
+
+// Shapes of the two GEMMs for the roofline (padded M, N, K and split-K).
+extern "C" int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape) {
+  using namespace ngw;
+  if (!s || !s->mixed || !shape) {
+    set_error("mixed operator not built");
+    return NGW_ERR_STATE;
+  }
+  NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
+  MixedOperator *op = s->mixed;
+  shape[0] = op->n_isdf; shape[1] = nb; shape[2] = op->ncv; shape[3] = op->BN1; shape[4] = op->split1;
+  shape[5] = op->ncv; shape[6] = nb; shape[7] = op->n_isdf; shape[8] = op->BN2;
+  return NGW_OK;
+}

@@ -72,7 +72,7 @@ def poisson(rho_cols, grid_idx, nfft, vcoul):
         box[ix[:, 0], ix[:, 1], ix[:, 2]] = rho_cols[:, k]
         f = np.fft.rfftn(box)
         f *= vcoul[:, :, : nfft // 2 + 1]
-        r = np.fft.irfftn(f, s=(nfft, nfft, nfft))
+        r = np.fft.irfftn(f, s=(nfft, nfft, nfft), axes=(0, 1, 2))
         out[:, k] = r[ix[:, 0], ix[:, 1], ix[:, 2]]
     return out
 

@@ -38,16 +38,17 @@ def matvec_isdf(vec, cmtrx, mmtrx, sqrtR, tamm_d=False):
     return h[:, 0] if one_d else h
 
 
-def polynomial_matvec_isdf(vec, polynomial, cmtrx, mmtrx, sqrtR):
+def polynomial_matvec_isdf(vec, polynomial, cmtrx, mmtrx, sqrtR, matvec=None):
     """p(H) x by Horner's rule, coefficients stored high->low
     (``polynomial(1) = a_n``).  Follows
     ``shared/apply_matvec_lowcomsym.F90:490-514`` (and ``shared/apply_matvec.f90:169-184``).
+    ``matvec`` overrides the H application (used to inject rounding-size noise).
     """
     npoly = len(polynomial) - 1
     hold = np.array(vec, dtype=np.float64, copy=True)
     hvec = None
     for k in range(1, npoly + 1):
-        hvec = matvec_isdf(hold, cmtrx, mmtrx, sqrtR)
+        hvec = matvec(hold) if matvec else matvec_isdf(hold, cmtrx, mmtrx, sqrtR)
         if k == 1:
             hvec = polynomial[0] * hvec + polynomial[1] * vec
         else:
@@ -118,17 +119,32 @@ def continued_fraction(a, b, zz):
     return s
 
 
+def perturbed(apply_h, rel, seed=1):
+    """Wrap an operator so every product carries a relative rounding-size
+    perturbation ``rel``.  Used to measure how sensitive the unreorthogonalised
+    recurrence is to rounding: two FP64 codes that are equal in exact
+    arithmetic differ by about this much per matvec."""
+    rng = np.random.default_rng(seed)
+
+    def f(x):
+        y = apply_h(x)
+        return y * (1.0 + rel * rng.standard_normal(y.shape))
+    return f
+
+
 def lanczos_spectra_isdf(v0, v0_norm, zz, niter, polynomial, cmtrx, mmtrx, sqrtR,
-                         tamm_d=False):
+                         tamm_d=False, perturb=0.0):
     """``lanczos_spectra_isdf_lowcomsym`` (``shared/lanczos_spectra_lowcomsym.F90:7-190``):
     the spectra <P|1/(zz-p(H))|P> for a block of start vectors.
     Returns (spectra (nz, blksz), a, b)."""
+    mv = lambda x: matvec_isdf(x, cmtrx, mmtrx, sqrtR, tamm_d=tamm_d)   # noqa: E731
+    if perturb:
+        mv = perturbed(mv, perturb)
     if tamm_d:
-        def apply_h(x):
-            return matvec_isdf(x, cmtrx, mmtrx, sqrtR, tamm_d=True)
+        apply_h = mv
     else:
         def apply_h(x):
-            return polynomial_matvec_isdf(x, polynomial, cmtrx, mmtrx, sqrtR)
+            return polynomial_matvec_isdf(x, polynomial, cmtrx, mmtrx, sqrtR, matvec=mv)
     a, b = lanczos_recurrence(apply_h, v0, v0_norm, niter)
     return continued_fraction(a, b, zz), a, b
 

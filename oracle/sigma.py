@@ -53,7 +53,7 @@ def energy_grid(e1_m, deltae, nen):
 
 
 def sigma_c_state(psi_intp, mmtrx, e1, nval, m1, nen, deltae, ecuts, niter,
-                  polynomial, tamm_d=False, bands=None, return_ab=False):
+                  polynomial, tamm_d=False, bands=None, return_ab=False, perturb=0.0):
     """Sigma_c(omega) (Ry, complex, length nen) of QP band ``m1`` (1-based),
     summed over ``bands`` (default: all bands 1..nmem).
 
@@ -75,9 +75,11 @@ def sigma_c_state(psi_intp, mmtrx, e1, nval, m1, nen, deltae, ecuts, niter,
     ezz = np.zeros((nen + 1, len(bands)), dtype=np.complex128)
     ezz[:nen, :] = (-zz[:, None] + e1[bands - 1][None, :]) * eta[None, :] + 1j * ecuts
     spectra, a, b = L.lanczos_spectra_isdf(p, pnorm, ezz, niter, polynomial, cm, mmtrx, sr,
-                                           tamm_d=tamm_d)
+                                           tamm_d=tamm_d, perturb=perturb)
     if tamm_d:
-        tmp = -spectra[:nen, :] * eta[None, :] * 2.0 ** 0.5 * pnorm2[None, :]
+        # 2.0**0.5 is a default-real (single precision) expression in the Fortran
+        sqrt2 = float(np.sqrt(np.float32(2.0)))
+        tmp = -spectra[:nen, :] * eta[None, :] * sqrt2 * pnorm2[None, :]
     else:
         tmp = ((spectra[nen:nen + 1, :] - spectra[:nen, :]) * eta[None, :] * 2.0
                * pnorm2[None, :] / ezz[:nen, :])
