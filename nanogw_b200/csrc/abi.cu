@@ -11,7 +11,10 @@
 
 namespace ngw {
 
-int mixed_build_operator(ngw_session *s);
+int mixed_build_operator(ngw_session *s, int kdef, int tda);
+int mixed_kdef(ngw_session *s);
+int mixed_set_deflation_values(ngw_session *s, const double *pvals);
+int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps);
 int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1);
 int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const double *g, int n,
                      double c0, double c1, int tda, double *out64);
@@ -115,6 +118,10 @@ static int matvec_f64_dev(ngw_session *s, int nb, double *hs, double *y, const d
   return NGW_OK;
 }
 
+int matvec_f64_dev_pub(ngw_session *s, int nb, double *hs, double *y, int tamm_d) {
+  return matvec_f64_dev(s, nb, hs, y, nullptr, tamm_d, 0, 0.0, 0.0, nullptr);
+}
+
 // out = p(H) vec by Horner (FP64), vec/out: (ncv, nb); hs scratch holds
 // (R^1/2) vec on entry and is clobbered.
 static int poly_f64_dev(ngw_session *s, int nb, const double *poly, int npoly, const double *vec,
@@ -132,6 +139,7 @@ struct PolyPlan {
   std::vector<double> poly;   // high -> low
   std::vector<double> cheb;   // Chebyshev coefficients (mixed)
   double c0 = 0, c1 = 1;
+  int kdef = 0;               // deflated eigenpairs (mixed)
 };
 
 // t = p(H) vec  (or A vec with TDA) on device, in the session's precision.
@@ -187,94 +195,55 @@ static int need_op(ngw_session *s) {
     NGW_CUDA(cudaGetLastError());
     s->have_C = true;
   }
-  if (s->precision == NGW_PREC_MIXED && !s->mixed) NGW_TRY(mixed_build_operator(s));
   return NGW_OK;
 }
 
-// Largest eigenvalue of C (or of A with TDA) from a 40-step FP64 Lanczos
-// run on one deterministic start vector: the Ritz value converges from
-// below, and the Chebyshev interval of the mixed path adds a margin.
-static double tridiag_max_eig(const std::vector<double> &a, const std::vector<double> &b, int k) {
-  // Sturm-count bisection on T = tridiag(b[1..k-1], a[0..k-1], b[1..k-1])
-  double lo = a[0], hi = a[0];
-  for (int i = 0; i < k; ++i) {
-    const double r = (i > 0 ? std::fabs(b[i]) : 0.0) + (i + 1 < k ? std::fabs(b[i + 1]) : 0.0);
-    lo = std::min(lo, a[i] - r);
-    hi = std::max(hi, a[i] + r);
-  }
-  auto count_below = [&](double x) {
-    int c = 0;
-    double d = 1.0;
-    for (int i = 0; i < k; ++i) {
-      const double bb = (i > 0) ? b[i] * b[i] : 0.0;
-      d = a[i] - x - (i > 0 ? bb / d : 0.0);
-      if (d == 0.0) d = -1e-300;
-      if (d < 0) ++c;
-    }
-    return c;
-  };
-  for (int it = 0; it < 200 && hi - lo > 1e-14 * std::max(1.0, std::fabs(hi)); ++it) {
-    const double mid = 0.5 * (lo + hi);
-    if (count_below(mid) >= k) hi = mid;
-    else lo = mid;
-  }
-  return hi;
+static double poly_eval(const std::vector<double> &p, double x) {
+  long double acc = 0.0L;
+  for (double c : p) acc = acc * x + (long double)c;
+  return (double)acc;
 }
 
-static int estimate_lambda_max(ngw_session *s, int tamm_d, double *out) {
-  const int ncv = s->ncv;
-  const int k = std::min(40, ncv);
-  std::vector<double> v(ncv);
-  uint64_t st = 0x9E3779B97F4A7C15ull;
-  double nrm = 0.0;
-  for (int i = 0; i < ncv; ++i) {
-    st = st * 6364136223846793005ull + 1442695040888963407ull;
-    v[i] = (double)((st >> 11) & ((1ull << 53) - 1)) / 9007199254740992.0 - 0.5;
-    nrm += v[i] * v[i];
-  }
-  nrm = std::sqrt(nrm);
-  double *d0, *V, *W, *hs, *tmp, *a, *b, *dn;
-  NGW_TRY(scratch(s, SL_IN, (size_t)ncv * 8, (void **)&d0));
-  NGW_TRY(scratch(s, SL_VEC, (size_t)ncv * 8, (void **)&V));
-  NGW_TRY(scratch(s, SL_WVEC, (size_t)ncv * 8, (void **)&W));
-  NGW_TRY(scratch(s, SL_HS, (size_t)ncv * 8, (void **)&hs));
-  NGW_TRY(scratch(s, SL_TMP, (size_t)ncv * 8, (void **)&tmp));
-  NGW_TRY(scratch(s, SL_A, (size_t)k * 8, (void **)&a));
-  NGW_TRY(scratch(s, SL_B, (size_t)k * 8, (void **)&b));
-  NGW_TRY(scratch(s, SL_PN, 8, (void **)&dn));
-  NGW_CUDA(cudaMemcpyAsync(d0, v.data(), (size_t)ncv * 8, cudaMemcpyHostToDevice, s->stream));
-  NGW_CUDA(cudaMemcpyAsync(dn, &nrm, 8, cudaMemcpyHostToDevice, s->stream));
-  PolyPlan pp;
-  pp.tamm_d = tamm_d;
-  pp.npoly = 1;
-  pp.poly = {1.0, 0.0};
-  const int prec = s->precision;
-  s->precision = NGW_PREC_FP64;
-  launch_lanczos_init(d0, ncv, dn, V, hs, s->d_sqrtR, ncv, 1, tamm_d, b, k, s->stream);
-  int rc = lanczos_dev(s, pp, 1, k, V, W, hs, tmp, a, b);
-  s->precision = prec;
-  NGW_TRY(rc);
-  std::vector<double> ha(k), hb(k);
-  NGW_CUDA(cudaMemcpyAsync(ha.data(), a, (size_t)k * 8, cudaMemcpyDeviceToHost, s->stream));
-  NGW_CUDA(cudaMemcpyAsync(hb.data(), b, (size_t)k * 8, cudaMemcpyDeviceToHost, s->stream));
-  NGW_CUDA(cudaStreamSynchronize(s->stream));
-  // stop at a (numerically) invariant subspace
-  int kk = k;
-  for (int i = 1; i < k; ++i)
-    if (!(hb[i] > 1e-12 * std::fabs(ha[0]))) {
-      kk = i;
-      break;
+// Mixed-precision plan: Chebyshev interval and deflated eigenpairs.
+// Eigenpairs of the operator (C, or A with TDA) come from an FP64 Lanczos run
+// with full reorthogonalisation (cached per operator).  Top eigenpairs are
+// deflated while |p(lambda_k)| exceeds 4x the largest |p| on [0, 1.05
+// lambda_{k+1}] (the reference's fit leaves that range), so the Clenshaw
+// recurrence only ever sees a spectrum on which p is bounded.
+static int plan_mixed(ngw_session *s, PolyPlan &pp, double lo_in, double hi_in) {
+  const int tda = pp.tamm_d;
+  if (hi_in > lo_in) {
+    pp.c0 = 0.5 * (hi_in + lo_in);
+    pp.c1 = 0.5 * (hi_in - lo_in);
+    pp.kdef = 0;
+  } else {
+    if (s->eig_tda != tda) NGW_TRY(compute_top_eigs(s, tda, 48, 160));
+    const std::vector<double> &r = s->eig_vals, &res = s->eig_res;
+    const int mm = (int)r.size();
+    int k = 0;
+    if (!tda) {
+      while (k < std::min(s->eig_k, mm - 1)) {
+        const double nxt = 1.05 * r[k + 1];
+        double pmax = 0.0;
+        for (int i = 0; i <= 2000; ++i) pmax = std::max(pmax, std::fabs(poly_eval(pp.poly, nxt * i / 2000.0)));
+        if (std::fabs(poly_eval(pp.poly, r[k])) > 4.0 * pmax && res[k] < 1e-6 * std::fabs(r[0])) ++k;
+        else break;
+      }
     }
-  *out = tridiag_max_eig(ha, hb, kk);
-  return NGW_OK;
-}
-
-// cached spectral interval of the session's operator for the Chebyshev form
-static int spectral_interval(ngw_session *s, int tamm_d, double *lo, double *hi) {
-  double &cache = tamm_d ? s->lmax_tda : s->lmax;
-  if (!(cache > 0.0)) NGW_TRY(estimate_lambda_max(s, tamm_d, &cache));
-  *lo = 0.0;
-  *hi = cache * 1.02;
+    const double top = (k < mm) ? r[k] + res[k] : 0.0;
+    const double hi = std::max(1.05 * top, 1e-12);
+    pp.c0 = 0.5 * hi;
+    pp.c1 = 0.5 * hi;
+    pp.kdef = k;
+  }
+  if (!tda) {
+    pp.cheb.resize(pp.npoly + 1);
+    monomial_to_chebyshev(pp.poly.data(), pp.npoly, pp.c0 - pp.c1, pp.c0 + pp.c1, pp.cheb.data());
+  }
+  if (!s->mixed || mixed_kdef(s) != pp.kdef) NGW_TRY(mixed_build_operator(s, pp.kdef, tda));
+  std::vector<double> pv(pp.kdef);
+  for (int j = 0; j < pp.kdef; ++j) pv[j] = tda ? s->eig_vals[j] : poly_eval(pp.poly, s->eig_vals[j]);
+  NGW_TRY(mixed_set_deflation_values(s, pv.data()));
   return NGW_OK;
 }
 
@@ -294,19 +263,9 @@ static int make_plan(ngw_session *s, PolyPlan &pp, const double *poly, int npoly
     }
   } else {
     pp.npoly = 1;
+    pp.poly = {1.0, 0.0};
   }
-  if (s->precision == NGW_PREC_MIXED) {
-    if (!(hi > lo)) {
-      set_error("mixed precision needs a spectral interval hi > lo (got %g, %g)", lo, hi);
-      return NGW_ERR_ARG;
-    }
-    pp.c0 = 0.5 * (hi + lo);
-    pp.c1 = 0.5 * (hi - lo);
-    if (!tamm_d) {
-      pp.cheb.resize(npoly + 1);
-      monomial_to_chebyshev(poly, npoly, lo, hi, pp.cheb.data());
-    }
-  }
+  if (s->precision == NGW_PREC_MIXED) NGW_TRY(plan_mixed(s, pp, lo, hi));
   return NGW_OK;
 }
 
@@ -365,7 +324,7 @@ void ngw_session_destroy(ngw_session *s) {
   mixed_free(s);
   for (auto &b : s->scratch)
     if (b.p) cudaFree(b.p);
-  void *ptrs[] = {s->d_psi, s->d_M, s->d_Mxc, s->d_cvpair, s->d_sqrtR, s->d_C, s->d_status};
+  void *ptrs[] = {s->d_psi, s->d_M, s->d_Mxc, s->d_cvpair, s->d_sqrtR, s->d_C, s->d_status, s->eig_U};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->cublas) cublasDestroy(s->cublas);
@@ -384,9 +343,6 @@ int ngw_set_precision(ngw_session *s, int mode) {
   }
   NGW_CUDA(cudaSetDevice(s->device));
   s->precision = mode;
-  if (mode == NGW_PREC_MIXED && s->have_isdf && s->have_pairs) {
-    NGW_TRY(need_op(s));
-  }
   return NGW_OK;
 }
 
@@ -410,7 +366,7 @@ int ngw_set_isdf(ngw_session *s, int n_isdf, int nmem, const double *psi_intp, c
   if (s->d_C) dfree(s, s->d_C, (size_t)s->n_isdf * s->ncv * 8);
   s->d_psi = s->d_M = s->d_Mxc = s->d_C = nullptr;
   s->have_C = false;
-  s->lmax = s->lmax_tda = 0.0;
+  s->eig_tda = -1;
   s->n_isdf = n_isdf;
   s->nmem = nmem;
   NGW_TRY(dalloc(s, (void **)&s->d_psi, (size_t)n_isdf * nmem * 8));
@@ -455,7 +411,7 @@ int ngw_set_pairs(ngw_session *s, int ncv, const int *cvpair, const double *sqrt
   if (s->d_C) dfree(s, s->d_C, (size_t)s->n_isdf * s->ncv * 8);
   s->d_C = nullptr;
   s->have_C = false;
-  s->lmax = s->lmax_tda = 0.0;
+  s->eig_tda = -1;
   s->ncv = ncv;
   NGW_TRY(dalloc(s, (void **)&s->d_cvpair, (size_t)2 * ncv * 4));
   NGW_TRY(dalloc(s, (void **)&s->d_sqrtR, (size_t)ncv * 8));
@@ -484,10 +440,13 @@ int ngw_matvec_isdf(ngw_session *s, const double *vec, double *hvec, int ld, int
   NGW_CUDA(cudaMemcpy2DAsync(din, (size_t)ncv * 8, vec, (size_t)ld * 8, (size_t)ncv * 8, nb,
                              cudaMemcpyHostToDevice, s->stream));
   if (s->precision == NGW_PREC_MIXED) {
-    // a single matvec in mixed precision: Chebyshev series "x" on [0, 2]
+    // one matvec in mixed precision: the degree-1 series p(x) = x
+    PolyPlan pp;
+    const double px[2] = {1.0, 0.0};
+    NGW_TRY(make_plan(s, pp, px, 1, tamm_d ? 1 : 0, 0.0, 0.0));
     NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
-    const double g[2] = {1.0, 1.0};
-    NGW_TRY(mixed_poly_apply(s, nb, din, ncv, g, 1, 1.0, 1.0, tamm_d ? 1 : 0, dout));
+    const double g[2] = {pp.c0, pp.c1};
+    NGW_TRY(mixed_poly_apply(s, nb, din, ncv, g, 1, pp.c0, pp.c1, tamm_d ? 1 : 0, dout));
   } else {
     launch_scale_rows(s->d_sqrtR, din, ncv, hs, ncv, ncv, nb, tamm_d, s->stream);
     NGW_TRY(matvec_f64_dev(s, nb, hs, dout, din, tamm_d, 0, 0.0, 0.0, nullptr));
@@ -534,10 +493,7 @@ int ngw_lanczos_spectra_isdf(ngw_session *s, const double *v0, const double *v0_
   NGW_CUDA(cudaSetDevice(s->device));
   const int ncv = s->ncv, nb = blksz;
   PolyPlan pp;
-  // mixed precision: Chebyshev interval [0, 1.02 lambda_max] of the operator
-  double lo = 0.0, hi = 0.0;
-  if (s->precision == NGW_PREC_MIXED) NGW_TRY(spectral_interval(s, tamm_d, &lo, &hi));
-  NGW_TRY(make_plan(s, pp, polynomial, npoly, tamm_d, lo, hi));
+  NGW_TRY(make_plan(s, pp, polynomial, npoly, tamm_d, 0.0, 0.0));
   double *dv0, *V, *W, *hs, *tmp, *a, *b, *dzz, *dspec, *dnorm;
   NGW_TRY(scratch(s, SL_IN, (size_t)ncv * nb * 8, (void **)&dv0));
   NGW_TRY(scratch(s, SL_VEC, (size_t)ncv * nb * 8, (void **)&V));
@@ -646,7 +602,6 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
   // positive definite, and the interval must contain its whole spectrum for the
   // Clenshaw recurrence to be stable (the reference's fit range need not).
   double lo = p->cheb_lo, hi = p->cheb_hi;
-  if (s->precision == NGW_PREC_MIXED && !(hi > lo)) NGW_TRY(spectral_interval(s, tamm_d, &lo, &hi));
   PolyPlan pp;
   NGW_TRY(make_plan(s, pp, p->polynomial, p->npoly, tamm_d, lo, hi));
   // chain blocking: whole QP states per block

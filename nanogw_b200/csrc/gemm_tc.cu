@@ -42,9 +42,8 @@ struct EpiParams {
   // EPI_SPLIT: D(m, n) -> out_hi/lo[n * ldo + m]
   bf16 *out_hi, *out_lo;
   int ldo;
-  // split-K
+  // split-K partials (EPI_SPLIT with nsplit > 1), reduced by k_splitk_reduce
   float *ws;
-  int *counters;
   // EPI_CLENSHAW: rows m = pair index, cols n = chain
   const double *s;       // sqrtR (Mv)
   const float *x;        // b_{k+1}  [n * ldx + m]
@@ -70,8 +69,12 @@ __device__ __forceinline__ void split_bf16(float v, bf16 &hi, bf16 &lo) {
   lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
 
+constexpr int NTHREADS = 256;
+
+// Epilogue loads for one 16-column chunk, issued before any arithmetic so the
+// global-memory latencies overlap.
 template <int BN, int STAGES>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(NTHREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
               const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
               GemmArgs ga, EpiParams ep, int *status) {
@@ -80,6 +83,8 @@ __global__ void __launch_bounds__(128, 1)
   constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
   constexpr uint32_t TMEM_COLS = (BN <= 32) ? 32 : (BN <= 64) ? 64 : (BN <= 128) ? 128 : 256;
   constexpr uint32_t IDESC = tc::idesc_bf16_f32(BM, BN);
+  constexpr int NCH = BN / 16;             // 16-column chunks
+  constexpr int NCH0 = (NCH + 1) / 2;      // chunks of warpgroup 0
 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -88,7 +93,6 @@ __global__ void __launch_bounds__(128, 1)
   __shared__ __align__(8) uint64_t empty_bar[STAGES];
   __shared__ __align__(8) uint64_t done_bar;
   __shared__ uint32_t tmem_base_sh;
-  __shared__ int last_flag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
@@ -119,7 +123,7 @@ __global__ void __launch_bounds__(128, 1)
   const uint32_t tmem_d = tmem_base_sh;
 
   if (warp == 0 && lane == 0) {
-    // ---- TMA producer ----
+    // ---- TMA producer: k-blocks of the concatenated segments ----
     for (int i = 0; i < nkb; ++i) {
       const int s = i % STAGES;
       if (i >= STAGES) {
@@ -128,7 +132,7 @@ __global__ void __launch_bounds__(128, 1)
       const int kbg = kb_begin + i;
       const int seg = kbg / ga.num_kb;
       const int kb = kbg - seg * ga.num_kb;
-      const CUtensorMap *ta = (seg == 2) ? &tA_lo : &tA_hi;
+      const CUtensorMap *ta = (seg == 2) ? &tA_lo : &tA_hi;   // (hi,hi) (hi,lo) (lo,hi)
       const CUtensorMap *tb = (seg == 1) ? &tB_lo : &tB_hi;
       const uint32_t bar = tc::smem_u32(&full_bar[s]);
       const uint32_t sa = tc::smem_u32(smem + s * STAGE_BYTES);
@@ -137,14 +141,10 @@ __global__ void __launch_bounds__(128, 1)
       tc::tma_load_2d(sa + A_BYTES, tb, bar, kb * BK, n0);
     }
   } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer ----
-    bool ok = true;
-    for (int i = 0; i < nkb && ok; ++i) {
+    // ---- MMA issuer (single thread) ----
+    for (int i = 0; i < nkb; ++i) {
       const int s = i % STAGES;
-      if (!tc::mbar_wait(tc::smem_u32(&full_bar[s]), (i / STAGES) & 1, status)) {
-        ok = false;
-        break;
-      }
+      if (!tc::mbar_wait(tc::smem_u32(&full_bar[s]), (i / STAGES) & 1, status)) break;
       tc::tc_fence_after();
       const uint32_t sa = tc::smem_u32(smem + s * STAGE_BYTES);
       const uint32_t sb = sa + A_BYTES;
@@ -160,100 +160,87 @@ __global__ void __launch_bounds__(128, 1)
   }
   __syncwarp();
 
-  // ---- epilogue: all four warps, thread <-> accumulator row ----
-  const bool have = tc::mbar_wait(tc::smem_u32(&done_bar), 0, status);
+  // ---- epilogue: 8 warps; warp w reads TMEM lanes 32*(w%4).., warpgroup w/4
+  // takes one half of the 16-column chunks ----
+  const bool have = tc::mbar_wait(tc::smem_u32(&done_bar), 0, status) && nkb > 0;
   tc::tc_fence_after();
-  const int mloc = warp * 32 + lane;
+  const int wl = warp & 3, wg = warp >> 2;
+  const int mloc = wl * 32 + lane;
   const int m = m0 + mloc;
-  const uint32_t trow = tmem_d + ((uint32_t)(warp * 32) << 16);
+  const uint32_t trow = tmem_d + ((uint32_t)(wl * 32) << 16);
+  const int ch_begin = wg == 0 ? 0 : NCH0;
+  const int ch_end = wg == 0 ? NCH0 : NCH;
 
-  if (ep.kind == EPI_SPLIT && ga.nsplit > 1) {
-    const int tiles_m = gridDim.x;
-    const int tile = blockIdx.y * tiles_m + blockIdx.x;
-    float *wsl = ep.ws + ((size_t)tile * ga.nsplit + split) * (size_t)(BN * BM);
-    for (int c = 0; c < BN; c += 16) {
+  if (ep.kind == EPI_SPLIT) {
+    const bool partial = ga.nsplit > 1;
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+    float *wsl = partial ? ep.ws + ((size_t)tile * ga.nsplit + split) * (size_t)(BN * BM) : nullptr;
+    for (int ch = ch_begin; ch < ch_end; ++ch) {
+      const int c = ch * 16;
       float v[16];
-      if (have && nkb > 0) {
+      if (have) {
         tc::tmem_ld16(trow + c, v);
       } else {
 #pragma unroll
         for (int j = 0; j < 16; ++j) v[j] = 0.f;
       }
+      if (partial) {
 #pragma unroll
-      for (int j = 0; j < 16; ++j) wsl[(size_t)(c + j) * BM + mloc] = v[j];
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int old = atomicAdd(&ep.counters[tile], 1);
-      last_flag = (old == ga.nsplit - 1);
-    }
-    __syncthreads();
-    if (last_flag) {
-      __threadfence();
-      const float *base = ep.ws + (size_t)tile * ga.nsplit * (size_t)(BN * BM);
-      for (int c = 0; c < BN; ++c) {
-        const int n = n0 + c;
-        float acc = 0.f;
-        for (int sp = 0; sp < ga.nsplit; ++sp)
-          acc += __ldcg(base + (size_t)sp * (BN * BM) + (size_t)c * BM + mloc);
-        if (m < ep.Mv && n < ep.Nv) {
-          bf16 hi, lo;
-          split_bf16(acc, hi, lo);
-          ep.out_hi[(size_t)n * ep.ldo + m] = hi;
-          ep.out_lo[(size_t)n * ep.ldo + m] = lo;
-        }
-      }
-      if (threadIdx.x == 0) ep.counters[tile] = 0;
-    }
-  } else if (ep.kind == EPI_SPLIT) {
-    for (int c = 0; c < BN; c += 16) {
-      float v[16];
-      if (have && nkb > 0) {
-        tc::tmem_ld16(trow + c, v);
-      } else {
+        for (int j = 0; j < 16; ++j) wsl[(size_t)(c + j) * BM + mloc] = v[j];
+      } else if (m < ep.Mv) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = 0.f;
-      }
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int n = n0 + c + j;
-        if (m < ep.Mv && n < ep.Nv) {
-          bf16 hi, lo;
-          split_bf16(v[j], hi, lo);
-          ep.out_hi[(size_t)n * ep.ldo + m] = hi;
-          ep.out_lo[(size_t)n * ep.ldo + m] = lo;
+        for (int j = 0; j < 16; ++j) {
+          const int n = n0 + c + j;
+          if (n < ep.Nv) {
+            bf16 hi, lo;
+            split_bf16(v[j], hi, lo);
+            ep.out_hi[(size_t)n * ep.ldo + m] = hi;
+            ep.out_lo[(size_t)n * ep.ldo + m] = lo;
+          }
         }
       }
     }
   } else {
-    // EPI_CLENSHAW
+    // EPI_CLENSHAW: y = R^2 x + 4 R^1/2 z (TDA: R x + 2 z);
+    // out = gamma v + alpha (y - c0 x) - beta b2; split((R^1/2 or 1) out)
     const bool mv = m < ep.Mv;
     const double si = mv ? ep.s[m] : 0.0;
     const double s2 = si * si;
-    for (int c = 0; c < BN; c += 16) {
-      float v[16];
-      if (have && nkb > 0) {
-        tc::tmem_ld16(trow + c, v);
+    const double sc = ep.tda ? 1.0 : si;
+    for (int ch = ch_begin; ch < ch_end; ++ch) {
+      const int c = ch * 16;
+      float z[16];
+      if (have) {
+        tc::tmem_ld16(trow + c, z);
       } else {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = 0.f;
+        for (int j = 0; j < 16; ++j) z[j] = 0.f;
       }
-#pragma unroll 4
+      if (!mv) continue;
+      const int nbase = n0 + c;
+      const int nj = min(16, ep.Nv - nbase);
+      if (nj <= 0) continue;
+      float xv[16], b2v[16];
+      double vv[16];
+#pragma unroll
       for (int j = 0; j < 16; ++j) {
-        const int n = n0 + c + j;
-        if (!mv || n >= ep.Nv) continue;
-        const double x = (double)ep.x[(size_t)n * ep.ldx + m];
-        const double z = (double)v[j];
-        const double y = ep.tda ? (s2 * x + 2.0 * z) : (s2 * s2 * x + 4.0 * si * z);
-        double o = ep.alpha * (y - ep.c0 * x);
-        if (ep.v) o += ep.gamma * ep.v[(size_t)n * ep.ldv + m];
-        if (ep.b2) o -= ep.beta * (double)ep.b2[(size_t)n * ep.ldx + m];
+        const size_t o = (size_t)(nbase + j) * ep.ldx + m;
+        xv[j] = (j < nj) ? __ldg(ep.x + o) : 0.f;
+        b2v[j] = (j < nj && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
+        vv[j] = (j < nj && ep.v) ? __ldg(ep.v + (size_t)(nbase + j) * ep.ldv + m) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        if (j >= nj) break;
+        const int n = nbase + j;
+        const double x = (double)xv[j];
+        const double y = ep.tda ? (s2 * x + 2.0 * (double)z[j]) : (s2 * s2 * x + 4.0 * si * (double)z[j]);
+        const double o = ep.gamma * vv[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
         if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = (float)o;
         if (ep.out64) ep.out64[(size_t)n * ep.ldv + m] = o;
         if (ep.s_hi) {
           bf16 hi, lo;
-          split_bf16((float)(ep.tda ? o : si * o), hi, lo);
+          split_bf16((float)(sc * o), hi, lo);
           ep.s_hi[(size_t)n * ep.lds + m] = hi;
           ep.s_lo[(size_t)n * ep.lds + m] = lo;
         }
@@ -266,6 +253,27 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 2) {
     tc::tc_fence_after();
     tc::tmem_dealloc(tmem_d, TMEM_COLS);
+  }
+}
+
+// Deterministic split-K reduction: D(m, n) = sum_s partial_s(m, n) in split
+// order, written as the split-BF16 pair.  One thread per output element,
+// consecutive threads on consecutive rows (coalesced partial reads).
+__global__ void k_splitk_reduce(const float *__restrict__ ws, int nsplit, int BN, int tiles_m,
+                                int Mv, int Nv, bf16 *__restrict__ out_hi, bf16 *__restrict__ out_lo,
+                                int ldo) {
+  const size_t total = (size_t)Mv * Nv;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int n = (int)(idx / Mv), m = (int)(idx % Mv);
+    const int tile = (n / BN) * tiles_m + m / BM;
+    const float *p = ws + (size_t)tile * nsplit * (size_t)(BN * BM) + (size_t)(n % BN) * BM + (m % BM);
+    float acc = 0.f;
+    for (int s = 0; s < nsplit; ++s) acc += __ldcg(p + (size_t)s * (BN * BM));
+    bf16 hi, lo;
+    split_bf16(acc, hi, lo);
+    out_hi[(size_t)n * ldo + m] = hi;
+    out_lo[(size_t)n * ldo + m] = lo;
   }
 }
 
@@ -322,7 +330,7 @@ static int launch_tc(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUt
     attr = true;
   }
   dim3 grid(tiles_m, tiles_n, ga.nsplit);
-  k_tc_gemm<BN, STAGES><<<grid, 128, smem, st>>>(a_hi, a_lo, b_hi, b_lo, ga, ep, status);
+  k_tc_gemm<BN, STAGES><<<grid, NTHREADS, smem, st>>>(a_hi, a_lo, b_hi, b_lo, ga, ep, status);
   NGW_CUDA(cudaGetLastError());
   return NGW_OK;
 }
@@ -365,24 +373,41 @@ __global__ void k_split_transpose(const double *__restrict__ C, int n_isdf, int 
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int mu = mu0 + r, cv = cv0 + threadIdx.x;
     if (mu < n_isdf && cv < ncv) {
-      bf16 h, l;
       const double x = tile[threadIdx.x][r];
-      h = __double2bfloat16(x);
-      l = __double2bfloat16(x - (double)__bfloat162float(h));
+      const bf16 h = __double2bfloat16(x);
+      const bf16 l = __double2bfloat16(x - (double)__bfloat162float(h));
       hi[(size_t)mu * ldk + cv] = h;
       lo[(size_t)mu * ldk + cv] = l;
     }
   }
 }
 
-// D (n_isdf, ncv) FP64 column-major -> A3[cv][mu] hi/lo (row length ldk)
+// rows (ncv, ncol) FP64 column-major scaled per pair by 1/(f*s) -> out rows
+// [row0 + j][cv] (A1 extension, row length ldk)
+__global__ void k_split_cols_to_rows(const double *__restrict__ X, int ncv, int ncol,
+                                     const double *__restrict__ s, double f, bf16 *__restrict__ hi,
+                                     bf16 *__restrict__ lo, int ldk, int row0) {
+  const int j = blockIdx.y;
+  for (int cv = blockIdx.x * blockDim.x + threadIdx.x; cv < ncv; cv += gridDim.x * blockDim.x) {
+    const double x = X[(size_t)j * ncv + cv] / (f * (s ? s[cv] : 1.0));
+    const bf16 h = __double2bfloat16(x);
+    const bf16 l = __double2bfloat16(x - (double)__bfloat162float(h));
+    hi[(size_t)(row0 + j) * ldk + cv] = h;
+    lo[(size_t)(row0 + j) * ldk + cv] = l;
+  }
+}
+
+// D (n_isdf, ncv) FP64 column-major -> A3[cv][mu] hi/lo (row length ldk);
+// extra columns mu = n_isdf + j hold -U(cv, j) / (4 s(cv))
 __global__ void k_split_rows(const double *__restrict__ D, int n_isdf, int ncv,
+                             const double *__restrict__ U, int k, const double *__restrict__ s,
                              bf16 *__restrict__ hi, bf16 *__restrict__ lo, int ldk) {
   const int cv = blockIdx.y;
-  for (int mu = blockIdx.x * blockDim.x + threadIdx.x; mu < n_isdf; mu += gridDim.x * blockDim.x) {
-    const double x = D[(size_t)cv * n_isdf + mu];
-    bf16 h = __double2bfloat16(x);
-    bf16 l = __double2bfloat16(x - (double)__bfloat162float(h));
+  for (int mu = blockIdx.x * blockDim.x + threadIdx.x; mu < n_isdf + k; mu += gridDim.x * blockDim.x) {
+    const double x = (mu < n_isdf) ? D[(size_t)cv * n_isdf + mu]
+                                   : -U[(size_t)(mu - n_isdf) * ncv + cv] / (4.0 * s[cv]);
+    const bf16 h = __double2bfloat16(x);
+    const bf16 l = __double2bfloat16(x - (double)__bfloat162float(h));
     hi[(size_t)cv * ldk + mu] = h;
     lo[(size_t)cv * ldk + mu] = l;
   }
@@ -405,61 +430,69 @@ __global__ void k_cheb_start(const double *__restrict__ v, int ldv, const double
 }
 
 struct MixedOperator {
-  int n_isdf = 0, ncv = 0;
-  int mu_pad = 0;     // rows of A1 (multiple of 128)
-  int mu_k = 0;       // K of GEMM2 (multiple of 64)
+  int n_isdf = 0, ncv = 0, kdef = 0, tda = 0;
+  int mu_pad = 0;     // rows of A1 = n_isdf + kdef, padded to 128
+  int mu_k = 0;       // K of GEMM2 = n_isdf + kdef, padded to 64
   int cv_pad = 0;     // K of GEMM1 / rows of A3 (multiple of 128)
   bf16 *A1_hi = nullptr, *A1_lo = nullptr, *A3_hi = nullptr, *A3_lo = nullptr;
   CUtensorMap tA1hi, tA1lo, tA3hi, tA3lo;
   size_t op_bytes = 0;
+  double *Up = nullptr;      // (ncv, kdef) U p(Lambda) for the current polynomial
   // chain buffers
   int nb_cap = 0, nb_pad = 0, BN1 = 128, BN2 = 128, split1 = 1;
   bf16 *S_hi = nullptr, *S_lo = nullptr, *T_hi = nullptr, *T_lo = nullptr;
   CUtensorMap tShi, tSlo, tThi, tTlo;
   float *bb[3] = {nullptr, nullptr, nullptr};
+  double *vperp = nullptr, *xo = nullptr;
   float *ws = nullptr;
-  int *counters = nullptr;
   size_t buf_bytes = 0;
 };
 
 static int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
-void mixed_free(ngw_session *s) {
-  MixedOperator *op = s->mixed;
-  if (!op) return;
-  void *ptrs[] = {op->A1_hi, op->A1_lo, op->A3_hi, op->A3_lo, op->S_hi, op->S_lo, op->T_hi,
-                  op->T_lo,  op->bb[0], op->bb[1], op->bb[2], op->ws,    op->counters};
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
-  s->bytes -= op->op_bytes + op->buf_bytes;
-  delete op;
-  s->mixed = nullptr;
-}
-
 static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
   void *ptrs[] = {op->S_hi, op->S_lo, op->T_hi, op->T_lo, op->bb[0], op->bb[1], op->bb[2],
-                  op->ws,   op->counters};
+                  op->ws,   op->vperp, op->xo};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   op->S_hi = op->S_lo = op->T_hi = op->T_lo = nullptr;
   op->bb[0] = op->bb[1] = op->bb[2] = nullptr;
   op->ws = nullptr;
-  op->counters = nullptr;
+  op->vperp = op->xo = nullptr;
   s->bytes -= op->buf_bytes;
   op->buf_bytes = 0;
   op->nb_cap = 0;
 }
 
-// Build A1 = split(C^T-layout) and A3 = split((M C) layout) from the FP64
-// pair products already in the session.
-int mixed_build_operator(ngw_session *s) {
+void mixed_free(ngw_session *s) {
+  MixedOperator *op = s->mixed;
+  if (!op) return;
+  free_chain_buffers(s, op);
+  void *ptrs[] = {op->A1_hi, op->A1_lo, op->A3_hi, op->A3_lo, op->Up};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  s->bytes -= op->op_bytes;
+  delete op;
+  s->mixed = nullptr;
+}
+
+int mixed_kdef(ngw_session *s) { return s->mixed ? s->mixed->kdef : -1; }
+
+int matvec_f64_dev_pub(ngw_session *s, int nb, double *hs, double *y, int tamm_d);
+
+// Build A1 = [C_isdf ; G^T] (G = (C U) / R^1/2, k rows) and
+// A3 = [(M C_isdf)^T | -U / (4 R^1/2)] in split-BF16 from the FP64 operator;
+// U = the first kdef Ritz vectors in s->eig_U (kdef = 0: no deflation).
+int mixed_build_operator(ngw_session *s, int kdef, int tda) {
   mixed_free(s);
   MixedOperator *op = new MixedOperator();
   s->mixed = op;
   op->n_isdf = s->n_isdf;
   op->ncv = s->ncv;
-  op->mu_pad = round_up(s->n_isdf, BM);
-  op->mu_k = round_up(s->n_isdf, BK);
+  op->kdef = kdef;
+  op->tda = tda;
+  op->mu_pad = round_up(s->n_isdf + kdef, BM);
+  op->mu_k = round_up(s->n_isdf + kdef, BK);
   op->cv_pad = round_up(s->ncv, BM);
   const size_t a1 = (size_t)op->mu_pad * op->cv_pad * sizeof(bf16);
   const size_t a3 = (size_t)op->cv_pad * op->mu_k * sizeof(bf16);
@@ -468,6 +501,10 @@ int mixed_build_operator(ngw_session *s) {
   NGW_CUDA(cudaMalloc(&op->A3_hi, a3));
   NGW_CUDA(cudaMalloc(&op->A3_lo, a3));
   op->op_bytes = 2 * (a1 + a3);
+  if (kdef > 0) {
+    NGW_CUDA(cudaMalloc(&op->Up, (size_t)s->ncv * kdef * 8));
+    op->op_bytes += (size_t)s->ncv * kdef * 8;
+  }
   s->bytes += op->op_bytes;
   cudaStream_t st = s->stream;
   NGW_CUDA(cudaMemsetAsync(op->A1_hi, 0, a1, st));
@@ -480,10 +517,30 @@ int mixed_build_operator(ngw_session *s) {
                                                     op->A1_lo, op->cv_pad);
     NGW_CUDA(cudaGetLastError());
   }
-  // D = M * C (FP64, cuBLAS), then split into A3[cv][mu]
+  const double one = 1.0, zero = 0.0;
+  if (kdef > 0) {
+    // G = (C U) / s  in FP64: C applied to the Ritz vectors with the FP64 matvec
+    double *hs = nullptr, *CU = nullptr;
+    NGW_CUDA(cudaMalloc(&hs, (size_t)s->ncv * kdef * 8));
+    NGW_CUDA(cudaMalloc(&CU, (size_t)s->ncv * kdef * 8));
+    launch_scale_rows(s->d_sqrtR, s->eig_U, s->ncv, hs, s->ncv, s->ncv, kdef, tda, st);
+    int rc = matvec_f64_dev_pub(s, kdef, hs, CU, tda);
+    if (rc == NGW_OK) {
+      int bx = std::min(64, (s->ncv + 255) / 256);
+      // TDA: the pair scaling is 1 (A x uses x, not R^1/2 x)
+      k_split_cols_to_rows<<<dim3(bx, kdef), 256, 0, st>>>(CU, s->ncv, kdef, tda ? nullptr : s->d_sqrtR,
+                                                          1.0, op->A1_hi, op->A1_lo, op->cv_pad,
+                                                          s->n_isdf);
+    }
+    NGW_CUDA(cudaStreamSynchronize(st));
+    cudaFree(hs);
+    cudaFree(CU);
+    NGW_TRY(rc);
+    NGW_CUDA(cudaGetLastError());
+  }
+  // D = M * C (FP64, cuBLAS), then split into A3[cv][mu] with the -U/(4s) columns
   double *D = nullptr;
   NGW_CUDA(cudaMalloc(&D, (size_t)s->n_isdf * s->ncv * sizeof(double)));
-  const double one = 1.0, zero = 0.0;
   cublasStatus_t cst = cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, s->n_isdf, s->ncv,
                                    s->n_isdf, &one, s->d_M, s->n_isdf, s->d_C, s->n_isdf, &zero,
                                    D, s->n_isdf);
@@ -493,9 +550,9 @@ int mixed_build_operator(ngw_session *s) {
     return NGW_ERR_CUDA;
   }
   {
-    int bx = (s->n_isdf + 127) / 128;
-    k_split_rows<<<dim3(bx, s->ncv), 128, 0, st>>>(D, s->n_isdf, s->ncv, op->A3_hi, op->A3_lo,
-                                                   op->mu_k);
+    int bx = (s->n_isdf + kdef + 127) / 128;
+    k_split_rows<<<dim3(bx, s->ncv), 128, 0, st>>>(D, s->n_isdf, s->ncv, s->eig_U, kdef,
+                                                   s->d_sqrtR, op->A3_hi, op->A3_lo, op->mu_k);
     NGW_CUDA(cudaGetLastError());
   }
   NGW_CUDA(cudaStreamSynchronize(st));
@@ -504,6 +561,19 @@ int mixed_build_operator(ngw_session *s) {
   NGW_TRY(make_tmap(&op->tA1lo, op->A1_lo, op->mu_pad, op->cv_pad, BM));
   NGW_TRY(make_tmap(&op->tA3hi, op->A3_hi, op->cv_pad, op->mu_k, BM));
   NGW_TRY(make_tmap(&op->tA3lo, op->A3_lo, op->cv_pad, op->mu_k, BM));
+  return NGW_OK;
+}
+
+// Up = U diag(pvals) for the current polynomial (device, ncv x kdef)
+int mixed_set_deflation_values(ngw_session *s, const double *pvals) {
+  MixedOperator *op = s->mixed;
+  if (!op || op->kdef == 0) return NGW_OK;
+  NGW_CUDA(cudaMemcpyAsync(op->Up, s->eig_U, (size_t)s->ncv * op->kdef * 8, cudaMemcpyDeviceToDevice,
+                           s->stream));
+  for (int j = 0; j < op->kdef; ++j) {
+    const double pv = pvals[j];
+    NGW_CUBLAS(cublasDscal(s->cublas, s->ncv, &pv, op->Up + (size_t)j * s->ncv, 1));
+  }
   return NGW_OK;
 }
 
@@ -520,6 +590,23 @@ static int pick_bn(int nb) {
   return best;
 }
 
+// split-K factor for GEMM1: fill the 148 SMs with at least 4 k-blocks per CTA
+static int pick_split(int tiles, int total_kb) {
+  int best = 1;
+  double best_eff = 0.0;
+  for (int sp = 1; sp <= 16; ++sp) {
+    if (total_kb / sp < 4) break;
+    const int ctas = tiles * sp;
+    const int waves = (ctas + 147) / 148;
+    const double eff = (double)ctas / (148.0 * waves);
+    if (eff > best_eff + 0.02) {
+      best_eff = eff;
+      best = sp;
+    }
+  }
+  return best;
+}
+
 int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
   MixedOperator *op = s->mixed;
   if (!op) {
@@ -530,14 +617,10 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
   if (bn2 <= 0) bn2 = pick_bn(nb);
   const int tiles_m1 = op->mu_pad / BM;
   const int tiles_n1 = (nb + bn1 - 1) / bn1;
-  if (split1 <= 0) {
-    const int total_kb = 3 * (op->cv_pad / BK);
-    split1 = 1;
-    while (tiles_m1 * tiles_n1 * split1 * 2 <= 148 && split1 * 2 * 4 <= total_kb) split1 *= 2;
-  }
-  const int nbp = round_up(nb, 256);
+  if (split1 <= 0) split1 = pick_split(tiles_m1 * tiles_n1, 3 * (op->cv_pad / BK));
   if (op->nb_cap >= nb && op->BN1 == bn1 && op->BN2 == bn2 && op->split1 == split1) return NGW_OK;
   free_chain_buffers(s, op);
+  const int nbp = round_up(nb, 256);
   op->BN1 = bn1;
   op->BN2 = bn2;
   op->split1 = split1;
@@ -545,22 +628,24 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
   const size_t sbytes = (size_t)nbp * op->cv_pad * sizeof(bf16);
   const size_t tbytes = (size_t)nbp * op->mu_k * sizeof(bf16);
   const size_t bbytes = (size_t)nbp * op->cv_pad * sizeof(float);
-  const size_t wsbytes = (size_t)tiles_m1 * ((nbp + bn1 - 1) / bn1) * split1 * bn1 * BM * sizeof(float);
-  const size_t cbytes = (size_t)tiles_m1 * ((nbp + bn1 - 1) / bn1) * sizeof(int);
+  const size_t vbytes = (size_t)nbp * s->ncv * sizeof(double);
+  const size_t xbytes = (size_t)nbp * std::max(op->kdef, 1) * sizeof(double);
+  const size_t wsbytes =
+      split1 > 1 ? (size_t)tiles_m1 * ((nbp + bn1 - 1) / bn1) * split1 * bn1 * BM * sizeof(float) : 16;
   NGW_CUDA(cudaMalloc(&op->S_hi, sbytes));
   NGW_CUDA(cudaMalloc(&op->S_lo, sbytes));
   NGW_CUDA(cudaMalloc(&op->T_hi, tbytes));
   NGW_CUDA(cudaMalloc(&op->T_lo, tbytes));
   for (int i = 0; i < 3; ++i) NGW_CUDA(cudaMalloc(&op->bb[i], bbytes));
+  NGW_CUDA(cudaMalloc(&op->vperp, vbytes));
+  NGW_CUDA(cudaMalloc(&op->xo, xbytes));
   NGW_CUDA(cudaMalloc(&op->ws, wsbytes));
-  NGW_CUDA(cudaMalloc(&op->counters, cbytes));
-  op->buf_bytes = 2 * sbytes + 2 * tbytes + 3 * bbytes + wsbytes + cbytes;
+  op->buf_bytes = 2 * sbytes + 2 * tbytes + 3 * bbytes + vbytes + xbytes + wsbytes;
   s->bytes += op->buf_bytes;
   NGW_CUDA(cudaMemsetAsync(op->S_hi, 0, sbytes, s->stream));
   NGW_CUDA(cudaMemsetAsync(op->S_lo, 0, sbytes, s->stream));
   NGW_CUDA(cudaMemsetAsync(op->T_hi, 0, tbytes, s->stream));
   NGW_CUDA(cudaMemsetAsync(op->T_lo, 0, tbytes, s->stream));
-  NGW_CUDA(cudaMemsetAsync(op->counters, 0, cbytes, s->stream));
   NGW_TRY(make_tmap(&op->tShi, op->S_hi, nbp, op->cv_pad, bn1));
   NGW_TRY(make_tmap(&op->tSlo, op->S_lo, nbp, op->cv_pad, bn1));
   NGW_TRY(make_tmap(&op->tThi, op->T_hi, nbp, op->mu_k, bn2));
@@ -569,7 +654,7 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
   return NGW_OK;
 }
 
-// One GEMM1 (T = C_isdf S) with split output into T_hi/T_lo.
+// One GEMM1 ([T; q] = A1 S) with split output into T_hi/T_lo.
 static int run_gemm1(ngw_session *s, int nb) {
   MixedOperator *op = s->mixed;
   GemmArgs ga;
@@ -579,17 +664,24 @@ static int run_gemm1(ngw_session *s, int nb) {
   EpiParams ep;
   std::memset(&ep, 0, sizeof(ep));
   ep.kind = EPI_SPLIT;
-  ep.Mv = op->n_isdf;
+  ep.Mv = op->n_isdf + op->kdef;
   ep.Nv = nb;
   ep.out_hi = op->T_hi;
   ep.out_lo = op->T_lo;
   ep.ldo = op->mu_k;
   ep.ws = op->ws;
-  ep.counters = op->counters;
   const int tiles_m = op->mu_pad / BM;
   const int tiles_n = (nb + op->BN1 - 1) / op->BN1;
-  return dispatch_tc(op->BN1, op->tA1hi, op->tA1lo, op->tShi, op->tSlo, tiles_m, tiles_n, ga, ep,
-                     s->d_status, s->stream);
+  NGW_TRY(dispatch_tc(op->BN1, op->tA1hi, op->tA1lo, op->tShi, op->tSlo, tiles_m, tiles_n, ga, ep,
+                      s->d_status, s->stream));
+  if (op->split1 > 1) {
+    const size_t total = (size_t)ep.Mv * nb;
+    int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
+    k_splitk_reduce<<<blocks, 256, 0, s->stream>>>(op->ws, op->split1, op->BN1, tiles_m, ep.Mv, nb,
+                                                   op->T_hi, op->T_lo, op->mu_k);
+    NGW_CUDA(cudaGetLastError());
+  }
+  return NGW_OK;
 }
 
 // One GEMM2 with the Clenshaw epilogue.
@@ -629,8 +721,8 @@ static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, co
 }
 
 // out64 (ncv x nb, ld ldv) = p(C) v with p given by Chebyshev coefficients
-// g[0..n] on [c0 - c1, c0 + c1].  v: FP64 (ld ldv).  Launch-only (no sync),
-// so it can be captured in a CUDA graph.
+// g[0..n] on [c0 - c1, c0 + c1] for the deflated part and U p(Lambda) U^T v
+// for the deflated eigenpairs.  Launch-only (no host synchronisation).
 int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const double *g, int n,
                      double c0, double c1, int tda, double *out64) {
   MixedOperator *op = s->mixed;
@@ -643,28 +735,46 @@ int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const dou
     return NGW_ERR_ARG;
   }
   cudaStream_t st = s->stream;
+  const int ncv = s->ncv, k = op->kdef;
+  const double one = 1.0, mone = -1.0, zero = 0.0;
+  const double *vin = v;
+  int ldin = ldv;
+  if (k > 0) {
+    // xo = U^T v ; vperp = v - U xo
+    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, k, nb, ncv, &one, s->eig_U, ncv, v, ldv,
+                           &zero, op->xo, k));
+    NGW_CUDA(cudaMemcpy2DAsync(op->vperp, (size_t)ncv * 8, v, (size_t)ldv * 8, (size_t)ncv * 8, nb,
+                               cudaMemcpyDeviceToDevice, st));
+    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, ncv, nb, k, &mone, s->eig_U, ncv, op->xo,
+                           k, &one, op->vperp, ncv));
+    vin = op->vperp;
+    ldin = ncv;
+  }
   {
-    int bx = (s->ncv + 255) / 256;
+    int bx = (ncv + 255) / 256;
     if (bx > 16) bx = 16;
-    k_cheb_start<<<dim3(bx, nb), 256, 0, st>>>(v, ldv, s->d_sqrtR, s->ncv, nb, g[n], tda,
-                                              op->bb[0], op->cv_pad, op->S_hi, op->S_lo,
-                                              op->cv_pad);
+    k_cheb_start<<<dim3(bx, nb), 256, 0, st>>>(vin, ldin, s->d_sqrtR, ncv, nb, g[n], tda, op->bb[0],
+                                              op->cv_pad, op->S_hi, op->S_lo, op->cv_pad);
     NGW_CUDA(cudaGetLastError());
   }
-  // buffers: cur = b_{k+1}, prev = b_{k+2}
-  int cur = 0, prev = -1;
-  for (int k = n - 1; k >= 1; --k) {
+  int cur = 0, prev = -1;   // slots of b_{k+1}, b_{k+2}
+  for (int kk = n - 1; kk >= 1; --kk) {
     NGW_TRY(run_gemm1(s, nb));
     // b_k goes to the slot that is neither b_{k+1} nor b_{k+2}
     const int outb = (prev < 0) ? 1 : 3 - cur - prev;
-    NGW_TRY(run_gemm2(s, nb, op->bb[cur], prev < 0 ? nullptr : op->bb[prev], v, ldv, g[k],
+    NGW_TRY(run_gemm2(s, nb, op->bb[cur], prev < 0 ? nullptr : op->bb[prev], vin, ldin, g[kk],
                       2.0 / c1, c0, 1.0, tda, op->bb[outb], nullptr, true));
     prev = cur;
     cur = outb;
   }
   NGW_TRY(run_gemm1(s, nb));
-  NGW_TRY(run_gemm2(s, nb, op->bb[cur], prev < 0 ? nullptr : op->bb[prev], v, ldv, g[0],
+  NGW_TRY(run_gemm2(s, nb, op->bb[cur], prev < 0 ? nullptr : op->bb[prev], vin, ldin, g[0],
                     1.0 / c1, c0, 1.0, tda, nullptr, out64, false));
+  if (k > 0) {
+    // out += U p(Lambda) xo
+    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, ncv, nb, k, &one, op->Up, ncv, op->xo,
+                           k, &one, out64, ldv));
+  }
   return NGW_OK;
 }
 
@@ -706,7 +816,7 @@ extern "C" int ngw_profile_mixed_gemms(ngw_session *s, int nb, int reps, double 
     return NGW_ERR_ARG;
   }
   if (!s->mixed) {
-    set_error("mixed operator not built (set precision to mixed and set the operator)");
+    set_error("mixed operator not built (run a mixed-precision solve first)");
     return NGW_ERR_STATE;
   }
   NGW_CUDA(cudaSetDevice(s->device));
@@ -738,7 +848,7 @@ extern "C" int ngw_profile_mixed_gemms(ngw_session *s, int nb, int reps, double 
   return check_status(s);
 }
 
-// Shapes of the two GEMMs for the roofline (padded M, N, K and split-K).
+// Shapes of the two GEMMs for the roofline (valid M, N, K, N tile, split-K).
 extern "C" int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape) {
   using namespace ngw;
   if (!s || !s->mixed || !shape) {
@@ -747,7 +857,8 @@ extern "C" int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape) {
   }
   NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
   MixedOperator *op = s->mixed;
-  shape[0] = op->n_isdf; shape[1] = nb; shape[2] = op->ncv; shape[3] = op->BN1; shape[4] = op->split1;
-  shape[5] = op->ncv; shape[6] = nb; shape[7] = op->n_isdf; shape[8] = op->BN2;
+  shape[0] = op->n_isdf + op->kdef; shape[1] = nb; shape[2] = op->ncv; shape[3] = op->BN1;
+  shape[4] = op->split1;
+  shape[5] = op->ncv; shape[6] = nb; shape[7] = op->n_isdf + op->kdef; shape[8] = op->BN2;
   return NGW_OK;
 }

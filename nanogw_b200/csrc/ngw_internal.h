@@ -71,7 +71,11 @@ struct ngw_session {
   bool have_isdf = false, have_pairs = false, have_C = false;
   ngw::MixedOperator *mixed = nullptr;
   int *d_status = nullptr;     // device status word
-  double lmax = 0.0, lmax_tda = 0.0;   // cached spectral upper bounds (C, A)
+  // top eigenpairs of C (FP64 Lanczos, full reorthogonalisation) for deflation
+  std::vector<double> eig_vals, eig_res;   // Ritz values (descending) and residual bounds
+  double *eig_U = nullptr;                  // (ncv, eig_k) Ritz vectors
+  size_t eig_U_bytes = 0;
+  int eig_k = 0, eig_tda = -1;
   // scratch (grown on demand)
   std::vector<ngw::DBuf> scratch;
   std::vector<void *> owned;
