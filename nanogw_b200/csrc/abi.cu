@@ -2,6 +2,7 @@
 // Lanczos spectra, Sigma_c driver, k_integrate and the QP Newton solve.
 // FP64 GEMMs of the plain path go through cuBLAS (library GEMMs); every other
 // step is a kernel of this library.
+#include <algorithm>
 #include <cstdarg>
 #include <cstring>
 #include <cmath>
@@ -15,6 +16,7 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda);
 int mixed_kdef(ngw_session *s);
 int mixed_set_deflation_values(ngw_session *s, const double *pvals);
 int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps);
+void extern_mixed_tune(ngw_session *s, int *tune);
 int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1);
 int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const double *g, int n,
                      double c0, double c1, int tda, double *out64);
@@ -217,18 +219,27 @@ static int plan_mixed(ngw_session *s, PolyPlan &pp, double lo_in, double hi_in) 
     pp.c1 = 0.5 * (hi_in - lo_in);
     pp.kdef = 0;
   } else {
-    if (s->eig_tda != tda) NGW_TRY(compute_top_eigs(s, tda, 48, 160));
+    if (s->eig_tda != tda) NGW_TRY(compute_top_eigs(s, tda, 64, 240));
     const std::vector<double> &r = s->eig_vals, &res = s->eig_res;
     const int mm = (int)r.size();
     int k = 0;
     if (!tda) {
-      while (k < std::min(s->eig_k, mm - 1)) {
-        const double nxt = 1.05 * r[k + 1];
-        double pmax = 0.0;
-        for (int i = 0; i <= 2000; ++i) pmax = std::max(pmax, std::fabs(poly_eval(pp.poly, nxt * i / 2000.0)));
-        if (std::fabs(poly_eval(pp.poly, r[k])) > 4.0 * pmax && res[k] < 1e-6 * std::fabs(r[0])) ++k;
-        else break;
-      }
+      // typical |p| on the spectrum: median over the Ritz values
+      std::vector<double> pv(mm);
+      for (int i = 0; i < mm; ++i) pv[i] = std::fabs(poly_eval(pp.poly, r[i]));
+      std::vector<double> srt(pv);
+      std::nth_element(srt.begin(), srt.begin() + mm / 2, srt.end());
+      const double typical = std::max(srt[mm / 2], 1e-300);
+      // deflate while the Clenshaw interval [0, 1.05 lambda_k] would hold
+      // values of |p| more than 8x the typical one
+      auto interval_max = [&](double h) {
+        double m = 0.0;
+        for (int i = 0; i <= 4000; ++i) m = std::max(m, std::fabs(poly_eval(pp.poly, h * i / 4000.0)));
+        return m;
+      };
+      while (k < std::min(s->eig_k, mm - 1) && interval_max(1.05 * (r[k] + res[k])) > 8.0 * typical &&
+             res[k] < 1e-6 * std::fabs(r[0]))
+        ++k;
     }
     const double top = (k < mm) ? r[k] + res[k] : 0.0;
     const double hi = std::max(1.05 * top, 1e-12);
@@ -267,6 +278,60 @@ static int make_plan(ngw_session *s, PolyPlan &pp, const double *poly, int npoly
   }
   if (s->precision == NGW_PREC_MIXED) NGW_TRY(plan_mixed(s, pp, lo, hi));
   return NGW_OK;
+}
+
+// Run `region` (launches only, no host synchronisation or allocation) on the
+// session stream, through a CUDA graph once the same key has been seen before.
+template <class F>
+static int run_graphed(ngw_session *s, const std::vector<unsigned long long> &key, F region) {
+  if (!s->use_graphs) return region();
+  ngw_session::GraphEntry *e = nullptr;
+  for (auto &g : s->graphs)
+    if (g.key == key) e = &g;
+  if (!e) {
+    if (s->graphs.size() >= 8) {
+      if (s->graphs.front().exec) cudaGraphExecDestroy(s->graphs.front().exec);
+      s->graphs.erase(s->graphs.begin());
+    }
+    s->graphs.push_back(ngw_session::GraphEntry());
+    e = &s->graphs.back();
+    e->key = key;
+  }
+  if (e->exec) {
+    NGW_CUDA(cudaGraphLaunch(e->exec, s->stream));
+    return NGW_OK;
+  }
+  if (e->seen == 0) {   // first time: run eagerly (sizes every scratch buffer)
+    e->seen = 1;
+    return region();
+  }
+  cudaGraph_t graph = nullptr;
+  NGW_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = region();
+  cudaError_t ce = cudaStreamEndCapture(s->stream, &graph);
+  if (rc != NGW_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ce != cudaSuccess) {
+    set_error("graph capture failed: %s", cudaGetErrorString(ce));
+    return NGW_ERR_CUDA;
+  }
+  ce = cudaGraphInstantiate(&e->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) {
+    e->exec = nullptr;
+    set_error("graph instantiate failed: %s", cudaGetErrorString(ce));
+    return NGW_ERR_CUDA;
+  }
+  NGW_CUDA(cudaGraphLaunch(e->exec, s->stream));
+  return NGW_OK;
+}
+
+static unsigned long long dbits(double x) {
+  unsigned long long u;
+  std::memcpy(&u, &x, 8);
+  return u;
 }
 
 }  // namespace ngw
@@ -308,6 +373,12 @@ int ngw_session_create(int device, ngw_session **out) {
   }
   cublasSetStream(s->cublas, s->stream);
   cublasSetMathMode(s->cublas, CUBLAS_DEFAULT_MATH);
+  // a fixed cuBLAS workspace lets its GEMMs be captured in CUDA graphs
+  if (dalloc(s, &s->cublas_ws, 64ull << 20) != NGW_OK) {
+    ngw_session_destroy(s);
+    return NGW_ERR_OOM;
+  }
+  cublasSetWorkspace(s->cublas, s->cublas_ws, 64ull << 20);
   if (dalloc(s, (void **)&s->d_status, sizeof(int)) != NGW_OK) {
     ngw_session_destroy(s);
     return NGW_ERR_OOM;
@@ -322,8 +393,11 @@ void ngw_session_destroy(ngw_session *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   mixed_free(s);
+  for (auto &g : s->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto &b : s->scratch)
     if (b.p) cudaFree(b.p);
+  if (s->cublas_ws) cudaFree(s->cublas_ws);
   void *ptrs[] = {s->d_psi, s->d_M, s->d_Mxc, s->d_cvpair, s->d_sqrtR, s->d_C, s->d_status, s->eig_U};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -651,24 +725,47 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
     NGW_CUDA(cudaMemcpyAsync(chb, hb.data(), (size_t)2 * nb * 4, cudaMemcpyHostToDevice, s->stream));
     NGW_CUDA(cudaMemcpyAsync(chq, hq.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
     NGW_CUDA(cudaStreamSynchronize(s->stream));
-    // start vectors  P = sqrtR * C^T M (psi_m psi_n)   (F90z:578-709), FP64
-    launch_pair_gather_cols(s->d_psi, n, chb, chb + nb, nb, cmn, s->stream);
-    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, n, nb, n, &one, s->d_M, n, cmn, n,
-                           &zero, cm, n));
-    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, ncv, nb, n, &one, s->d_C, n, cm, n,
-                           &zero, P, ncv));
-    launch_norms(P, ncv, nb, s->d_sqrtR, tamm_d, P2, pn2, s->stream);
-    NGW_CUDA(cudaMemsetAsync(a, 0, (size_t)niter * nb * 8, s->stream));
-    NGW_CUDA(cudaMemsetAsync(b, 0, (size_t)niter * nb * 8, s->stream));
-    // pnorm = sqrt(pnorm2), v0 = P / pnorm   (F90z:707-709, lanczos_spectra_lowcomsym.F90:68-70)
-    launch_sqrt_vec(pn2, pn, nb, s->stream);
-    launch_lanczos_init(P2, ncv, pn, V, hs, s->d_sqrtR, ncv, nb, tamm_d, b, niter, s->stream);
-    NGW_TRY(lanczos_dev(s, pp, nb, niter, V, W, hs, tmp, a, b));
-    launch_sigma_spectra(a, b, niter, nb, de1, chb + nb, chq, zz0, de, nen, p->ecuts, p->nval, S,
-                         s->stream);
-    launch_sigma_reduce(S, pn2, de1, chb + nb, zz0 + q0, de, nen, p->ecuts, p->nval, nbsum, nq,
-                        tamm_d, sig + (size_t)2 * q0 * nen, 0, s->stream);
-    NGW_CUDA(cudaGetLastError());
+    auto region = [&]() -> int {
+      // start vectors  P = sqrtR * C^T M (psi_m psi_n)   (F90z:578-709), FP64
+      launch_pair_gather_cols(s->d_psi, n, chb, chb + nb, nb, cmn, s->stream);
+      NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, n, nb, n, &one, s->d_M, n, cmn, n,
+                             &zero, cm, n));
+      NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, ncv, nb, n, &one, s->d_C, n, cm, n,
+                             &zero, P, ncv));
+      launch_norms(P, ncv, nb, s->d_sqrtR, tamm_d, P2, pn2, s->stream);
+      NGW_CUDA(cudaMemsetAsync(a, 0, (size_t)niter * nb * 8, s->stream));
+      NGW_CUDA(cudaMemsetAsync(b, 0, (size_t)niter * nb * 8, s->stream));
+      // pnorm = sqrt(pnorm2), v0 = P / pnorm   (F90z:707-709, lanczos_spectra_lowcomsym.F90:68-70)
+      launch_sqrt_vec(pn2, pn, nb, s->stream);
+      launch_lanczos_init(P2, ncv, pn, V, hs, s->d_sqrtR, ncv, nb, tamm_d, b, niter, s->stream);
+      NGW_TRY(lanczos_dev(s, pp, nb, niter, V, W, hs, tmp, a, b));
+      launch_sigma_spectra(a, b, niter, nb, de1, chb + nb, chq, zz0, de, nen, p->ecuts, p->nval, S,
+                           s->stream);
+      launch_sigma_reduce(S, pn2, de1, chb + nb, zz0 + q0, de, nen, p->ecuts, p->nval, nbsum, nq,
+                          tamm_d, sig + (size_t)2 * q0 * nen, 0, s->stream);
+      NGW_CUDA(cudaGetLastError());
+      return NGW_OK;
+    };
+    std::vector<unsigned long long> key = {
+        (unsigned long long)s->precision, (unsigned long long)nb, (unsigned long long)niter,
+        (unsigned long long)pp.npoly, (unsigned long long)tamm_d, (unsigned long long)nen,
+        (unsigned long long)p->nval, (unsigned long long)nbsum, (unsigned long long)nq,
+        (unsigned long long)q0, (unsigned long long)pp.kdef, dbits(p->ecuts), dbits(de),
+        dbits(pp.c0), dbits(pp.c1)};
+    for (double c : pp.poly) key.push_back(dbits(c));
+    for (double c : pp.cheb) key.push_back(dbits(c));
+    for (const void *ptr : {(const void *)cmn, (const void *)cm, (const void *)P, (const void *)P2,
+                            (const void *)pn2, (const void *)pn, (const void *)V, (const void *)W,
+                            (const void *)hs, (const void *)tmp, (const void *)a, (const void *)b,
+                            (const void *)S, (const void *)chb, (const void *)chq, (const void *)de1,
+                            (const void *)zz0, (const void *)sig, (const void *)s->mixed})
+      key.push_back((unsigned long long)(uintptr_t)ptr);
+    if (s->mixed) {
+      int tune[4];
+      extern_mixed_tune(s, tune);
+      for (int t : tune) key.push_back((unsigned long long)t);
+    }
+    NGW_TRY(run_graphed(s, key, region));
     if (alpha)
       NGW_CUDA(cudaMemcpyAsync(alpha + (size_t)q0 * nbsum * niter, a, (size_t)niter * nb * 8,
                                cudaMemcpyDeviceToHost, s->stream));

@@ -73,8 +73,8 @@ constexpr int NTHREADS = 256;
 
 // Epilogue loads for one 16-column chunk, issued before any arithmetic so the
 // global-memory latencies overlap.
-template <int BN, int STAGES>
-__global__ void __launch_bounds__(NTHREADS, 1)
+template <int BN, int STAGES, int MINB>
+__global__ void __launch_bounds__(NTHREADS, MINB)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
               const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
               GemmArgs ga, EpiParams ep, int *status) {
@@ -175,21 +175,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const bool partial = ga.nsplit > 1;
     const int tile = blockIdx.y * gridDim.x + blockIdx.x;
     float *wsl = partial ? ep.ws + ((size_t)tile * ga.nsplit + split) * (size_t)(BN * BM) : nullptr;
-    for (int ch = ch_begin; ch < ch_end; ++ch) {
-      const int c = ch * 16;
-      float v[16];
+    for (int ch = 2 * ch_begin; ch < 2 * ch_end; ++ch) {
+      const int c = ch * 8;
+      float v[8];
       if (have) {
-        tc::tmem_ld16(trow + c, v);
+        tc::tmem_ld8(trow + c, v);
       } else {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = 0.f;
+        for (int j = 0; j < 8; ++j) v[j] = 0.f;
       }
       if (partial) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) wsl[(size_t)(c + j) * BM + mloc] = v[j];
+        for (int j = 0; j < 8; ++j) wsl[(size_t)(c + j) * BM + mloc] = v[j];
       } else if (m < ep.Mv) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < 8; ++j) {
           const int n = n0 + c + j;
           if (n < ep.Nv) {
             bf16 hi, lo;
@@ -202,35 +202,36 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
   } else {
     // EPI_CLENSHAW: y = R^2 x + 4 R^1/2 z (TDA: R x + 2 z);
-    // out = gamma v + alpha (y - c0 x) - beta b2; split((R^1/2 or 1) out)
+    // out = gamma v + alpha (y - c0 x) - beta b2; split((R^1/2 or 1) out).
+    // 8-column chunks keep the register count low enough for 2 CTAs per SM.
     const bool mv = m < ep.Mv;
     const double si = mv ? ep.s[m] : 0.0;
     const double s2 = si * si;
     const double sc = ep.tda ? 1.0 : si;
-    for (int ch = ch_begin; ch < ch_end; ++ch) {
-      const int c = ch * 16;
-      float z[16];
+    for (int ch = 2 * ch_begin; ch < 2 * ch_end; ++ch) {
+      const int c = ch * 8;
+      float z[8];
       if (have) {
-        tc::tmem_ld16(trow + c, z);
+        tc::tmem_ld8(trow + c, z);
       } else {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) z[j] = 0.f;
+        for (int j = 0; j < 8; ++j) z[j] = 0.f;
       }
       if (!mv) continue;
       const int nbase = n0 + c;
-      const int nj = min(16, ep.Nv - nbase);
+      const int nj = min(8, ep.Nv - nbase);
       if (nj <= 0) continue;
-      float xv[16], b2v[16];
-      double vv[16];
+      float xv[8], b2v[8];
+      double vv[8];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
+      for (int j = 0; j < 8; ++j) {
         const size_t o = (size_t)(nbase + j) * ep.ldx + m;
         xv[j] = (j < nj) ? __ldg(ep.x + o) : 0.f;
         b2v[j] = (j < nj && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
         vv[j] = (j < nj && ep.v) ? __ldg(ep.v + (size_t)(nbase + j) * ep.ldv + m) : 0.0;
       }
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
+      for (int j = 0; j < 8; ++j) {
         if (j >= nj) break;
         const int n = nbase + j;
         const double x = (double)xv[j];
@@ -318,41 +319,60 @@ static int make_tmap(CUtensorMap *map, const void *ptr, int rows, int cols, int 
   return NGW_OK;
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int MINB>
 static int launch_tc(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
                      const CUtensorMap &b_lo, int tiles_m, int tiles_n, const GemmArgs &ga,
                      const EpiParams &ep, int *status, cudaStream_t st) {
   constexpr size_t smem = (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) + 1024;
   static bool attr = false;
   if (!attr) {
-    NGW_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES>,
+    NGW_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, MINB>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
   }
   dim3 grid(tiles_m, tiles_n, ga.nsplit);
-  k_tc_gemm<BN, STAGES><<<grid, NTHREADS, smem, st>>>(a_hi, a_lo, b_hi, b_lo, ga, ep, status);
+  k_tc_gemm<BN, STAGES, MINB><<<grid, NTHREADS, smem, st>>>(a_hi, a_lo, b_hi, b_lo, ga, ep, status);
   NGW_CUDA(cudaGetLastError());
   return NGW_OK;
 }
 
-// supported N tiles (multiples of 16, <= 256); chosen per chain count
+// Supported N tiles (multiples of 16, <= 256).  Variant 0 ("deep"): one CTA
+// per SM with a long TMA ring; variant 1 ("shallow", N <= 160): 3-4 stages
+// and <= 128 registers so two CTAs share an SM and one CTA's epilogue
+// overlaps the other's main loop.
 static const int kBNs[] = {64, 80, 96, 128, 144, 160, 192, 240, 256};
 
-static int dispatch_tc(int BN, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
+static bool has_shallow(int BN) { return BN <= 160; }
+
+static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
                        const CUtensorMap &b_hi, const CUtensorMap &b_lo, int tiles_m, int tiles_n,
                        const GemmArgs &ga, const EpiParams &ep, int *status, cudaStream_t st) {
-  switch (BN) {
-    case 64: return launch_tc<64, 8>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st);
-    case 80: return launch_tc<80, 8>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st);
-    case 96: return launch_tc<96, 8>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st);
-    case 128: return launch_tc<128, 6>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st);
-    case 144: return launch_tc<144, 6>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st);
-    case 160: return launch_tc<160, 5>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st);
-    case 192: return launch_tc<192, 5>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st);
-    case 240: return launch_tc<240, 4>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st);
-    case 256: return launch_tc<256, 4>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st);
+#define NGW_TC(BNV, ST, MB) \
+  return launch_tc<BNV, ST, MB>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st)
+  if (var == 0) {
+    switch (BN) {
+      case 64: NGW_TC(64, 8, 1);
+      case 80: NGW_TC(80, 8, 1);
+      case 96: NGW_TC(96, 7, 1);
+      case 128: NGW_TC(128, 6, 1);
+      case 144: NGW_TC(144, 6, 1);
+      case 160: NGW_TC(160, 5, 1);
+      case 192: NGW_TC(192, 5, 1);
+      case 240: NGW_TC(240, 4, 1);
+      case 256: NGW_TC(256, 4, 1);
+    }
+  } else {
+    switch (BN) {
+      case 64: NGW_TC(64, 4, 2);
+      case 80: NGW_TC(80, 4, 2);
+      case 96: NGW_TC(96, 3, 2);
+      case 128: NGW_TC(128, 3, 2);
+      case 144: NGW_TC(144, 3, 2);
+      case 160: NGW_TC(160, 3, 2);
+    }
   }
-  set_error("unsupported N tile %d", BN);
+#undef NGW_TC
+  set_error("unsupported N tile %d / variant %d", BN, var);
   return NGW_ERR_ARG;
 }
 
@@ -439,7 +459,11 @@ struct MixedOperator {
   size_t op_bytes = 0;
   double *Up = nullptr;      // (ncv, kdef) U p(Lambda) for the current polynomial
   // chain buffers
-  int nb_cap = 0, nb_pad = 0, BN1 = 128, BN2 = 128, split1 = 1;
+  int nb_cap = 0, nb_pad = 0;
+  // tile choice (autotuned per chain count): N tile, kernel variant, split-K
+  int BN1 = 128, var1 = 0, split1 = 1, BN2 = 128, var2 = 0;
+  int tuned_nb = -1, maps_bn1 = -1, maps_bn2 = -1;
+  size_t ws_bytes = 0;
   bf16 *S_hi = nullptr, *S_lo = nullptr, *T_hi = nullptr, *T_lo = nullptr;
   CUtensorMap tShi, tSlo, tThi, tTlo;
   float *bb[3] = {nullptr, nullptr, nullptr};
@@ -462,6 +486,8 @@ static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
   s->bytes -= op->buf_bytes;
   op->buf_bytes = 0;
   op->nb_cap = 0;
+  op->maps_bn1 = op->maps_bn2 = -1;
+  op->tuned_nb = -1;
 }
 
 void mixed_free(ngw_session *s) {
@@ -477,6 +503,15 @@ void mixed_free(ngw_session *s) {
 }
 
 int mixed_kdef(ngw_session *s) { return s->mixed ? s->mixed->kdef : -1; }
+
+// current tile choice (part of the CUDA-graph key)
+void extern_mixed_tune(ngw_session *s, int *tune) {
+  MixedOperator *op = s->mixed;
+  tune[0] = op->BN1 * 16 + op->var1;
+  tune[1] = op->split1;
+  tune[2] = op->BN2 * 16 + op->var2;
+  tune[3] = op->nb_cap;
+}
 
 int matvec_f64_dev_pub(ngw_session *s, int nb, double *hs, double *y, int tamm_d);
 
@@ -577,80 +612,148 @@ int mixed_set_deflation_values(ngw_session *s, const double *pvals) {
   return NGW_OK;
 }
 
-static int pick_bn(int nb) {
-  // smallest padding waste, then the larger tile
-  int best = 128, best_pad = 1 << 30;
+static int encode_chain_maps(MixedOperator *op, int bn1, int bn2) {
+  if (op->maps_bn1 != bn1) {
+    NGW_TRY(make_tmap(&op->tShi, op->S_hi, op->nb_pad, op->cv_pad, bn1));
+    NGW_TRY(make_tmap(&op->tSlo, op->S_lo, op->nb_pad, op->cv_pad, bn1));
+    op->maps_bn1 = bn1;
+  }
+  if (op->maps_bn2 != bn2) {
+    NGW_TRY(make_tmap(&op->tThi, op->T_hi, op->nb_pad, op->mu_k, bn2));
+    NGW_TRY(make_tmap(&op->tTlo, op->T_lo, op->nb_pad, op->mu_k, bn2));
+    op->maps_bn2 = bn2;
+  }
+  return NGW_OK;
+}
+
+static int run_gemm1(ngw_session *s, int nb);
+static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, const double *v,
+                     int ldv, double gamma, double alpha, double c0, double beta, int tda,
+                     float *out32, double *out64, bool write_split);
+
+// Autotuner: time every admissible (N tile, variant, split-K) for GEMM1 and
+// (N tile, variant) for GEMM2 on the session's buffers and keep the fastest.
+static int autotune(ngw_session *s, int nb) {
+  MixedOperator *op = s->mixed;
+  cudaEvent_t e0, e1;
+  NGW_CUDA(cudaEventCreate(&e0));
+  NGW_CUDA(cudaEventCreate(&e1));
+  auto time_it = [&](auto fn, float *ms) -> int {
+    NGW_TRY(fn());
+    NGW_CUDA(cudaEventRecord(e0, s->stream));
+    for (int r = 0; r < 3; ++r) NGW_TRY(fn());
+    NGW_CUDA(cudaEventRecord(e1, s->stream));
+    NGW_CUDA(cudaEventSynchronize(e1));
+    NGW_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    return NGW_OK;
+  };
+  const int total_kb1 = 3 * (op->cv_pad / BK);
+  const int tiles_m1 = op->mu_pad / BM;
+  float best1 = 1e30f, best2 = 1e30f;
+  int b_bn1 = 128, b_v1 = 0, b_sp1 = 1, b_bn2 = 128, b_v2 = 0;
   for (int bn : kBNs) {
-    int pad = round_up(nb, bn) - nb;
-    if (pad < best_pad || (pad == best_pad && bn > best)) {
-      best = bn;
-      best_pad = pad;
+    if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
+    const int waste = round_up(nb, bn) - nb;
+    if (waste * 8 > nb && bn != kBNs[0]) continue;     // at most 12.5% padding
+    for (int var = 0; var < 2; ++var) {
+      if (var == 1 && !has_shallow(bn)) continue;
+      const int tiles = tiles_m1 * ((nb + bn - 1) / bn);
+      for (int sp : {1, 2, 3, 4, 6, 8, 12, 16}) {
+        if (sp > 1 && total_kb1 / sp < 4) break;
+        if ((size_t)tiles * sp * bn * BM * sizeof(float) > op->ws_bytes && sp > 1) break;
+        if (tiles * sp > 4 * 148) break;
+        op->BN1 = bn;
+        op->var1 = var;
+        op->split1 = sp;
+        NGW_TRY(encode_chain_maps(op, bn, op->maps_bn2 < 0 ? bn : op->maps_bn2));
+        float ms = 0;
+        NGW_TRY(time_it([&]() { return run_gemm1(s, nb); }, &ms));
+        if (ms < best1) {
+          best1 = ms;
+          b_bn1 = bn;
+          b_v1 = var;
+          b_sp1 = sp;
+        }
+      }
+      op->BN2 = bn;
+      op->var2 = var;
+      NGW_TRY(encode_chain_maps(op, op->maps_bn1, bn));
+      float ms = 0;
+      NGW_TRY(time_it([&]() {
+        return run_gemm2(s, nb, op->bb[0], op->bb[1], nullptr, 0, 0.0, 1.0, 0.0, 1.0, op->tda,
+                         op->bb[2], nullptr, true);
+      }, &ms));
+      if (ms < best2) {
+        best2 = ms;
+        b_bn2 = bn;
+        b_v2 = var;
+      }
     }
   }
-  return best;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  op->BN1 = b_bn1;
+  op->var1 = b_v1;
+  op->split1 = b_sp1;
+  op->BN2 = b_bn2;
+  op->var2 = b_v2;
+  NGW_TRY(encode_chain_maps(op, b_bn1, b_bn2));
+  // buffers used for timing held scratch values: clear the operands again
+  NGW_CUDA(cudaMemsetAsync(op->T_hi, 0, (size_t)op->nb_pad * op->mu_k * sizeof(bf16), s->stream));
+  NGW_CUDA(cudaMemsetAsync(op->T_lo, 0, (size_t)op->nb_pad * op->mu_k * sizeof(bf16), s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  op->tuned_nb = nb;
+  return check_status(s);
 }
 
-// split-K factor for GEMM1: fill the 148 SMs with at least 4 k-blocks per CTA
-static int pick_split(int tiles, int total_kb) {
-  int best = 1;
-  double best_eff = 0.0;
-  for (int sp = 1; sp <= 16; ++sp) {
-    if (total_kb / sp < 4) break;
-    const int ctas = tiles * sp;
-    const int waves = (ctas + 147) / 148;
-    const double eff = (double)ctas / (148.0 * waves);
-    if (eff > best_eff + 0.02) {
-      best_eff = eff;
-      best = sp;
-    }
-  }
-  return best;
-}
-
+// Chain buffers for nb chains and the tuned tile choice (bn1/bn2/split1 > 0
+// force a choice instead of tuning).
 int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
   MixedOperator *op = s->mixed;
   if (!op) {
     set_error("mixed operator not built");
     return NGW_ERR_STATE;
   }
-  if (bn1 <= 0) bn1 = pick_bn(nb);
-  if (bn2 <= 0) bn2 = pick_bn(nb);
-  const int tiles_m1 = op->mu_pad / BM;
-  const int tiles_n1 = (nb + bn1 - 1) / bn1;
-  if (split1 <= 0) split1 = pick_split(tiles_m1 * tiles_n1, 3 * (op->cv_pad / BK));
-  if (op->nb_cap >= nb && op->BN1 == bn1 && op->BN2 == bn2 && op->split1 == split1) return NGW_OK;
-  free_chain_buffers(s, op);
-  const int nbp = round_up(nb, 256);
-  op->BN1 = bn1;
-  op->BN2 = bn2;
-  op->split1 = split1;
-  op->nb_pad = nbp;
-  const size_t sbytes = (size_t)nbp * op->cv_pad * sizeof(bf16);
-  const size_t tbytes = (size_t)nbp * op->mu_k * sizeof(bf16);
-  const size_t bbytes = (size_t)nbp * op->cv_pad * sizeof(float);
-  const size_t vbytes = (size_t)nbp * s->ncv * sizeof(double);
-  const size_t xbytes = (size_t)nbp * std::max(op->kdef, 1) * sizeof(double);
-  const size_t wsbytes =
-      split1 > 1 ? (size_t)tiles_m1 * ((nbp + bn1 - 1) / bn1) * split1 * bn1 * BM * sizeof(float) : 16;
-  NGW_CUDA(cudaMalloc(&op->S_hi, sbytes));
-  NGW_CUDA(cudaMalloc(&op->S_lo, sbytes));
-  NGW_CUDA(cudaMalloc(&op->T_hi, tbytes));
-  NGW_CUDA(cudaMalloc(&op->T_lo, tbytes));
-  for (int i = 0; i < 3; ++i) NGW_CUDA(cudaMalloc(&op->bb[i], bbytes));
-  NGW_CUDA(cudaMalloc(&op->vperp, vbytes));
-  NGW_CUDA(cudaMalloc(&op->xo, xbytes));
-  NGW_CUDA(cudaMalloc(&op->ws, wsbytes));
-  op->buf_bytes = 2 * sbytes + 2 * tbytes + 3 * bbytes + vbytes + xbytes + wsbytes;
-  s->bytes += op->buf_bytes;
-  NGW_CUDA(cudaMemsetAsync(op->S_hi, 0, sbytes, s->stream));
-  NGW_CUDA(cudaMemsetAsync(op->S_lo, 0, sbytes, s->stream));
-  NGW_CUDA(cudaMemsetAsync(op->T_hi, 0, tbytes, s->stream));
-  NGW_CUDA(cudaMemsetAsync(op->T_lo, 0, tbytes, s->stream));
-  NGW_TRY(make_tmap(&op->tShi, op->S_hi, nbp, op->cv_pad, bn1));
-  NGW_TRY(make_tmap(&op->tSlo, op->S_lo, nbp, op->cv_pad, bn1));
-  NGW_TRY(make_tmap(&op->tThi, op->T_hi, nbp, op->mu_k, bn2));
-  NGW_TRY(make_tmap(&op->tTlo, op->T_lo, nbp, op->mu_k, bn2));
-  op->nb_cap = nbp;
+  if (op->nb_cap < nb) {
+    free_chain_buffers(s, op);
+    const int nbp = round_up(nb, 256);
+    op->nb_pad = nbp;
+    const size_t sbytes = (size_t)nbp * op->cv_pad * sizeof(bf16);
+    const size_t tbytes = (size_t)nbp * op->mu_k * sizeof(bf16);
+    const size_t bbytes = (size_t)nbp * op->cv_pad * sizeof(float);
+    const size_t vbytes = (size_t)nbp * s->ncv * sizeof(double);
+    const size_t xbytes = (size_t)nbp * std::max(op->kdef, 1) * sizeof(double);
+    // split-K partials: enough for 16 splits of the smallest tile grid
+    const size_t wsbytes = (size_t)(op->mu_pad / BM) * ((nbp + 63) / 64) * 16 * 64 * BM * sizeof(float);
+    NGW_CUDA(cudaMalloc(&op->S_hi, sbytes));
+    NGW_CUDA(cudaMalloc(&op->S_lo, sbytes));
+    NGW_CUDA(cudaMalloc(&op->T_hi, tbytes));
+    NGW_CUDA(cudaMalloc(&op->T_lo, tbytes));
+    for (int i = 0; i < 3; ++i) NGW_CUDA(cudaMalloc(&op->bb[i], bbytes));
+    NGW_CUDA(cudaMalloc(&op->vperp, vbytes));
+    NGW_CUDA(cudaMalloc(&op->xo, xbytes));
+    NGW_CUDA(cudaMalloc(&op->ws, wsbytes));
+    op->ws_bytes = wsbytes;
+    op->buf_bytes = 2 * sbytes + 2 * tbytes + 3 * bbytes + vbytes + xbytes + wsbytes;
+    s->bytes += op->buf_bytes;
+    NGW_CUDA(cudaMemsetAsync(op->S_hi, 0, sbytes, s->stream));
+    NGW_CUDA(cudaMemsetAsync(op->S_lo, 0, sbytes, s->stream));
+    NGW_CUDA(cudaMemsetAsync(op->T_hi, 0, tbytes, s->stream));
+    NGW_CUDA(cudaMemsetAsync(op->T_lo, 0, tbytes, s->stream));
+    for (int i = 0; i < 3; ++i) NGW_CUDA(cudaMemsetAsync(op->bb[i], 0, bbytes, s->stream));
+    op->nb_cap = nbp;
+    op->maps_bn1 = op->maps_bn2 = -1;
+    op->tuned_nb = -1;
+  }
+  if (bn1 > 0 && bn2 > 0) {
+    op->BN1 = bn1;
+    op->BN2 = bn2;
+    op->var1 = op->var2 = 0;
+    op->split1 = split1 > 0 ? split1 : 1;
+    op->tuned_nb = -2;
+    return encode_chain_maps(op, bn1, bn2);
+  }
+  if (op->tuned_nb != nb) NGW_TRY(autotune(s, nb));
   return NGW_OK;
 }
 
@@ -672,8 +775,8 @@ static int run_gemm1(ngw_session *s, int nb) {
   ep.ws = op->ws;
   const int tiles_m = op->mu_pad / BM;
   const int tiles_n = (nb + op->BN1 - 1) / op->BN1;
-  NGW_TRY(dispatch_tc(op->BN1, op->tA1hi, op->tA1lo, op->tShi, op->tSlo, tiles_m, tiles_n, ga, ep,
-                      s->d_status, s->stream));
+  NGW_TRY(dispatch_tc(op->BN1, op->var1, op->tA1hi, op->tA1lo, op->tShi, op->tSlo, tiles_m, tiles_n,
+                      ga, ep, s->d_status, s->stream));
   if (op->split1 > 1) {
     const size_t total = (size_t)ep.Mv * nb;
     int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
@@ -716,8 +819,8 @@ static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, co
   ep.lds = op->cv_pad;
   const int tiles_m = op->cv_pad / BM;
   const int tiles_n = (nb + op->BN2 - 1) / op->BN2;
-  return dispatch_tc(op->BN2, op->tA3hi, op->tA3lo, op->tThi, op->tTlo, tiles_m, tiles_n, ga, ep,
-                     s->d_status, s->stream);
+  return dispatch_tc(op->BN2, op->var2, op->tA3hi, op->tA3lo, op->tThi, op->tTlo, tiles_m, tiles_n,
+                     ga, ep, s->d_status, s->stream);
 }
 
 // out64 (ncv x nb, ld ldv) = p(C) v with p given by Chebyshev coefficients

@@ -76,6 +76,15 @@ struct ngw_session {
   double *eig_U = nullptr;                  // (ncv, eig_k) Ritz vectors
   size_t eig_U_bytes = 0;
   int eig_k = 0, eig_tda = -1;
+  // CUDA graphs of the per-block Sigma_c region, keyed by shapes + pointers
+  struct GraphEntry {
+    std::vector<unsigned long long> key;
+    cudaGraphExec_t exec = nullptr;
+    int seen = 0;
+  };
+  std::vector<GraphEntry> graphs;
+  void *cublas_ws = nullptr;
+  bool use_graphs = true;
   // scratch (grown on demand)
   std::vector<ngw::DBuf> scratch;
   std::vector<void *> owned;
