@@ -136,6 +136,9 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--cpu-niter", type=int, default=15)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="profiling case: two mixed Sigma_c requests with --ncu-niter Lanczos steps")
+    ap.add_argument("--ncu-niter", type=int, default=3)
     args = ap.parse_args()
     W = max(3, args.warmup)
     K = args.steps
@@ -182,6 +185,19 @@ def main():
                 "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
+        return
+
+    if args.ncu_case:
+        with ngw.Session(local, "fp64") as sess:
+            op, qp, poly = build_workload(sess, wl)
+            cv, sr = op.pairs()
+            sess.set_isdf(op.psi_intp, op.mmtrx)
+            sess.set_pairs(cv, sr)
+            sess.set_precision(args.precision)
+            for _ in range(2):
+                sess.calculate_sigma_lanczos(op.e1, op.nval, qp, wl["nen"], wl["deltae"], wl["ecuts"],
+                                             args.ncu_niter, poly)
+        print("ncu case done", flush=True)
         return
 
     sess = ngw.Session(local, "fp64")
@@ -247,14 +263,15 @@ def main():
     roof = None
     if args.precision == "mixed":
         us1, us2 = sess.profile_mixed_gemms(nb, reps=50)
-        M1, N1, K1, BN1, sp1, M2, N2, K2, BN2 = sess.mixed_gemm_shapes(nb)
+        M1, N1, K1, BN1, sp1, M2, N2, K2, BN2, v1, v2 = sess.mixed_gemm_shapes(nb)
         flops = 2.0 * M1 * N1 * K1 + 2.0 * M2 * N2 * K2
         achieved = flops / ((us1 + us2) * 1e-6) / 1e12
         hbm, bf16, bf16s, src = load_peaks()
         roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
                 "frac": achieved / bf16, "traffic": None,
                 "kernel": "k_tc_gemm (GEMM1 + GEMM2 of one matvec)",
-                "us_per_launch": [us1, us2], "shapes": [[M1, N1, K1, BN1, sp1], [M2, N2, K2, BN2]],
+                "us_per_launch": [us1, us2], "shapes": [[M1, N1, K1, BN1, sp1, v1], [M2, N2, K2, BN2, 1, v2]],
+                "tiles_env": f"{BN1},{v1},{sp1},{BN2},{v2}",
                 "peak_source": f"{src} (bf16 dense, burst)",
                 "executed_bf16_frac": 3.0 * achieved / bf16}
 

@@ -22,6 +22,8 @@
 
 #include <cmath>
 #include <cstring>
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
 
 #include "ngw_internal.h"
@@ -753,6 +755,19 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
     op->tuned_nb = -2;
     return encode_chain_maps(op, bn1, bn2);
   }
+  // NGW_TILES="bn1,var1,split1,bn2,var2" fixes the tiles (reproducible profiling)
+  if (const char *env = getenv("NGW_TILES")) {
+    int t[5];
+    if (sscanf(env, "%d,%d,%d,%d,%d", &t[0], &t[1], &t[2], &t[3], &t[4]) == 5) {
+      op->BN1 = t[0];
+      op->var1 = t[1];
+      op->split1 = t[2];
+      op->BN2 = t[3];
+      op->var2 = t[4];
+      op->tuned_nb = nb;
+      return encode_chain_maps(op, t[0], t[3]);
+    }
+  }
   if (op->tuned_nb != nb) NGW_TRY(autotune(s, nb));
   return NGW_OK;
 }
@@ -963,5 +978,6 @@ extern "C" int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape) {
   shape[0] = op->n_isdf + op->kdef; shape[1] = nb; shape[2] = op->ncv; shape[3] = op->BN1;
   shape[4] = op->split1;
   shape[5] = op->ncv; shape[6] = nb; shape[7] = op->n_isdf + op->kdef; shape[8] = op->BN2;
+  shape[9] = op->var1; shape[10] = op->var2;
   return NGW_OK;
 }
