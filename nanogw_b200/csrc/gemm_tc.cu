@@ -259,6 +259,227 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent, warp-specialised variant.  One CTA per SM walks a static list
+// of work items (tile_m fastest, then tile_n, then split); each stage of the
+// TMA ring holds A_hi, A_lo, B_hi and B_lo of one 64-wide k-block, so the three
+// split-BF16 products (hi*hi, hi*lo, lo*hi) are 12 MMAs on operands loaded
+// once.  Two TMEM accumulators alternate between tiles: the MMA thread fills
+// one while the two epilogue warpgroups (warps 4-11) drain the other.
+constexpr int PTHREADS = 384;
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(PTHREADS, 1)
+    k_tc_gemm_p(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
+                const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
+                GemmArgs ga, EpiParams ep, int tiles_m, int tiles_n, int *status) {
+  constexpr uint32_t A_BYTES = BM * BK * 2;
+  constexpr uint32_t B_BYTES = BN * BK * 2;
+  constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  constexpr uint32_t TMEM_COLS = (2 * BN <= 128) ? 128 : (2 * BN <= 256) ? 256 : 512;
+  constexpr uint32_t ACC_STRIDE = TMEM_COLS / 2;   // accumulator buffers on aligned columns
+  constexpr uint32_t IDESC = tc::idesc_bf16_f32(BM, BN);
+  constexpr int NCH = BN / 8;               // 8-column chunks
+  constexpr int NCH0 = (NCH + 1) / 2;       // chunks of epilogue warpgroup 0
+
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  __shared__ __align__(8) uint64_t full_bar[STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[STAGES];
+  __shared__ __align__(8) uint64_t accf_bar[2];
+  __shared__ __align__(8) uint64_t acce_bar[2];
+  __shared__ uint32_t tmem_base_sh;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total_kb = ga.num_kb;           // k-blocks of the reduction (fused segments)
+  const int kb_per = (total_kb + ga.nsplit - 1) / ga.nsplit;
+  const int nwork = tiles_m * tiles_n * ga.nsplit;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc::mbar_init(tc::smem_u32(&full_bar[s]), 1);
+      tc::mbar_init(tc::smem_u32(&empty_bar[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(tc::smem_u32(&accf_bar[b]), 1);
+      tc::mbar_init(tc::smem_u32(&acce_bar[b]), 256);
+    }
+    tc::fence_barrier_init();
+    tc::prefetch_tmap(&tA_hi);
+    tc::prefetch_tmap(&tA_lo);
+    tc::prefetch_tmap(&tB_hi);
+    tc::prefetch_tmap(&tB_lo);
+  }
+  if (warp == 2) {
+    tc::tmem_alloc(tc::smem_u32(&tmem_base_sh), TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem_base = tmem_base_sh;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer ----
+      int it = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < nwork && ok; w += gridDim.x) {
+        const int tm = w % tiles_m, tn = (w / tiles_m) % tiles_n, sp = w / (tiles_m * tiles_n);
+        const int kb0 = sp * kb_per, kb1 = min(total_kb, kb0 + kb_per);
+        for (int kb = kb0; kb < kb1; ++kb, ++it) {
+          const int s = it % STAGES;
+          if (it >= STAGES && !tc::mbar_wait(tc::smem_u32(&empty_bar[s]), ((it / STAGES) - 1) & 1, status)) {
+            ok = false;
+            break;
+          }
+          const uint32_t bar = tc::smem_u32(&full_bar[s]);
+          const uint32_t sa = tc::smem_u32(smem + s * STAGE_BYTES);
+          tc::mbar_arrive_expect_tx(bar, STAGE_BYTES);
+          tc::tma_load_2d(sa, &tA_hi, bar, kb * BK, tm * BM);
+          tc::tma_load_2d(sa + A_BYTES, &tA_lo, bar, kb * BK, tm * BM);
+          tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kb * BK, tn * BN);
+          tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kb * BK, tn * BN);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer ----
+      int it = 0, t = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < nwork && ok; w += gridDim.x, ++t) {
+        const int sp = w / (tiles_m * tiles_n);
+        const int kb0 = sp * kb_per, kb1 = min(total_kb, kb0 + kb_per);
+        const int buf = t & 1;
+        if (t >= 2 && !tc::mbar_wait(tc::smem_u32(&acce_bar[buf]), ((t >> 1) - 1) & 1, status)) break;
+        tc::tc_fence_after();
+        const uint32_t tacc = tmem_base + buf * ACC_STRIDE;
+        for (int kb = kb0; kb < kb1; ++kb, ++it) {
+          const int s = it % STAGES;
+          if (!tc::mbar_wait(tc::smem_u32(&full_bar[s]), (it / STAGES) & 1, status)) {
+            ok = false;
+            break;
+          }
+          tc::tc_fence_after();
+          const uint32_t sa = tc::smem_u32(smem + s * STAGE_BYTES);
+          const uint32_t sah = sa, sal = sa + A_BYTES, sbh = sa + 2 * A_BYTES, sbl = sbh + B_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            const uint32_t acc0 = (kb > kb0 || kk > 0) ? 1u : 0u;
+            tc::mma_bf16(tacc, tc::smem_desc_sw128(sah + kk * 32), tc::smem_desc_sw128(sbh + kk * 32), IDESC, acc0);
+            tc::mma_bf16(tacc, tc::smem_desc_sw128(sah + kk * 32), tc::smem_desc_sw128(sbl + kk * 32), IDESC, 1u);
+            tc::mma_bf16(tacc, tc::smem_desc_sw128(sal + kk * 32), tc::smem_desc_sw128(sbh + kk * 32), IDESC, 1u);
+          }
+          tc::mma_commit(tc::smem_u32(&empty_bar[s]));
+        }
+        tc::mma_commit(tc::smem_u32(&accf_bar[buf]));
+      }
+    }
+  } else if (warp >= 4) {
+    // ---- epilogue: warps 4..11, lanes 32*(warp%4).., warpgroup (warp-4)/4 ----
+    const int wl = warp & 3, wg = (warp - 4) >> 2;
+    const int mloc = wl * 32 + lane;
+    const int ch_begin = wg == 0 ? 0 : NCH0;
+    const int ch_end = wg == 0 ? NCH0 : NCH;
+    int t = 0;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x, ++t) {
+      const int tm = w % tiles_m, tn = (w / tiles_m) % tiles_n, sp = w / (tiles_m * tiles_n);
+      const int kb0 = sp * kb_per, kb1 = min(total_kb, kb0 + kb_per);
+      const int buf = t & 1;
+      const bool have = tc::mbar_wait(tc::smem_u32(&accf_bar[buf]), (t >> 1) & 1, status) && kb1 > kb0;
+      tc::tc_fence_after();
+      const uint32_t trow = tmem_base + buf * ACC_STRIDE + ((uint32_t)(wl * 32) << 16);
+      const int m0 = tm * BM, n0 = tn * BN;
+      const int m = m0 + mloc;
+      if (ep.kind == EPI_SPLIT) {
+        const bool partial = ga.nsplit > 1;
+        const int tile = tn * tiles_m + tm;
+        float *wsl = partial ? ep.ws + ((size_t)tile * ga.nsplit + sp) * (size_t)(BN * BM) : nullptr;
+        for (int ch = ch_begin; ch < ch_end; ++ch) {
+          const int c = ch * 8;
+          float v[8];
+          if (have) {
+            tc::tmem_ld8(trow + c, v);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = 0.f;
+          }
+          if (partial) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) wsl[(size_t)(c + j) * BM + mloc] = v[j];
+          } else if (m < ep.Mv) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int n = n0 + c + j;
+              if (n < ep.Nv) {
+                bf16 hi, lo;
+                split_bf16(v[j], hi, lo);
+                ep.out_hi[(size_t)n * ep.ldo + m] = hi;
+                ep.out_lo[(size_t)n * ep.ldo + m] = lo;
+              }
+            }
+          }
+        }
+      } else {
+        const bool mv = m < ep.Mv;
+        const double si = mv ? ep.s[m] : 0.0;
+        const double s2 = si * si;
+        const double sc = ep.tda ? 1.0 : si;
+        for (int ch = ch_begin; ch < ch_end; ++ch) {
+          const int c = ch * 8;
+          float z[8];
+          if (have) {
+            tc::tmem_ld8(trow + c, z);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) z[j] = 0.f;
+          }
+          if (!mv) continue;
+          const int nbase = n0 + c;
+          const int nj = min(8, ep.Nv - nbase);
+          if (nj <= 0) continue;
+          float xv[8], b2v[8];
+          double vv[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const size_t o = (size_t)(nbase + j) * ep.ldx + m;
+            xv[j] = (j < nj) ? __ldg(ep.x + o) : 0.f;
+            b2v[j] = (j < nj && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
+            vv[j] = (j < nj && ep.v) ? __ldg(ep.v + (size_t)(nbase + j) * ep.ldv + m) : 0.0;
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            if (j >= nj) break;
+            const int n = nbase + j;
+            const double x = (double)xv[j];
+            const double y = ep.tda ? (s2 * x + 2.0 * (double)z[j]) : (s2 * s2 * x + 4.0 * si * (double)z[j]);
+            const double o = ep.gamma * vv[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
+            if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = (float)o;
+            if (ep.out64) ep.out64[(size_t)n * ep.ldv + m] = o;
+            if (ep.s_hi) {
+              bf16 hi, lo;
+              split_bf16((float)(sc * o), hi, lo);
+              ep.s_hi[(size_t)n * ep.lds + m] = hi;
+              ep.s_lo[(size_t)n * ep.lds + m] = lo;
+            }
+          }
+        }
+      }
+      tc::tc_fence_before();
+      tc::mbar_arrive(tc::smem_u32(&acce_bar[buf]));
+    }
+  }
+
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem_base, TMEM_COLS);
+  }
+}
+
 // Deterministic split-K reduction: D(m, n) = sum_s partial_s(m, n) in split
 // order, written as the split-BF16 pair.  One thread per output element,
 // consecutive threads on consecutive rows (coalesced partial reads).
@@ -338,6 +559,29 @@ static int launch_tc(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUt
   return NGW_OK;
 }
 
+template <int BN, int STAGES>
+static int launch_tc_p(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
+                       const CUtensorMap &b_lo, int tiles_m, int tiles_n, const GemmArgs &ga,
+                       const EpiParams &ep, int *status, cudaStream_t st) {
+  constexpr size_t smem = (size_t)STAGES * (2 * BM * BK * 2 + 2 * BN * BK * 2) + 1024;
+  static bool attr = false;
+  if (!attr) {
+    NGW_CUDA(cudaFuncSetAttribute(k_tc_gemm_p<BN, STAGES>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  GemmArgs g2 = ga;
+  g2.num_kb = ga.num_kb;   // fused segments: one k-block carries all three products
+  const int nwork = tiles_m * tiles_n * ga.nsplit;
+  const int grid = std::min(nwork, 148);
+  k_tc_gemm_p<BN, STAGES><<<grid, PTHREADS, smem, st>>>(a_hi, a_lo, b_hi, b_lo, g2, ep, tiles_m,
+                                                        tiles_n, status);
+  NGW_CUDA(cudaGetLastError());
+  return NGW_OK;
+}
+
+static bool has_persistent(int BN) { return BN <= 160; }
+
 // Supported N tiles (multiples of 16, <= 256).  Variant 0 ("deep"): one CTA
 // per SM with a long TMA ring; variant 1 ("shallow", N <= 160): 3-4 stages
 // and <= 128 registers so two CTAs share an SM and one CTA's epilogue
@@ -351,6 +595,19 @@ static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorM
                        const GemmArgs &ga, const EpiParams &ep, int *status, cudaStream_t st) {
 #define NGW_TC(BNV, ST, MB) \
   return launch_tc<BNV, ST, MB>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st)
+#define NGW_TCP(BNV, ST) \
+  return launch_tc_p<BNV, ST>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st)
+  if (var == 2) {
+    switch (BN) {
+      case 64: NGW_TCP(64, 4);
+      case 80: NGW_TCP(80, 4);
+      case 96: NGW_TCP(96, 4);
+      case 128: NGW_TCP(128, 3);
+      case 144: NGW_TCP(144, 3);
+      case 160: NGW_TCP(160, 3);
+    }
+  }
+#undef NGW_TCP
   if (var == 0) {
     switch (BN) {
       case 64: NGW_TC(64, 8, 1);
@@ -657,11 +914,13 @@ static int autotune(ngw_session *s, int nb) {
     if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
     const int waste = round_up(nb, bn) - nb;
     if (waste * 8 > nb && bn != kBNs[0]) continue;     // at most 12.5% padding
-    for (int var = 0; var < 2; ++var) {
+    for (int var = 0; var < 3; ++var) {
       if (var == 1 && !has_shallow(bn)) continue;
+      if (var == 2 && !has_persistent(bn)) continue;
       const int tiles = tiles_m1 * ((nb + bn - 1) / bn);
+      const int tkb = (var == 2) ? total_kb1 / 3 : total_kb1;
       for (int sp : {1, 2, 3, 4, 6, 8, 12, 16}) {
-        if (sp > 1 && total_kb1 / sp < 4) break;
+        if (sp > 1 && tkb / sp < 3) break;
         if ((size_t)tiles * sp * bn * BM * sizeof(float) > op->ws_bytes && sp > 1) break;
         if (tiles * sp > 4 * 148) break;
         op->BN1 = bn;
