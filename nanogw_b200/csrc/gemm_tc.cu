@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
+#include <utility>
 
 #include "ngw_internal.h"
 #include "tc_gemm.cuh"
@@ -123,6 +124,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem_d = tmem_base_sh;
+  tc::pdl_wait();                 // operands / epilogue inputs come from the previous kernel
+  tc::pdl_launch_dependents();
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer: k-blocks of the concatenated segments ----
@@ -319,6 +322,8 @@ __global__ void __launch_bounds__(PTHREADS, 1)
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem_base = tmem_base_sh;
+  tc::pdl_wait();                 // operands / epilogue inputs come from the previous kernel
+  tc::pdl_launch_dependents();
 
   if (warp == 0) {
     if (lane == 0) {
@@ -486,6 +491,8 @@ __global__ void __launch_bounds__(PTHREADS, 1)
 __global__ void k_splitk_reduce(const float *__restrict__ ws, int nsplit, int BN, int tiles_m,
                                 int Mv, int Nv, bf16 *__restrict__ out_hi, bf16 *__restrict__ out_lo,
                                 int ldo) {
+  tc::pdl_wait();
+  tc::pdl_launch_dependents();
   const size_t total = (size_t)Mv * Nv;
   for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
        idx += (size_t)gridDim.x * blockDim.x) {
@@ -542,6 +549,33 @@ static int make_tmap(CUtensorMap *map, const void *ptr, int rows, int cols, int 
   return NGW_OK;
 }
 
+// Launch with the programmatic-stream-serialisation attribute so the kernel's
+// prologue overlaps the previous kernel's tail (disable with NGW_PDL=0).
+static bool pdl_enabled() {
+  static int en = -1;
+  if (en < 0) {
+    const char *e = getenv("NGW_PDL");
+    en = (e && e[0] == '0') ? 0 : 1;
+  }
+  return en == 1;
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 template <int BN, int STAGES, int MINB>
 static int launch_tc(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
                      const CUtensorMap &b_lo, int tiles_m, int tiles_n, const GemmArgs &ga,
@@ -554,8 +588,8 @@ static int launch_tc(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUt
     attr = true;
   }
   dim3 grid(tiles_m, tiles_n, ga.nsplit);
-  k_tc_gemm<BN, STAGES, MINB><<<grid, NTHREADS, smem, st>>>(a_hi, a_lo, b_hi, b_lo, ga, ep, status);
-  NGW_CUDA(cudaGetLastError());
+  NGW_CUDA(launch_pdl(k_tc_gemm<BN, STAGES, MINB>, grid, dim3(NTHREADS), smem, st, a_hi, a_lo, b_hi,
+                      b_lo, ga, ep, status));
   return NGW_OK;
 }
 
@@ -574,9 +608,8 @@ static int launch_tc_p(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const C
   g2.num_kb = ga.num_kb;   // fused segments: one k-block carries all three products
   const int nwork = tiles_m * tiles_n * ga.nsplit;
   const int grid = std::min(nwork, 148);
-  k_tc_gemm_p<BN, STAGES><<<grid, PTHREADS, smem, st>>>(a_hi, a_lo, b_hi, b_lo, g2, ep, tiles_m,
-                                                        tiles_n, status);
-  NGW_CUDA(cudaGetLastError());
+  NGW_CUDA(launch_pdl(k_tc_gemm_p<BN, STAGES>, dim3(grid), dim3(PTHREADS), smem, st, a_hi, a_lo, b_hi,
+                      b_lo, g2, ep, tiles_m, tiles_n, status));
   return NGW_OK;
 }
 
@@ -1054,9 +1087,8 @@ static int run_gemm1(ngw_session *s, int nb) {
   if (op->split1 > 1) {
     const size_t total = (size_t)ep.Mv * nb;
     int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
-    k_splitk_reduce<<<blocks, 256, 0, s->stream>>>(op->ws, op->split1, op->BN1, tiles_m, ep.Mv, nb,
-                                                   op->T_hi, op->T_lo, op->mu_k);
-    NGW_CUDA(cudaGetLastError());
+    NGW_CUDA(launch_pdl(k_splitk_reduce, dim3(blocks), dim3(256), 0, s->stream, (const float *)op->ws,
+                        op->split1, op->BN1, tiles_m, ep.Mv, nb, op->T_hi, op->T_lo, op->mu_k));
   }
   return NGW_OK;
 }
