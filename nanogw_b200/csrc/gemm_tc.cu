@@ -962,6 +962,8 @@ static int autotune(ngw_session *s, int nb) {
         NGW_TRY(encode_chain_maps(op, bn, op->maps_bn2 < 0 ? bn : op->maps_bn2));
         float ms = 0;
         NGW_TRY(time_it([&]() { return run_gemm1(s, nb); }, &ms));
+        if (getenv("NGW_TUNE_VERBOSE"))
+          fprintf(stderr, "tune gemm1 bn=%d var=%d split=%d: %.2f us\n", bn, var, sp, 1e3f * ms / 3);
         if (ms < best1) {
           best1 = ms;
           b_bn1 = bn;
@@ -977,6 +979,8 @@ static int autotune(ngw_session *s, int nb) {
         return run_gemm2(s, nb, op->bb[0], op->bb[1], nullptr, 0, 0.0, 1.0, 0.0, 1.0, op->tda,
                          op->bb[2], nullptr, true);
       }, &ms));
+      if (getenv("NGW_TUNE_VERBOSE"))
+        fprintf(stderr, "tune gemm2 bn=%d var=%d: %.2f us\n", bn, var, 1e3f * ms / 3);
       if (ms < best2) {
         best2 = ms;
         b_bn2 = bn;
