@@ -126,6 +126,22 @@ int ngw_qp_newton(ngw_session *s, int nqp, int nen, const double *sigma_c_ev,
                   const double *sigx_ev, const double *vxc_ev, double xacc_ev,
                   double *eqp_ev, double *zfac, int *ierr);
 
+/* QP Newton solve that allocates nothing; no counterpart in the reference.
+ * For callers that cannot call cudaMalloc (a driver that hands out device
+ * memory from its own pool, code running during stream capture, a process
+ * whose allocator holds all free memory).  Every pointer is a DEVICE pointer
+ * with the layout of ngw_qp_newton; the call is ordered on `stream`
+ * (cudaStream_t, NULL = default stream) and returns without synchronising.
+ * The spline workspace is a fixed device array of 2^18 doubles shared by all
+ * calls on a device: nqp * 4 * nen must not exceed 262144 (NGW_ERR_BUDGET
+ * otherwise), and calls whose kernels overlap on the GPU race on it.  The
+ * first call on each device looks up the array's address; make it before any
+ * stream capture. */
+int ngw_qp_newton_noalloc(int nqp, int nen, const double *sigma_c_ev, const double *e1_ev,
+                          const double *e0_ev, double deltae_ev, const double *sigx_ev,
+                          const double *vxc_ev, double xacc_ev, double *eqp_ev, double *zfac,
+                          int *ierr, void *stream);
+
 /* ---- measurement ---- */
 /* Average device time (us) of one launch of each mixed-precision GEMM for nb
  * chains (GEMM1: T = C_isdf S, GEMM2: Z = (M C_isdf)^T T with its Clenshaw
