@@ -168,6 +168,13 @@ int ngw_build_coulomb_kernel(ngw_session *s, int ngrid, int n_isdf, const double
                              const int *grid_idx, int nfft, double h, double trunc,
                              double *mmtrx);
 
+/* f_xc block: M_xc = ntrans/hcub * zeta^T (f_xc * zeta), f_xc the LDA kernel
+ * of rho (shared/xc_module.F90:853-893, Ry bohr^3) -- replaces
+ * shared/isdf_parallel_sym_UltraLowMem.F90:809-839.  rho (ngrid) > 0;
+ * fxc_out (ngrid) optional. */
+int ngw_build_fxc_kernel(ngw_session *s, int ngrid, int n_isdf, const double *zeta,
+                         const double *rho, double h, double *mxc, double *fxc_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -189,6 +189,16 @@ class Session:
         check(lib().ngw_mixed_gemm_shapes(self._h, int(nb), _p(sh)))
         return [int(x) for x in sh]
 
+    def build_fxc_kernel(self, zeta, rho, h, return_fxc=False):
+        """M_xc = zeta^T (f_xc * zeta) / hcub with the LDA f_xc of rho (Ry)."""
+        zt = _f64(zeta)
+        r = np.ascontiguousarray(rho, dtype=np.float64)
+        ngrid, n_isdf = zt.shape
+        m = np.zeros((n_isdf, n_isdf), order="F")
+        f = np.zeros(ngrid) if return_fxc else None
+        check(lib().ngw_build_fxc_kernel(self._h, ngrid, n_isdf, _p(zt), _p(r), float(h), _p(m), _p(f)))
+        return (m, f) if return_fxc else m
+
     def build_coulomb_kernel(self, zeta, grid_idx, nfft, h, trunc):
         zt = _f64(zeta)
         g = np.ascontiguousarray(grid_idx, dtype=np.int32)

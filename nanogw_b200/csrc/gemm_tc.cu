@@ -24,7 +24,9 @@
 #include <cstring>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <utility>
 
 #include "ngw_internal.h"
@@ -1004,6 +1006,22 @@ static int autotune(ngw_session *s, int nb) {
   return check_status(s);
 }
 
+// Process-wide cache of tile choices, keyed by the GEMM shapes: every session
+// with the same shapes uses the same tiles (and therefore the same summation
+// order), so a request gives bit-identical results alone or among others.
+struct TuneKey {
+  int mu_pad, cv_pad, mu_k, kdef, n_isdf, ncv, nb, tda;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(mu_pad, cv_pad, mu_k, kdef, n_isdf, ncv, nb, tda) <
+           std::tie(o.mu_pad, o.cv_pad, o.mu_k, o.kdef, o.n_isdf, o.ncv, o.nb, o.tda);
+  }
+};
+struct TuneVal {
+  int bn1, var1, split1, bn2, var2;
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneVal> g_tune;
+
 // Chain buffers for nb chains and the tuned tile choice (bn1/bn2/split1 > 0
 // force a choice instead of tuning).
 int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
@@ -1064,7 +1082,22 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
       return encode_chain_maps(op, t[0], t[3]);
     }
   }
-  if (op->tuned_nb != nb) NGW_TRY(autotune(s, nb));
+  if (op->tuned_nb != nb) {
+    const TuneKey key{op->mu_pad, op->cv_pad, op->mu_k, op->kdef, op->n_isdf, op->ncv, nb, op->tda};
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      op->BN1 = it->second.bn1;
+      op->var1 = it->second.var1;
+      op->split1 = it->second.split1;
+      op->BN2 = it->second.bn2;
+      op->var2 = it->second.var2;
+      op->tuned_nb = nb;
+      return encode_chain_maps(op, op->BN1, op->BN2);
+    }
+    NGW_TRY(autotune(s, nb));
+    g_tune[key] = TuneVal{op->BN1, op->var1, op->split1, op->BN2, op->var2};
+  }
   return NGW_OK;
 }
 

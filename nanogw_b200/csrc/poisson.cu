@@ -196,3 +196,104 @@ extern "C" int ngw_build_coulomb_kernel(ngw_session *s, int ngrid, int n_isdf, c
   dfree(s, dg, (size_t)3 * ngrid * 4);
   return rc;
 }
+
+// ---------------------------------------------------------------------------
+// f_xc block of the ISDF kernel:  M_xc = ntrans/hcub * zeta^T (f_xc * zeta)
+// (shared/isdf_parallel_sym_UltraLowMem.F90:809-839).  f_xc is the
+// unpolarised LDA kernel of shared/xc_module.F90:853-893 (fxc_get, kflag 1/2):
+// 2 * (f_x + f_c) in Ry bohr^3, with f_x the analytic Slater exchange kernel
+// and f_c libxc's finite difference of the Perdew-Zunger potential
+// (LIB/libxc/src/lda.c:153-182, delta_rho = 1e-8, centred unless rho < 2 delta).
+namespace ngw {
+
+__device__ __forceinline__ double pz_vc(double rho) {
+  const double gamma = -0.1423, beta1 = 1.0529, beta2 = 0.3334;
+  const double a = 0.0311, b = -0.048, c = 0.0020, d = -0.0116;
+  const double rs = cbrt(3.0 / (4.0 * M_PI * rho));
+  if (rs >= 1.0) {
+    const double srs = sqrt(rs);
+    const double den = 1.0 + beta1 * srs + beta2 * rs;
+    const double ec = gamma / den;
+    return ec * (1.0 + 7.0 / 6.0 * beta1 * srs + 4.0 / 3.0 * beta2 * rs) / den;
+  }
+  const double lrs = log(rs);
+  return a * lrs + (b - a / 3.0) + 2.0 / 3.0 * c * rs * lrs + (2.0 * d - c) * rs / 3.0;
+}
+
+__global__ void k_fxc_lda(const double *__restrict__ rho, int n, double *__restrict__ fxc) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double r = rho[i];
+    const double eps_x = -0.75 * cbrt(3.0 / M_PI) * cbrt(r);
+    const double fx = 4.0 / 9.0 * eps_x / r;
+    const double dr = 1e-8;
+    double fc;
+    if (r < 2.0 * dr) fc = (pz_vc(r + dr) - pz_vc(r)) / dr;
+    else fc = (pz_vc(r + dr) - pz_vc(r - dr)) / (2.0 * dr);
+    fxc[i] = (fx + fc) * 2.0;
+  }
+}
+
+__global__ void k_scale_cols_by(const double *__restrict__ z, const double *__restrict__ f, int n,
+                                int ncol, double *__restrict__ out) {
+  const int col = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[(size_t)col * n + i] = f[i] * z[(size_t)col * n + i];
+}
+
+}  // namespace ngw
+
+extern "C" int ngw_build_fxc_kernel(ngw_session *s, int ngrid, int n_isdf, const double *zeta,
+                                    const double *rho, double h, double *mxc, double *fxc_out) {
+  using namespace ngw;
+  if (!s || ngrid <= 0 || n_isdf <= 0 || !zeta || !rho || h <= 0 || !mxc) {
+    set_error("ngw_build_fxc_kernel: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  for (int i = 0; i < ngrid; ++i)
+    if (!(rho[i] > 0.0) || !std::isfinite(rho[i])) {
+      set_error("ngw_build_fxc_kernel: density must be positive and finite (point %d)", i);
+      return NGW_ERR_NONFINITE;
+    }
+  NGW_CUDA(cudaSetDevice(s->device));
+  double *dz = nullptr, *dfz = nullptr, *drho = nullptr, *dfxc = nullptr, *dm = nullptr;
+  const size_t zb = (size_t)ngrid * n_isdf * 8;
+  int rc = NGW_OK;
+  do {
+    if (dalloc(s, (void **)&dz, zb) || dalloc(s, (void **)&dfz, zb) ||
+        dalloc(s, (void **)&drho, (size_t)ngrid * 8) || dalloc(s, (void **)&dfxc, (size_t)ngrid * 8) ||
+        dalloc(s, (void **)&dm, (size_t)n_isdf * n_isdf * 8)) {
+      rc = NGW_ERR_OOM;
+      break;
+    }
+    if (cudaMemcpyAsync(dz, zeta, zb, cudaMemcpyHostToDevice, s->stream) ||
+        cudaMemcpyAsync(drho, rho, (size_t)ngrid * 8, cudaMemcpyHostToDevice, s->stream)) {
+      set_error("copy to device failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    k_fxc_lda<<<std::min(1024, (ngrid + 255) / 256), 256, 0, s->stream>>>(drho, ngrid, dfxc);
+    k_scale_cols_by<<<dim3(std::min(256, (ngrid + 255) / 256), n_isdf), 256, 0, s->stream>>>(
+        dz, dfxc, ngrid, n_isdf, dfz);
+    const double nf = 1.0 / (h * h * h), zero = 0.0;
+    if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n_isdf, n_isdf, ngrid, &nf, dz, ngrid, dfz,
+                    ngrid, &zero, dm, n_isdf) != CUBLAS_STATUS_SUCCESS) {
+      set_error("cublasDgemm (zeta^T f zeta) failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    if (cudaMemcpyAsync(mxc, dm, (size_t)n_isdf * n_isdf * 8, cudaMemcpyDeviceToHost, s->stream) ||
+        (fxc_out && cudaMemcpyAsync(fxc_out, dfxc, (size_t)ngrid * 8, cudaMemcpyDeviceToHost, s->stream)) ||
+        cudaStreamSynchronize(s->stream)) {
+      set_error("copy back failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+  } while (0);
+  cudaStreamSynchronize(s->stream);
+  dfree(s, dz, zb);
+  dfree(s, dfz, zb);
+  dfree(s, drho, (size_t)ngrid * 8);
+  dfree(s, dfxc, (size_t)ngrid * 8);
+  dfree(s, dm, (size_t)n_isdf * n_isdf * 8);
+  return rc;
+}

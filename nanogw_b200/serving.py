@@ -1,0 +1,173 @@
+"""Continuous-batching request loop for Sigma_c solves.
+
+Requests (one molecule's ISDF operator + the QP states to solve) arrive over
+time; the server keeps a pool of workers, each a library session with its own
+CUDA stream, cuBLAS handle, graph cache and device-resident state (orbitals at
+the ISDF points, Coulomb kernel, pair products, split-BF16 operands, deflated
+eigenpairs, Lanczos vectors).  A request is admitted when a worker is free and
+the device memory it needs fits the budget next to everything already
+resident; it is routed to a worker that already holds its molecule when one is
+free (the operator then stays resident and is not re-uploaded).  Requests on
+different workers run concurrently on the device -- a new request starts as
+soon as a slot frees, it does not wait for a batch to form.
+
+Latency = finish - arrival; throughput = QP states solved per second.
+"""
+import heapq
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .api import RYD, Session
+
+
+@dataclass
+class SigmaRequest:
+    rid: int
+    mol_id: int
+    psi_intp: np.ndarray
+    mmtrx: np.ndarray
+    e1: np.ndarray
+    nval: int
+    qp_bands: np.ndarray
+    polynomial: np.ndarray
+    niter: int = 150
+    nen: int = 400
+    deltae: float = 4.0
+    ecuts: float = 0.02
+    sigx_ev: float = -12.0
+    vxc_ev: float = -10.0
+    arrival: float = 0.0
+    # filled in by the server
+    start: float = field(default=0.0)
+    finish: float = field(default=0.0)
+    worker: int = field(default=-1)
+    sigma: np.ndarray = field(default=None)
+    eqp: np.ndarray = field(default=None)
+
+    @property
+    def nmem(self):
+        return self.psi_intp.shape[1]
+
+    @property
+    def ncv(self):
+        return self.nval * (self.nmem - self.nval)
+
+    def footprint_bytes(self):
+        """Device memory the request needs: operator (FP64 + split-BF16 +
+        pair products) and Lanczos / Clenshaw state of all its chains."""
+        n, ncv, nb = self.psi_intp.shape[0], self.ncv, len(self.qp_bands) * self.nmem
+        op = 8 * (n * self.nmem + n * n + n * ncv) + 2 * 2 * 2 * (n + 64) * (ncv + 128)
+        chains = nb * ncv * (8 * 6 + 4 * 3 + 2 * 2) + nb * self.niter * 16 + nb * (self.nen + 1) * 16
+        return int(op + chains + (96 << 20))
+
+
+class SigmaServer:
+    def __init__(self, device=0, workers=2, precision="mixed", hbm_budget_gb=150.0, solver=None):
+        """`solver(worker, request)` replaces the device solve (host-logic tests)."""
+        self.device = device
+        self.precision = precision
+        self.budget = int(hbm_budget_gb * (1 << 30))
+        self.solver = solver
+        self.sessions = [] if solver else [Session(device, precision) for _ in range(workers)]
+        self.nworkers = workers
+        self.resident = [None] * workers          # mol_id held by each worker
+        self.peak_used = 0
+
+    def close(self):
+        for s in self.sessions:
+            s.close()
+
+    def _solve(self, w, req):
+        if self.solver:
+            self.solver(w, req)
+            self.resident[w] = req.mol_id
+            return
+        from .api import lowcomsym_pairs, sqrt_r
+        s = self.sessions[w]
+        if self.resident[w] != req.mol_id:
+            s.set_isdf(req.psi_intp, req.mmtrx)
+            cv = lowcomsym_pairs(req.nval, req.nmem)
+            s.set_pairs(cv, sqrt_r(req.e1, cv))
+            self.resident[w] = req.mol_id
+        sig = s.calculate_sigma_lanczos(req.e1, req.nval, req.qp_bands, req.nen, req.deltae, req.ecuts,
+                                        req.niter, req.polynomial)
+        e1 = req.e1[req.qp_bands - 1] * RYD
+        eqp, _, _ = s.qp_newton(sig * RYD, e1, e1, req.deltae * RYD, req.sigx_ev, req.vxc_ev)
+        req.sigma = sig
+        req.eqp = eqp
+
+    def run(self, requests, realtime=True):
+        """Serve `requests` (arrival times in seconds from the start).  With
+        realtime=False every request is available at t=0 (closed loop)."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        lock = threading.Condition()
+        free = list(range(self.nworkers))
+        inflight = {}
+        used = [0]
+        pending = []          # arrived, not admitted: heap of (arrival, rid, req)
+        t0 = time.perf_counter()
+        errors = []
+
+        def worker_done(w, req):
+            with lock:
+                req.finish = time.perf_counter() - t0
+                free.append(w)
+                used[0] -= req.footprint_bytes()
+                del inflight[req.rid]
+                lock.notify_all()
+
+        def work(w, req):
+            try:
+                self._solve(w, req)
+            except Exception as e:       # keep serving; report at the end
+                errors.append((req.rid, repr(e)))
+            worker_done(w, req)
+
+        threads = []
+        i = 0
+        with lock:
+            while i < len(reqs) or pending or inflight:
+                now = time.perf_counter() - t0
+                while i < len(reqs) and (not realtime or reqs[i].arrival <= now):
+                    heapq.heappush(pending, (reqs[i].arrival, reqs[i].rid, reqs[i]))
+                    i += 1
+                admitted = False
+                while pending and free:
+                    _, _, req = pending[0]
+                    need = req.footprint_bytes()
+                    if used[0] + need > self.budget and inflight:
+                        break
+                    heapq.heappop(pending)
+                    # prefer a free worker that already holds this molecule
+                    w = next((x for x in free if self.resident[x] == req.mol_id), free[0])
+                    free.remove(w)
+                    used[0] += need
+                    self.peak_used = max(self.peak_used, used[0])
+                    inflight[req.rid] = req
+                    req.start = time.perf_counter() - t0
+                    req.worker = w
+                    th = threading.Thread(target=work, args=(w, req), daemon=True)
+                    threads.append(th)
+                    th.start()
+                    admitted = True
+                if admitted:
+                    continue
+                if i < len(reqs) and realtime:
+                    timeout = max(0.0, reqs[i].arrival - (time.perf_counter() - t0))
+                    lock.wait(timeout=timeout if timeout > 0 else 0.0005)
+                else:
+                    lock.wait(timeout=0.05)
+        for th in threads:
+            th.join()
+        wall = time.perf_counter() - t0
+        if errors:
+            raise RuntimeError(f"{len(errors)} requests failed, first: {errors[0]}")
+        lat = np.array([r.finish - r.arrival for r in reqs])
+        solves = sum(len(r.qp_bands) for r in reqs)
+        return {"requests": len(reqs), "solves": solves, "wall_s": wall,
+                "solves_per_s": solves / wall,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3)}

@@ -172,6 +172,18 @@ def test_coulomb_kernel_build(small_system):
     assert _rel(got, ref) < 1e-11
 
 
+def test_fxc_kernel_build(small_system):
+    from oracle import fxc as OF
+    S = small_system
+    mol = S.mol
+    with ngw.Session(0) as s:
+        mxc, f = s.build_fxc_kernel(S.zeta, mol.rho, mol.h, return_fxc=True)
+    fref = OF.fxc_lda(mol.rho)
+    assert np.max(np.abs(f - fref) / np.abs(fref)) < 1e-6
+    _, ref = OI.kernel_mmtrx(S.zeta, S.zeta, mol.hcub, fxc=fref)
+    assert _rel(mxc, ref) < 1e-6
+
+
 def test_errors_are_codes(small_system):
     S = small_system
     with ngw.Session(0) as s:
