@@ -166,12 +166,14 @@ static int lanczos_dev(ngw_session *s, const PolyPlan &pp, int nb, int niter, do
   // wvec = p(H) vec
   NGW_TRY(apply_poly(s, pp, nb, V, hs, W));
   launch_lanczos_first(W, V, s->ncv, nb, a, b, niter, s->stream);
+  // the scaled copy hs feeds only the FP64 path's first DGEMM
+  double *hsn = (s->precision == NGW_PREC_MIXED) ? nullptr : hs;
   if (niter >= 2)
-    launch_lanczos_prescale(W, V, s->ncv, nb, 1, b, niter, s->d_sqrtR, hs, pp.tamm_d, s->stream);
+    launch_lanczos_prescale(W, V, s->ncv, nb, 1, b, niter, s->d_sqrtR, hsn, pp.tamm_d, s->stream);
   double *vec = W, *wvec = V;   // roles after the swap
   for (int k = 1; k < niter; ++k) {
     NGW_TRY(apply_poly(s, pp, nb, vec, hs, tmp));
-    launch_lanczos_step(wvec, vec, tmp, s->ncv, nb, k, a, b, niter, s->d_sqrtR, hs, pp.tamm_d,
+    launch_lanczos_step(wvec, vec, tmp, s->ncv, nb, k, a, b, niter, s->d_sqrtR, hsn, pp.tamm_d,
                         (k + 1 < niter) ? 1 : 0, s->stream);
     if (k + 1 < niter) {
       double *t = vec;

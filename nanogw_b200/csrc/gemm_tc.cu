@@ -53,8 +53,12 @@ struct EpiParams {
   const double *s;       // sqrtR (Mv)
   const float *x;        // b_{k+1}  [n * ldx + m]
   const float *b2;       // b_{k+2}  (nullable)
-  const double *v;       // Lanczos vector [n * ldv + m]
-  int ldx, ldv;
+  const float *v;        // the vector p is applied to (deflated), FP32 [n * ldx + m]
+  int ldx, ldv;          // ldv: leading dimension of out64
+  // final step only: out64 += Up(m, :) . xo(:, n) (deflated eigenpairs, FP64)
+  const double *Up;      // (ncv, kdef) column-major
+  const double *xo;      // (kdef, nb) column-major
+  int kdef;
   double gamma, alpha, c0, beta;
   int tda;
   float *out32;          // b_k (nullable)
@@ -235,7 +239,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         const size_t o = (size_t)(nbase + j) * ep.ldx + m;
         xv[j] = (j < nj) ? __ldg(ep.x + o) : 0.f;
         b2v[j] = (j < nj && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
-        vv[j] = (j < nj && ep.v) ? __ldg(ep.v + (size_t)(nbase + j) * ep.ldv + m) : 0.0;
+        vv[j] = (j < nj && ep.v) ? (double)__ldg(ep.v + o) : 0.0;
       }
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
@@ -245,7 +249,12 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         const double y = ep.tda ? (s2 * x + 2.0 * (double)z[j]) : (s2 * s2 * x + 4.0 * si * (double)z[j]);
         const double o = ep.gamma * vv[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
         if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = (float)o;
-        if (ep.out64) ep.out64[(size_t)n * ep.ldv + m] = o;
+        if (ep.out64) {
+          double od = o;
+          for (int q = 0; q < ep.kdef; ++q)
+            od += ep.Up[(size_t)q * ep.Mv + m] * ep.xo[(size_t)n * ep.kdef + q];
+          ep.out64[(size_t)n * ep.ldv + m] = od;
+        }
         if (ep.s_hi) {
           bf16 hi, lo;
           split_bf16((float)(sc * o), hi, lo);
@@ -454,7 +463,7 @@ __global__ void __launch_bounds__(PTHREADS, 1)
             const size_t o = (size_t)(nbase + j) * ep.ldx + m;
             xv[j] = (j < nj) ? __ldg(ep.x + o) : 0.f;
             b2v[j] = (j < nj && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
-            vv[j] = (j < nj && ep.v) ? __ldg(ep.v + (size_t)(nbase + j) * ep.ldv + m) : 0.0;
+            vv[j] = (j < nj && ep.v) ? (double)__ldg(ep.v + o) : 0.0;
           }
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
@@ -464,7 +473,12 @@ __global__ void __launch_bounds__(PTHREADS, 1)
             const double y = ep.tda ? (s2 * x + 2.0 * (double)z[j]) : (s2 * s2 * x + 4.0 * si * (double)z[j]);
             const double o = ep.gamma * vv[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
             if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = (float)o;
-            if (ep.out64) ep.out64[(size_t)n * ep.ldv + m] = o;
+            if (ep.out64) {
+              double od = o;
+              for (int q = 0; q < ep.kdef; ++q)
+                od += ep.Up[(size_t)q * ep.Mv + m] * ep.xo[(size_t)n * ep.kdef + q];
+              ep.out64[(size_t)n * ep.ldv + m] = od;
+            }
             if (ep.s_hi) {
               bf16 hi, lo;
               split_bf16((float)(sc * o), hi, lo);
@@ -727,13 +741,19 @@ __global__ void k_split_rows(const double *__restrict__ D, int n_isdf, int ncv,
   }
 }
 
-// Clenshaw start: b_n = g * v (FP32) and split((R^1/2 or 1) * b_n)
-__global__ void k_cheb_start(const double *__restrict__ v, int ldv, const double *__restrict__ s,
-                             int ncv, int nb, double g, int tda, float *__restrict__ bn, int ldx,
-                             bf16 *__restrict__ shi, bf16 *__restrict__ slo, int lds) {
+// Clenshaw start: v_perp = v - U xo (deflated part, stored FP32), b_n = g v_perp
+// (FP32) and split((R^1/2 or 1) * b_n) for the first GEMM1.
+__global__ void k_cheb_start(const double *__restrict__ v, int ldv, const double *__restrict__ U,
+                             const double *__restrict__ xo, int kdef, const double *__restrict__ s,
+                             int ncv, int nb, double g, int tda, float *__restrict__ vp,
+                             float *__restrict__ bn, int ldx, bf16 *__restrict__ shi,
+                             bf16 *__restrict__ slo, int lds) {
   const int j = blockIdx.y;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
-    const double b = g * v[(size_t)j * ldv + i];
+    double x = v[(size_t)j * ldv + i];
+    for (int q = 0; q < kdef; ++q) x -= U[(size_t)q * ncv + i] * xo[(size_t)j * kdef + q];
+    vp[(size_t)j * ldx + i] = (float)x;
+    const double b = g * x;
     bn[(size_t)j * ldx + i] = (float)b;
     const double u = tda ? b : s[i] * b;
     bf16 h, l;
@@ -761,7 +781,8 @@ struct MixedOperator {
   bf16 *S_hi = nullptr, *S_lo = nullptr, *T_hi = nullptr, *T_lo = nullptr;
   CUtensorMap tShi, tSlo, tThi, tTlo;
   float *bb[3] = {nullptr, nullptr, nullptr};
-  double *vperp = nullptr, *xo = nullptr;
+  float *vperp = nullptr;
+  double *xo = nullptr;
   float *ws = nullptr;
   size_t buf_bytes = 0;
 };
@@ -776,7 +797,8 @@ static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
   op->S_hi = op->S_lo = op->T_hi = op->T_lo = nullptr;
   op->bb[0] = op->bb[1] = op->bb[2] = nullptr;
   op->ws = nullptr;
-  op->vperp = op->xo = nullptr;
+  op->vperp = nullptr;
+  op->xo = nullptr;
   s->bytes -= op->buf_bytes;
   op->buf_bytes = 0;
   op->nb_cap = 0;
@@ -921,9 +943,9 @@ static int encode_chain_maps(MixedOperator *op, int bn1, int bn2) {
 }
 
 static int run_gemm1(ngw_session *s, int nb);
-static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, const double *v,
+static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, const float *v,
                      int ldv, double gamma, double alpha, double c0, double beta, int tda,
-                     float *out32, double *out64, bool write_split);
+                     float *out32, double *out64, bool write_split, bool add_defl = false);
 
 // Autotuner: time every admissible (N tile, variant, split-K) for GEMM1 and
 // (N tile, variant) for GEMM2 on the session's buffers and keep the fastest.
@@ -1037,7 +1059,7 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
     const size_t sbytes = (size_t)nbp * op->cv_pad * sizeof(bf16);
     const size_t tbytes = (size_t)nbp * op->mu_k * sizeof(bf16);
     const size_t bbytes = (size_t)nbp * op->cv_pad * sizeof(float);
-    const size_t vbytes = (size_t)nbp * s->ncv * sizeof(double);
+    const size_t vbytes = (size_t)nbp * op->cv_pad * sizeof(float);
     const size_t xbytes = (size_t)nbp * std::max(op->kdef, 1) * sizeof(double);
     // split-K partials: enough for 16 splits of the smallest tile grid
     const size_t wsbytes = (size_t)(op->mu_pad / BM) * ((nbp + 63) / 64) * 16 * 64 * BM * sizeof(float);
@@ -1131,9 +1153,9 @@ static int run_gemm1(ngw_session *s, int nb) {
 }
 
 // One GEMM2 with the Clenshaw epilogue.
-static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, const double *v,
+static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, const float *v,
                      int ldv, double gamma, double alpha, double c0, double beta, int tda,
-                     float *out32, double *out64, bool write_split) {
+                     float *out32, double *out64, bool write_split, bool add_defl) {
   MixedOperator *op = s->mixed;
   GemmArgs ga;
   ga.num_kb = op->mu_k / BK;
@@ -1160,6 +1182,11 @@ static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, co
   ep.s_hi = write_split ? op->S_hi : nullptr;
   ep.s_lo = write_split ? op->S_lo : nullptr;
   ep.lds = op->cv_pad;
+  if (add_defl && op->kdef > 0) {
+    ep.Up = op->Up;
+    ep.xo = op->xo;
+    ep.kdef = op->kdef;
+  }
   const int tiles_m = op->cv_pad / BM;
   const int tiles_n = (nb + op->BN2 - 1) / op->BN2;
   return dispatch_tc(op->BN2, op->var2, op->tA3hi, op->tA3lo, op->tThi, op->tTlo, tiles_m, tiles_n,
@@ -1182,45 +1209,33 @@ int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const dou
   }
   cudaStream_t st = s->stream;
   const int ncv = s->ncv, k = op->kdef;
-  const double one = 1.0, mone = -1.0, zero = 0.0;
-  const double *vin = v;
-  int ldin = ldv;
-  if (k > 0) {
-    // xo = U^T v ; vperp = v - U xo
+  const double one = 1.0, zero = 0.0;
+  if (k > 0)   // xo = U^T v (FP64); v_perp and the U p(Lambda) xo term are fused below
     NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, k, nb, ncv, &one, s->eig_U, ncv, v, ldv,
                            &zero, op->xo, k));
-    NGW_CUDA(cudaMemcpy2DAsync(op->vperp, (size_t)ncv * 8, v, (size_t)ldv * 8, (size_t)ncv * 8, nb,
-                               cudaMemcpyDeviceToDevice, st));
-    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, ncv, nb, k, &mone, s->eig_U, ncv, op->xo,
-                           k, &one, op->vperp, ncv));
-    vin = op->vperp;
-    ldin = ncv;
-  }
   {
     int bx = (ncv + 255) / 256;
     if (bx > 16) bx = 16;
-    k_cheb_start<<<dim3(bx, nb), 256, 0, st>>>(vin, ldin, s->d_sqrtR, ncv, nb, g[n], tda, op->bb[0],
-                                              op->cv_pad, op->S_hi, op->S_lo, op->cv_pad);
+    k_cheb_start<<<dim3(bx, nb), 256, 0, st>>>(v, ldv, s->eig_U, op->xo, k, s->d_sqrtR, ncv, nb, g[n],
+                                              tda, op->vperp, op->bb[0], op->cv_pad, op->S_hi,
+                                              op->S_lo, op->cv_pad);
     NGW_CUDA(cudaGetLastError());
   }
+  const float *vin = op->vperp;
   int cur = 0, prev = -1;   // slots of b_{k+1}, b_{k+2}
   for (int kk = n - 1; kk >= 1; --kk) {
     NGW_TRY(run_gemm1(s, nb));
     // b_k goes to the slot that is neither b_{k+1} nor b_{k+2}
     const int outb = (prev < 0) ? 1 : 3 - cur - prev;
-    NGW_TRY(run_gemm2(s, nb, op->bb[cur], prev < 0 ? nullptr : op->bb[prev], vin, ldin, g[kk],
+    NGW_TRY(run_gemm2(s, nb, op->bb[cur], prev < 0 ? nullptr : op->bb[prev], vin, ldv, g[kk],
                       2.0 / c1, c0, 1.0, tda, op->bb[outb], nullptr, true));
     prev = cur;
     cur = outb;
   }
   NGW_TRY(run_gemm1(s, nb));
-  NGW_TRY(run_gemm2(s, nb, op->bb[cur], prev < 0 ? nullptr : op->bb[prev], vin, ldin, g[0],
-                    1.0 / c1, c0, 1.0, tda, nullptr, out64, false));
-  if (k > 0) {
-    // out += U p(Lambda) xo
-    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, ncv, nb, k, &one, op->Up, ncv, op->xo,
-                           k, &one, out64, ldv));
-  }
+  // final step: p(C) v = g_0 v_perp + Chat b_1 - b_2 + U p(Lambda) xo
+  NGW_TRY(run_gemm2(s, nb, op->bb[cur], prev < 0 ? nullptr : op->bb[prev], vin, ldv, g[0],
+                    1.0 / c1, c0, 1.0, tda, nullptr, out64, false, true));
   return NGW_OK;
 }
 

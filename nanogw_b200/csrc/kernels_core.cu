@@ -198,7 +198,7 @@ __device__ __forceinline__ void prescale_chain(double *w, double *v, int ncv, do
     double wi = w[i] / bk;
     w[i] = wi;
     v[i] = -v[i] * bk;
-    hs[i] = tamm_d ? wi : s[i] * wi;
+    if (hs) hs[i] = tamm_d ? wi : s[i] * wi;
   }
 }
 
@@ -237,8 +237,8 @@ __global__ void k_lanczos_prescale(double *__restrict__ w, double *__restrict__ 
                                    int tamm_d) {
   const int j = blockIdx.x;
   const double bk = b[(size_t)j * niter + k];
-  prescale_chain(w + (size_t)j * ncv, v + (size_t)j * ncv, ncv, bk, s, hs + (size_t)j * ncv,
-                 tamm_d);
+  prescale_chain(w + (size_t)j * ncv, v + (size_t)j * ncv, ncv, bk, s,
+                 hs ? hs + (size_t)j * ncv : nullptr, tamm_d);
 }
 
 void launch_lanczos_prescale(double *w, double *v, int ncv, int nb, int k, const double *b,
@@ -278,7 +278,7 @@ __global__ void k_lanczos_step(double *__restrict__ w, double *__restrict__ v,
     }
     const double bk1 = sqrt(block_sum<LNT>(acc, sh));
     if (threadIdx.x == 0) b[(size_t)j * niter + k + 1] = bk1;
-    if (prescale_next) prescale_chain(wj, vj, ncv, bk1, s, hs + (size_t)j * ncv, tamm_d);
+    if (prescale_next) prescale_chain(wj, vj, ncv, bk1, s, hs ? hs + (size_t)j * ncv : nullptr, tamm_d);
   }
 }
 
