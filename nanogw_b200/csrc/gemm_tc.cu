@@ -635,7 +635,7 @@ static bool has_persistent(int BN) { return BN <= 160; }
 // per SM with a long TMA ring; variant 1 ("shallow", N <= 160): 3-4 stages
 // and <= 128 registers so two CTAs share an SM and one CTA's epilogue
 // overlaps the other's main loop.
-static const int kBNs[] = {64, 80, 96, 128, 144, 160, 192, 240, 256};
+static const int kBNs[] = {32, 48, 64, 80, 96, 128, 144, 160, 192, 240, 256};
 
 static bool has_shallow(int BN) { return BN <= 160; }
 
@@ -648,6 +648,8 @@ static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorM
   return launch_tc_p<BNV, ST>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st)
   if (var == 2) {
     switch (BN) {
+      case 32: NGW_TCP(32, 4);
+      case 48: NGW_TCP(48, 4);
       case 64: NGW_TCP(64, 4);
       case 80: NGW_TCP(80, 4);
       case 96: NGW_TCP(96, 4);
@@ -659,6 +661,8 @@ static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorM
 #undef NGW_TCP
   if (var == 0) {
     switch (BN) {
+      case 32: NGW_TC(32, 8, 1);
+      case 48: NGW_TC(48, 8, 1);
       case 64: NGW_TC(64, 8, 1);
       case 80: NGW_TC(80, 8, 1);
       case 96: NGW_TC(96, 7, 1);
@@ -671,6 +675,8 @@ static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorM
     }
   } else {
     switch (BN) {
+      case 32: NGW_TC(32, 4, 2);
+      case 48: NGW_TC(48, 4, 2);
       case 64: NGW_TC(64, 4, 2);
       case 80: NGW_TC(80, 4, 2);
       case 96: NGW_TC(96, 3, 2);
