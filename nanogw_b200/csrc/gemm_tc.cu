@@ -82,14 +82,16 @@ constexpr int NTHREADS = 256;
 
 // Epilogue loads for one 16-column chunk, issued before any arithmetic so the
 // global-memory latencies overlap.
-template <int BN, int STAGES, int MINB>
+template <int BN, int STAGES, int MINB, bool FUSED>
 __global__ void __launch_bounds__(NTHREADS, MINB)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
               const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
               GemmArgs ga, EpiParams ep, int *status) {
+  // FUSED: one stage holds A_hi, A_lo, B_hi, B_lo of a k-block and carries all
+  // three split products; otherwise one stage is one (A, B) pair of a segment.
   constexpr uint32_t A_BYTES = BM * BK * 2;
   constexpr uint32_t B_BYTES = BN * BK * 2;
-  constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
+  constexpr uint32_t STAGE_BYTES = FUSED ? 2 * (A_BYTES + B_BYTES) : A_BYTES + B_BYTES;
   constexpr uint32_t TMEM_COLS = (BN <= 32) ? 32 : (BN <= 64) ? 64 : (BN <= 128) ? 128 : 256;
   constexpr uint32_t IDESC = tc::idesc_bf16_f32(BM, BN);
   constexpr int NCH = BN / 16;             // 16-column chunks
@@ -106,7 +108,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int split = blockIdx.z;
-  const int total_kb = ga.num_kb * ga.nseg;
+  const int total_kb = FUSED ? ga.num_kb : ga.num_kb * ga.nseg;
   const int kb_per = (total_kb + ga.nsplit - 1) / ga.nsplit;
   const int kb_begin = split * kb_per;
   const int kb_end = min(total_kb, kb_begin + kb_per);
@@ -141,15 +143,22 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         if (!tc::mbar_wait(tc::smem_u32(&empty_bar[s]), ((i / STAGES) - 1) & 1, status)) break;
       }
       const int kbg = kb_begin + i;
-      const int seg = kbg / ga.num_kb;
-      const int kb = kbg - seg * ga.num_kb;
-      const CUtensorMap *ta = (seg == 2) ? &tA_lo : &tA_hi;   // (hi,hi) (hi,lo) (lo,hi)
-      const CUtensorMap *tb = (seg == 1) ? &tB_lo : &tB_hi;
       const uint32_t bar = tc::smem_u32(&full_bar[s]);
       const uint32_t sa = tc::smem_u32(smem + s * STAGE_BYTES);
       tc::mbar_arrive_expect_tx(bar, STAGE_BYTES);
-      tc::tma_load_2d(sa, ta, bar, kb * BK, m0);
-      tc::tma_load_2d(sa + A_BYTES, tb, bar, kb * BK, n0);
+      if (FUSED) {
+        tc::tma_load_2d(sa, &tA_hi, bar, kbg * BK, m0);
+        tc::tma_load_2d(sa + A_BYTES, &tA_lo, bar, kbg * BK, m0);
+        tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kbg * BK, n0);
+        tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kbg * BK, n0);
+      } else {
+        const int seg = kbg / ga.num_kb;
+        const int kb = kbg - seg * ga.num_kb;
+        const CUtensorMap *ta = (seg == 2) ? &tA_lo : &tA_hi;   // (hi,hi) (hi,lo) (lo,hi)
+        const CUtensorMap *tb = (seg == 1) ? &tB_lo : &tB_hi;
+        tc::tma_load_2d(sa, ta, bar, kb * BK, m0);
+        tc::tma_load_2d(sa + A_BYTES, tb, bar, kb * BK, n0);
+      }
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer (single thread) ----
@@ -158,12 +167,23 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
       if (!tc::mbar_wait(tc::smem_u32(&full_bar[s]), (i / STAGES) & 1, status)) break;
       tc::tc_fence_after();
       const uint32_t sa = tc::smem_u32(smem + s * STAGE_BYTES);
-      const uint32_t sb = sa + A_BYTES;
+      if (FUSED) {
+        const uint32_t sal = sa + A_BYTES, sbh = sa + 2 * A_BYTES, sbl = sbh + B_BYTES;
 #pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk) {
-        const uint64_t ad = tc::smem_desc_sw128(sa + kk * 32);
-        const uint64_t bd = tc::smem_desc_sw128(sb + kk * 32);
-        tc::mma_bf16(tmem_d, ad, bd, IDESC, (i > 0 || kk > 0) ? 1u : 0u);
+        for (int kk = 0; kk < BK / 16; ++kk) {
+          const uint32_t acc0 = (i > 0 || kk > 0) ? 1u : 0u;
+          tc::mma_bf16(tmem_d, tc::smem_desc_sw128(sa + kk * 32), tc::smem_desc_sw128(sbh + kk * 32), IDESC, acc0);
+          tc::mma_bf16(tmem_d, tc::smem_desc_sw128(sa + kk * 32), tc::smem_desc_sw128(sbl + kk * 32), IDESC, 1u);
+          tc::mma_bf16(tmem_d, tc::smem_desc_sw128(sal + kk * 32), tc::smem_desc_sw128(sbh + kk * 32), IDESC, 1u);
+        }
+      } else {
+        const uint32_t sb = sa + A_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk) {
+          const uint64_t ad = tc::smem_desc_sw128(sa + kk * 32);
+          const uint64_t bd = tc::smem_desc_sw128(sb + kk * 32);
+          tc::mma_bf16(tmem_d, ad, bd, IDESC, (i > 0 || kk > 0) ? 1u : 0u);
+        }
       }
       tc::mma_commit(tc::smem_u32(&empty_bar[s]));
     }
@@ -592,20 +612,20 @@ static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, siz
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
-template <int BN, int STAGES, int MINB>
+template <int BN, int STAGES, int MINB, bool FUSED = false>
 static int launch_tc(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
                      const CUtensorMap &b_lo, int tiles_m, int tiles_n, const GemmArgs &ga,
                      const EpiParams &ep, int *status, cudaStream_t st) {
-  constexpr size_t smem = (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) + 1024;
+  constexpr size_t smem = (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) * (FUSED ? 2 : 1) + 1024;
   static bool attr = false;
   if (!attr) {
-    NGW_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, MINB>,
+    NGW_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, MINB, FUSED>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
   }
   dim3 grid(tiles_m, tiles_n, ga.nsplit);
-  NGW_CUDA(launch_pdl(k_tc_gemm<BN, STAGES, MINB>, grid, dim3(NTHREADS), smem, st, a_hi, a_lo, b_hi,
-                      b_lo, ga, ep, status));
+  NGW_CUDA(launch_pdl(k_tc_gemm<BN, STAGES, MINB, FUSED>, grid, dim3(NTHREADS), smem, st, a_hi, a_lo,
+                      b_hi, b_lo, ga, ep, status));
   return NGW_OK;
 }
 
@@ -630,6 +650,8 @@ static int launch_tc_p(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const C
 }
 
 static bool has_persistent(int BN) { return BN <= 160; }
+static bool has_fused(int BN) { return BN <= 128; }
+static bool has_fused2(int BN) { return BN <= 64; }
 
 // Supported N tiles (multiples of 16, <= 256).  Variant 0 ("deep"): one CTA
 // per SM with a long TMA ring; variant 1 ("shallow", N <= 160): 3-4 stages
@@ -659,6 +681,26 @@ static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorM
     }
   }
 #undef NGW_TCP
+#define NGW_TCF(BNV, ST, MB) \
+  return launch_tc<BNV, ST, MB, true>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st)
+  if (var == 3) {
+    switch (BN) {
+      case 32: NGW_TCF(32, 5, 1);
+      case 48: NGW_TCF(48, 4, 1);
+      case 64: NGW_TCF(64, 4, 1);
+      case 80: NGW_TCF(80, 4, 1);
+      case 96: NGW_TCF(96, 3, 1);
+      case 128: NGW_TCF(128, 3, 1);
+    }
+  }
+  if (var == 4) {
+    switch (BN) {
+      case 32: NGW_TCF(32, 2, 2);
+      case 48: NGW_TCF(48, 2, 2);
+      case 64: NGW_TCF(64, 2, 2);
+    }
+  }
+#undef NGW_TCF
   if (var == 0) {
     switch (BN) {
       case 32: NGW_TC(32, 8, 1);
@@ -977,11 +1019,13 @@ static int autotune(ngw_session *s, int nb) {
     if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
     const int waste = round_up(nb, bn) - nb;
     if (waste * 8 > nb && bn != kBNs[0]) continue;     // at most 12.5% padding
-    for (int var = 0; var < 3; ++var) {
+    for (int var = 0; var < 5; ++var) {
       if (var == 1 && !has_shallow(bn)) continue;
       if (var == 2 && !has_persistent(bn)) continue;
+      if (var == 3 && !has_fused(bn)) continue;
+      if (var == 4 && !has_fused2(bn)) continue;
       const int tiles = tiles_m1 * ((nb + bn - 1) / bn);
-      const int tkb = (var == 2) ? total_kb1 / 3 : total_kb1;
+      const int tkb = (var >= 2) ? total_kb1 / 3 : total_kb1;
       for (int sp : {1, 2, 3, 4, 6, 8, 12, 16}) {
         if (sp > 1 && tkb / sp < 3) break;
         if ((size_t)tiles * sp * bn * BM * sizeof(float) > op->ws_bytes && sp > 1) break;
