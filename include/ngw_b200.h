@@ -32,6 +32,9 @@
  *   ngw_build_coulomb_kernel      -- Mmtrx build, shared/isdf_parallel_sym_UltraLowMem.F90:687-889
  *                                    (dpoisson shared/fft_module.F90z:122,
  *                                     dcreate_coul_0D shared/fft_module.F90z:628)
+ *   ngw_build_fxc_kernel          -- f_xc block, shared/isdf_parallel_sym_UltraLowMem.F90:809-839
+ *   ngw_build_isdf_kernel         -- ISDF fit + both kernel blocks on the device,
+ *                                    shared/isdf_parallel_sym_UltraLowMem.F90:439-889
  */
 #ifndef NGW_B200_H
 #define NGW_B200_H
@@ -174,6 +177,20 @@ int ngw_build_coulomb_kernel(ngw_session *s, int ngrid, int n_isdf, const double
  * fxc_out (ngrid) optional. */
 int ngw_build_fxc_kernel(ngw_session *s, int ngrid, int n_isdf, const double *zeta,
                          const double *rho, double h, double *mxc, double *fxc_out);
+
+/* ISDF fit and kernel on the device (shared/isdf_parallel_sym_UltraLowMem.F90:439-889):
+ * psi (ngrid x nmem) orbitals on the grid, intp (n_isdf) 1-based grid indices
+ * of the interpolation points (after ngw_dedup_points), mv = highest band of
+ * the "valence" product P (max(nval, QP bands)).  Fits zeta from
+ *   P = psi_intp[:, :mv] psi[:, :mv]^T,  Q = psi_intp psi^T,
+ *   A = P_intp * Q_intp,  B = P * Q,  A zeta^T = B  (LU, partial pivoting)
+ * and builds M_C (and M_xc when rho != NULL) without copying zeta to the host.
+ * Out: psi_intp (n_isdf x nmem), mmtrx (n_isdf x n_isdf), mxc (same; needed
+ * when rho is given).  A singular A (repeated points) returns NGW_ERR_ARG. */
+int ngw_build_isdf_kernel(ngw_session *s, int ngrid, int nmem, const double *psi,
+                          const int *grid_idx, int n_isdf, const int *intp, int mv, int nfft,
+                          double h, double trunc, const double *rho, double *psi_intp,
+                          double *mmtrx, double *mxc);
 
 #ifdef __cplusplus
 }

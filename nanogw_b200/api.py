@@ -199,6 +199,22 @@ class Session:
         check(lib().ngw_build_fxc_kernel(self._h, ngrid, n_isdf, _p(zt), _p(r), float(h), _p(m), _p(f)))
         return (m, f) if return_fxc else m
 
+    def build_isdf_kernel(self, psi, grid_idx, intp, mv, nfft, h, trunc, rho=None):
+        """ISDF fit + kernel blocks on the device.  Returns (psi_intp, M_C, M_xc or None)."""
+        ps = _f64(psi)
+        g = np.ascontiguousarray(grid_idx, dtype=np.int32)
+        ip = np.ascontiguousarray(intp, dtype=np.int32)
+        ngrid, nmem = ps.shape
+        n_isdf = len(ip)
+        pi = np.zeros((n_isdf, nmem), order="F")
+        m = np.zeros((n_isdf, n_isdf), order="F")
+        r = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64)
+        mx = None if rho is None else np.zeros((n_isdf, n_isdf), order="F")
+        check(lib().ngw_build_isdf_kernel(self._h, ngrid, nmem, _p(ps), _p(g), n_isdf, _p(ip), int(mv),
+                                          int(nfft), float(h), float(trunc), _p(r), _p(pi), _p(m),
+                                          _p(mx)))
+        return pi, m, mx
+
     def build_coulomb_kernel(self, zeta, grid_idx, nfft, h, trunc):
         zt = _f64(zeta)
         g = np.ascontiguousarray(grid_idx, dtype=np.int32)

@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels_core.cu", "gemm_tc.cu", "deflate.cu", "abi.cu", "poisson.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels_core.cu", "gemm_tc.cu", "deflate.cu", "abi.cu", "poisson.cu", "noalloc.cu", "isdf_fit.cu"]
 CXX_SOURCES = ["host_setup.cpp"]
 
 
@@ -58,7 +58,7 @@ def build(verbose=False, force=False):
                   "-I", os.path.join(CUDA_HOME, "include"), "-c", s, "-o", o], verbose)
     if force or _stale(OUT, objs):
         tmp = OUT + ".tmp"
-        _run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcublas", "-lcufft", "-lcudart",
+        _run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcublas", "-lcufft", "-lcusolver", "-lcudart",
               "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64")], verbose)
         shutil.move(tmp, OUT)
     return OUT

@@ -78,6 +78,91 @@ __global__ void k_mul_coulomb(cufftDoubleComplex *__restrict__ f, const double *
   }
 }
 
+
+// M = (ntrans / hcub) zeta^T (v_c zeta) from a device-resident zeta
+// (ngrid x n_isdf, column-major) and grid coordinates (3 x ngrid).
+int coulomb_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const int *dg, int nfft,
+                 double h, double trunc, double *dm) {
+  const int n = nfft;
+  const size_t bsz = (size_t)n * n * n;
+  const size_t csz = (size_t)n * n * (n / 2 + 1);
+  // batch so that the boxes stay under ~2 GB
+  int batch = (int)std::max<size_t>(1, (size_t)(2ull << 30) / (bsz * 8 + csz * 16));
+  if (batch > n_isdf) batch = n_isdf;
+  double *dvz = nullptr, *box = nullptr, *vtab = nullptr;
+  cufftDoubleComplex *spec = nullptr;
+  int rc = NGW_OK;
+  cufftHandle pf = 0, pb = 0;
+  bool have_pf = false, have_pb = false;
+  do {
+    if (dalloc(s, (void **)&dvz, (size_t)ngrid * n_isdf * 8) || dalloc(s, (void **)&box, bsz * batch * 8) ||
+        dalloc(s, (void **)&spec, csz * batch * 16) || dalloc(s, (void **)&vtab, csz * 8)) {
+      rc = NGW_ERR_OOM;
+      break;
+    }
+    const double b = 2.0 * M_PI / ((double)n * h);
+    k_coulomb_table<<<1024, 256, 0, s->stream>>>(vtab, n, b, trunc);
+    int dims[3] = {n, n, n};
+    if (cufftPlanMany(&pf, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, batch) != CUFFT_SUCCESS) {
+      set_error("cufftPlanMany D2Z failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    have_pf = true;
+    if (cufftPlanMany(&pb, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, batch) != CUFFT_SUCCESS) {
+      set_error("cufftPlanMany Z2D failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    have_pb = true;
+    cufftSetStream(pf, s->stream);
+    cufftSetStream(pb, s->stream);
+    const double scale = 1.0 / ((double)n * (double)n * (double)n);
+    for (int c0 = 0; c0 < n_isdf && rc == NGW_OK; c0 += batch) {
+      const int nc = std::min(batch, n_isdf - c0);
+      cudaMemsetAsync(box, 0, bsz * batch * 8, s->stream);
+      int bx = (ngrid + 255) / 256;
+      if (bx > 256) bx = 256;
+      k_pack<<<dim3(bx, nc), 256, 0, s->stream>>>(dz + (size_t)c0 * ngrid, ngrid, ngrid, dg, n, box, nc);
+      if (cufftExecD2Z(pf, box, spec) != CUFFT_SUCCESS) {
+        set_error("cufftExecD2Z failed");
+        rc = NGW_ERR_CUDA;
+        break;
+      }
+      k_mul_coulomb<<<2048, 256, 0, s->stream>>>(spec, vtab, csz, batch);
+      if (cufftExecZ2D(pb, spec, box) != CUFFT_SUCCESS) {
+        set_error("cufftExecZ2D failed");
+        rc = NGW_ERR_CUDA;
+        break;
+      }
+      k_unpack<<<dim3(bx, nc), 256, 0, s->stream>>>(box, ngrid, dg, n, scale, dvz + (size_t)c0 * ngrid,
+                                                    ngrid);
+    }
+    if (rc != NGW_OK) break;
+    if (cudaGetLastError() != cudaSuccess) {
+      set_error("Poisson kernels failed to launch");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    const double nf = 1.0 / (h * h * h);
+    const double zero = 0.0;
+    if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n_isdf, n_isdf, ngrid, &nf, dz, ngrid, dvz, ngrid,
+                    &zero, dm, n_isdf) != CUBLAS_STATUS_SUCCESS) {
+      set_error("cublasDgemm (zeta^T v zeta) failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+  } while (0);
+  cudaStreamSynchronize(s->stream);
+  if (have_pf) cufftDestroy(pf);
+  if (have_pb) cufftDestroy(pb);
+  dfree(s, dvz, (size_t)ngrid * n_isdf * 8);
+  dfree(s, box, bsz * batch * 8);
+  dfree(s, spec, csz * batch * 16);
+  dfree(s, vtab, csz * 8);
+  return rc;
+}
+
 }  // namespace ngw
 
 using namespace ngw;
@@ -91,107 +176,32 @@ extern "C" int ngw_build_coulomb_kernel(ngw_session *s, int ngrid, int n_isdf, c
     return NGW_ERR_ARG;
   }
   NGW_CUDA(cudaSetDevice(s->device));
-  const int n = nfft;
-  const size_t bsz = (size_t)n * n * n;
-  const size_t csz = (size_t)n * n * (n / 2 + 1);
-  // batch so that the boxes stay under ~2 GB
-  int batch = (int)std::max<size_t>(1, (size_t)(2ull << 30) / (bsz * 8 + csz * 16));
-  if (batch > n_isdf) batch = n_isdf;
-  double *dz = nullptr, *dvz = nullptr, *box = nullptr, *vtab = nullptr, *dm = nullptr;
-  cufftDoubleComplex *spec = nullptr;
+  double *dz = nullptr, *dm = nullptr;
   int *dg = nullptr;
   int rc = NGW_OK;
-  cufftHandle pf = 0, pb = 0;
-  bool have_pf = false, have_pb = false;
-  auto fail = [&](int code) {
-    rc = code;
-    return code;
-  };
   do {
     if (dalloc(s, (void **)&dz, (size_t)ngrid * n_isdf * 8) ||
-        dalloc(s, (void **)&dvz, (size_t)ngrid * n_isdf * 8) ||
-        dalloc(s, (void **)&box, bsz * batch * 8) ||
-        dalloc(s, (void **)&spec, csz * batch * 16) || dalloc(s, (void **)&vtab, csz * 8) ||
-        dalloc(s, (void **)&dm, (size_t)n_isdf * n_isdf * 8) ||
-        dalloc(s, (void **)&dg, (size_t)3 * ngrid * 4)) {
-      fail(NGW_ERR_OOM);
+        dalloc(s, (void **)&dm, (size_t)n_isdf * n_isdf * 8) || dalloc(s, (void **)&dg, (size_t)3 * ngrid * 4)) {
+      rc = NGW_ERR_OOM;
       break;
     }
     if (cudaMemcpyAsync(dz, zeta, (size_t)ngrid * n_isdf * 8, cudaMemcpyHostToDevice, s->stream) ||
         cudaMemcpyAsync(dg, grid_idx, (size_t)3 * ngrid * 4, cudaMemcpyHostToDevice, s->stream)) {
       set_error("copy to device failed");
-      fail(NGW_ERR_CUDA);
+      rc = NGW_ERR_CUDA;
       break;
     }
-    const double b = 2.0 * M_PI / ((double)n * h);
-    k_coulomb_table<<<1024, 256, 0, s->stream>>>(vtab, n, b, trunc);
-    int dims[3] = {n, n, n};
-    if (cufftPlanMany(&pf, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, batch) != CUFFT_SUCCESS) {
-      set_error("cufftPlanMany D2Z failed");
-      fail(NGW_ERR_CUDA);
-      break;
-    }
-    have_pf = true;
-    if (cufftPlanMany(&pb, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, batch) != CUFFT_SUCCESS) {
-      set_error("cufftPlanMany Z2D failed");
-      fail(NGW_ERR_CUDA);
-      break;
-    }
-    have_pb = true;
-    cufftSetStream(pf, s->stream);
-    cufftSetStream(pb, s->stream);
-    const double scale = 1.0 / ((double)n * (double)n * (double)n);
-    for (int c0 = 0; c0 < n_isdf && rc == NGW_OK; c0 += batch) {
-      const int nc = std::min(batch, n_isdf - c0);
-      cudaMemsetAsync(box, 0, bsz * batch * 8, s->stream);
-      int bx = (ngrid + 255) / 256;
-      if (bx > 256) bx = 256;
-      k_pack<<<dim3(bx, nc), 256, 0, s->stream>>>(dz + (size_t)c0 * ngrid, ngrid, ngrid, dg, n, box,
-                                                  nc);
-      if (cufftExecD2Z(pf, box, spec) != CUFFT_SUCCESS) {
-        set_error("cufftExecD2Z failed");
-        fail(NGW_ERR_CUDA);
-        break;
-      }
-      k_mul_coulomb<<<2048, 256, 0, s->stream>>>(spec, vtab, csz, batch);
-      if (cufftExecZ2D(pb, spec, box) != CUFFT_SUCCESS) {
-        set_error("cufftExecZ2D failed");
-        fail(NGW_ERR_CUDA);
-        break;
-      }
-      k_unpack<<<dim3(bx, nc), 256, 0, s->stream>>>(box, ngrid, dg, n, scale,
-                                                    dvz + (size_t)c0 * ngrid, ngrid);
-    }
+    rc = coulomb_core(s, ngrid, n_isdf, dz, dg, nfft, h, trunc, dm);
     if (rc != NGW_OK) break;
-    if (cudaGetLastError() != cudaSuccess) {
-      set_error("Poisson kernels failed to launch");
-      fail(NGW_ERR_CUDA);
-      break;
-    }
-    // M = (ntrans / hcub) zeta^T (v_c zeta)
-    const double nf = 1.0 / (h * h * h);
-    const double zero = 0.0;
-    if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n_isdf, n_isdf, ngrid, &nf, dz, ngrid, dvz,
-                    ngrid, &zero, dm, n_isdf) != CUBLAS_STATUS_SUCCESS) {
-      set_error("cublasDgemm (zeta^T v zeta) failed");
-      fail(NGW_ERR_CUDA);
-      break;
-    }
     if (cudaMemcpyAsync(mmtrx, dm, (size_t)n_isdf * n_isdf * 8, cudaMemcpyDeviceToHost, s->stream) ||
         cudaStreamSynchronize(s->stream)) {
       set_error("copy back failed");
-      fail(NGW_ERR_CUDA);
+      rc = NGW_ERR_CUDA;
       break;
     }
   } while (0);
   cudaStreamSynchronize(s->stream);
-  if (have_pf) cufftDestroy(pf);
-  if (have_pb) cufftDestroy(pb);
   dfree(s, dz, (size_t)ngrid * n_isdf * 8);
-  dfree(s, dvz, (size_t)ngrid * n_isdf * 8);
-  dfree(s, box, bsz * batch * 8);
-  dfree(s, spec, csz * batch * 16);
-  dfree(s, vtab, csz * 8);
   dfree(s, dm, (size_t)n_isdf * n_isdf * 8);
   dfree(s, dg, (size_t)3 * ngrid * 4);
   return rc;
@@ -240,6 +250,43 @@ __global__ void k_scale_cols_by(const double *__restrict__ z, const double *__re
     out[(size_t)col * n + i] = f[i] * z[(size_t)col * n + i];
 }
 
+
+// M_xc = (ntrans / hcub) zeta^T (f_xc * zeta) from device-resident zeta and rho.
+int fxc_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const double *drho, double h,
+             double *dm, double *dfxc) {
+  double *dfz = nullptr;
+  const size_t zb = (size_t)ngrid * n_isdf * 8;
+  int rc = NGW_OK;
+  do {
+    if (dalloc(s, (void **)&dfz, zb)) {
+      rc = NGW_ERR_OOM;
+      break;
+    }
+    k_fxc_lda<<<std::min(1024, (ngrid + 255) / 256), 256, 0, s->stream>>>(drho, ngrid, dfxc);
+    k_scale_cols_by<<<dim3(std::min(256, (ngrid + 255) / 256), n_isdf), 256, 0, s->stream>>>(
+        dz, dfxc, ngrid, n_isdf, dfz);
+    const double nf = 1.0 / (h * h * h), zero = 0.0;
+    if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n_isdf, n_isdf, ngrid, &nf, dz, ngrid, dfz, ngrid,
+                    &zero, dm, n_isdf) != CUBLAS_STATUS_SUCCESS) {
+      set_error("cublasDgemm (zeta^T f zeta) failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+  } while (0);
+  cudaStreamSynchronize(s->stream);
+  dfree(s, dfz, zb);
+  return rc;
+}
+
+int check_density(int ngrid, const double *rho, const char *who) {
+  for (int i = 0; i < ngrid; ++i)
+    if (!(rho[i] > 0.0) || !std::isfinite(rho[i])) {
+      set_error("%s: density must be positive and finite (point %d)", who, i);
+      return NGW_ERR_NONFINITE;
+    }
+  return NGW_OK;
+}
+
 }  // namespace ngw
 
 extern "C" int ngw_build_fxc_kernel(ngw_session *s, int ngrid, int n_isdf, const double *zeta,
@@ -249,19 +296,14 @@ extern "C" int ngw_build_fxc_kernel(ngw_session *s, int ngrid, int n_isdf, const
     set_error("ngw_build_fxc_kernel: bad arguments");
     return NGW_ERR_ARG;
   }
-  for (int i = 0; i < ngrid; ++i)
-    if (!(rho[i] > 0.0) || !std::isfinite(rho[i])) {
-      set_error("ngw_build_fxc_kernel: density must be positive and finite (point %d)", i);
-      return NGW_ERR_NONFINITE;
-    }
+  if (int e = check_density(ngrid, rho, "ngw_build_fxc_kernel")) return e;
   NGW_CUDA(cudaSetDevice(s->device));
-  double *dz = nullptr, *dfz = nullptr, *drho = nullptr, *dfxc = nullptr, *dm = nullptr;
+  double *dz = nullptr, *drho = nullptr, *dfxc = nullptr, *dm = nullptr;
   const size_t zb = (size_t)ngrid * n_isdf * 8;
   int rc = NGW_OK;
   do {
-    if (dalloc(s, (void **)&dz, zb) || dalloc(s, (void **)&dfz, zb) ||
-        dalloc(s, (void **)&drho, (size_t)ngrid * 8) || dalloc(s, (void **)&dfxc, (size_t)ngrid * 8) ||
-        dalloc(s, (void **)&dm, (size_t)n_isdf * n_isdf * 8)) {
+    if (dalloc(s, (void **)&dz, zb) || dalloc(s, (void **)&drho, (size_t)ngrid * 8) ||
+        dalloc(s, (void **)&dfxc, (size_t)ngrid * 8) || dalloc(s, (void **)&dm, (size_t)n_isdf * n_isdf * 8)) {
       rc = NGW_ERR_OOM;
       break;
     }
@@ -271,16 +313,8 @@ extern "C" int ngw_build_fxc_kernel(ngw_session *s, int ngrid, int n_isdf, const
       rc = NGW_ERR_CUDA;
       break;
     }
-    k_fxc_lda<<<std::min(1024, (ngrid + 255) / 256), 256, 0, s->stream>>>(drho, ngrid, dfxc);
-    k_scale_cols_by<<<dim3(std::min(256, (ngrid + 255) / 256), n_isdf), 256, 0, s->stream>>>(
-        dz, dfxc, ngrid, n_isdf, dfz);
-    const double nf = 1.0 / (h * h * h), zero = 0.0;
-    if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n_isdf, n_isdf, ngrid, &nf, dz, ngrid, dfz,
-                    ngrid, &zero, dm, n_isdf) != CUBLAS_STATUS_SUCCESS) {
-      set_error("cublasDgemm (zeta^T f zeta) failed");
-      rc = NGW_ERR_CUDA;
-      break;
-    }
+    rc = fxc_core(s, ngrid, n_isdf, dz, drho, h, dm, dfxc);
+    if (rc != NGW_OK) break;
     if (cudaMemcpyAsync(mxc, dm, (size_t)n_isdf * n_isdf * 8, cudaMemcpyDeviceToHost, s->stream) ||
         (fxc_out && cudaMemcpyAsync(fxc_out, dfxc, (size_t)ngrid * 8, cudaMemcpyDeviceToHost, s->stream)) ||
         cudaStreamSynchronize(s->stream)) {
@@ -291,7 +325,6 @@ extern "C" int ngw_build_fxc_kernel(ngw_session *s, int ngrid, int n_isdf, const
   } while (0);
   cudaStreamSynchronize(s->stream);
   dfree(s, dz, zb);
-  dfree(s, dfz, zb);
   dfree(s, drho, (size_t)ngrid * 8);
   dfree(s, dfxc, (size_t)ngrid * 8);
   dfree(s, dm, (size_t)n_isdf * n_isdf * 8);

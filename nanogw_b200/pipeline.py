@@ -6,8 +6,10 @@ the ISDF fit of the interpolation vectors zeta
 (``shared/isdf_parallel_sym_UltraLowMem.F90:439-667``) and the Coulomb block
 ``M = ntrans/hcub zeta^T v_c zeta`` built on the device
 (``:687-889``; library entry ``ngw_build_coulomb_kernel``).
-The fit (P, Q products and the A zeta^T = B solve) runs on the host with
-LAPACK in this version.
+The fit (P, Q products and the A zeta^T = B solve) runs on the device by
+default (``ngw_build_isdf_kernel``; zeta stays in HBM and feeds the Poisson
+build directly); ``device_fit=False`` keeps the numpy fit (host LAPACK) for
+machines without a GPU.
 """
 from dataclasses import dataclass
 
@@ -26,6 +28,7 @@ class IsdfOperator:
     nval: int
     cvt_iters: int
     zeta: np.ndarray = None
+    mxc: np.ndarray = None   # f_xc block (n_isdf, n_isdf), Ry, when built
 
     @property
     def nmem(self):
@@ -61,18 +64,27 @@ def isdf_fit(psi, psi_intp, mv, nmem):
 
 
 def build_operator(mol, n_isdf, session, qp_bands=(), seed=0, max_cvt_iter=100000,
-                   keep_zeta=False):
+                   keep_zeta=False, device_fit=True, with_fxc=False):
     grid = mol.grid
     init = synth.cvt_initial_points(grid, n_isdf, seed if seed else mol.seed)
     intp, _, iters = host.cvt(grid, mol.rho, init, max_cvt_iter)
     intp = host.dedup_points(intp, mol.rho)
-    psi_intp = np.asfortranarray(mol.psi[intp - 1, :])
     mv = max([mol.nval] + [int(b) for b in qp_bands])
-    zeta = isdf_fit(mol.psi, psi_intp, mv, mol.nmem)
     nfft = fft_box_size(mol.rmax, mol.h)
-    M = session.build_coulomb_kernel(zeta, mol.grid_idx, nfft, mol.h, 2.0 * mol.rmax)
-    return IsdfOperator(psi_intp=psi_intp, mmtrx=np.asfortranarray(M), intp=intp, e1=mol.e1.copy(),
-                        nval=mol.nval, cvt_iters=iters, zeta=zeta if keep_zeta else None)
+    mxc = None
+    if device_fit and not keep_zeta:
+        psi_intp, M, mxc = session.build_isdf_kernel(mol.psi, mol.grid_idx, intp, mv, nfft, mol.h,
+                                                     2.0 * mol.rmax, mol.rho if with_fxc else None)
+        zeta = None
+    else:
+        psi_intp = np.asfortranarray(mol.psi[intp - 1, :])
+        zeta = isdf_fit(mol.psi, psi_intp, mv, mol.nmem)
+        M = session.build_coulomb_kernel(zeta, mol.grid_idx, nfft, mol.h, 2.0 * mol.rmax)
+        if with_fxc:
+            mxc = session.build_fxc_kernel(zeta, mol.rho, mol.h)
+    op = IsdfOperator(psi_intp=psi_intp, mmtrx=np.asfortranarray(M), intp=intp, e1=mol.e1.copy(),
+                      nval=mol.nval, cvt_iters=iters, zeta=zeta if keep_zeta else None, mxc=mxc)
+    return op
 
 
 def qp_bands_near_gap(nval, nqp):

@@ -203,3 +203,36 @@ def test_errors_are_codes(small_system):
         assert e.value.code == ngw._lib.NGW_ERR_ARG
     with pytest.raises(NGWError):
         ngw.Session(device=999)
+
+
+def test_isdf_kernel_build_on_device(small_system):
+    """Device ISDF fit (P/Q DGEMMs, Hadamard, LU solve) + Coulomb and f_xc
+    blocks against the oracle's fit and kernels.  cond(A) of this system is
+    ~1.3e8, so two backward-stable LU solves may differ by ~cond * eps ~ 3e-8
+    in zeta; the blocks are compared at 1e-6 relative."""
+    from oracle import fxc as OF
+    S = small_system
+    mol = S.mol
+    with ngw.Session(0) as s:
+        pi, m, mx = s.build_isdf_kernel(mol.psi, mol.grid_idx, S.intp, S.nval + 1, S.nfft, mol.h,
+                                        2.0 * mol.rmax, mol.rho)
+    assert np.array_equal(pi, S.psi_intp)
+    assert _rel(m, S.M) < 1e-6
+    _, ref = OI.kernel_mmtrx(S.zeta, S.zeta, mol.hcub, fxc=OF.fxc_lda(mol.rho))
+    assert _rel(mx, ref) < 1e-6
+
+
+def test_isdf_kernel_build_rejects_repeated_points(small_system):
+    S = small_system
+    mol = S.mol
+    intp = S.intp.copy()
+    intp[5] = intp[4]          # two identical rows of A: singular
+    with ngw.Session(0) as s:
+        with pytest.raises(NGWError) as e:
+            s.build_isdf_kernel(mol.psi, mol.grid_idx, intp, S.nval + 1, S.nfft, mol.h, 2.0 * mol.rmax)
+        assert e.value.code == ngw._lib.NGW_ERR_ARG
+        bad = S.intp.copy()
+        bad[0] = mol.psi.shape[0] + 1
+        with pytest.raises(NGWError) as e:
+            s.build_isdf_kernel(mol.psi, mol.grid_idx, bad, S.nval + 1, S.nfft, mol.h, 2.0 * mol.rmax)
+        assert e.value.code == ngw._lib.NGW_ERR_ARG
