@@ -277,7 +277,7 @@ def main():
     roof = None
     if args.precision == "mixed":
         us1, us2 = sess.profile_mixed_gemms(nb, reps=50)
-        M1, N1, K1, BN1, sp1, M2, N2, K2, BN2, v1, v2 = sess.mixed_gemm_shapes(nb)
+        M1, N1, K1, BN1, sp1, M2, N2, K2, BN2, v1, v2, r1, r2 = sess.mixed_gemm_shapes(nb)
         flops = 2.0 * M1 * N1 * K1 + 2.0 * M2 * N2 * K2
         achieved = flops / ((us1 + us2) * 1e-6) / 1e12
         hbm, bf16, bf16s, src = load_peaks()
@@ -285,7 +285,7 @@ def main():
                 "frac": achieved / bf16, "traffic": None,
                 "kernel": "k_tc_gemm (GEMM1 + GEMM2 of one matvec)",
                 "us_per_launch": [us1, us2], "shapes": [[M1, N1, K1, BN1, sp1, v1], [M2, N2, K2, BN2, 1, v2]],
-                "tiles_env": f"{BN1},{v1},{sp1},{BN2},{v2}",
+                "tiles_env": f"{BN1},{v1},{sp1},{BN2},{v2},{r1},{r2}",
                 "peak_source": f"{src} (bf16 dense, burst)",
                 "executed_bf16_frac": 3.0 * achieved / bf16}
 

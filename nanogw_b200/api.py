@@ -185,7 +185,7 @@ class Session:
         return float(t1[0]), float(t2[0])
 
     def mixed_gemm_shapes(self, nb):
-        sh = np.zeros(11, dtype=np.int32)
+        sh = np.zeros(13, dtype=np.int32)
         check(lib().ngw_mixed_gemm_shapes(self._h, int(nb), _p(sh)))
         return [int(x) for x in sh]
 

@@ -778,15 +778,15 @@ __global__ void k_split_cols_to_rows(const double *__restrict__ X, int ncv, int 
 __global__ void k_split_rows(const double *__restrict__ D, int n_isdf, int ncv,
                              const double *__restrict__ U, int k, const double *__restrict__ s,
                              bf16 *__restrict__ hi, bf16 *__restrict__ lo, int ldk) {
-  const int cv = blockIdx.y;
-  for (int mu = blockIdx.x * blockDim.x + threadIdx.x; mu < n_isdf + k; mu += gridDim.x * blockDim.x) {
-    const double x = (mu < n_isdf) ? D[(size_t)cv * n_isdf + mu]
-                                   : -U[(size_t)(mu - n_isdf) * ncv + cv] / (4.0 * s[cv]);
-    const bf16 h = __double2bfloat16(x);
-    const bf16 l = __double2bfloat16(x - (double)__bfloat162float(h));
-    hi[(size_t)cv * ldk + mu] = h;
-    lo[(size_t)cv * ldk + mu] = l;
-  }
+  for (int cv = blockIdx.y; cv < ncv; cv += gridDim.y)
+    for (int mu = blockIdx.x * blockDim.x + threadIdx.x; mu < n_isdf + k; mu += gridDim.x * blockDim.x) {
+      const double x = (mu < n_isdf) ? D[(size_t)cv * n_isdf + mu]
+                                     : -U[(size_t)(mu - n_isdf) * ncv + cv] / (4.0 * s[cv]);
+      const bf16 h = __double2bfloat16(x);
+      const bf16 l = __double2bfloat16(x - (double)__bfloat162float(h));
+      hi[(size_t)cv * ldk + mu] = h;
+      lo[(size_t)cv * ldk + mu] = l;
+    }
 }
 
 // Clenshaw start: v_perp = v - U xo (deflated part, stored FP32), b_n = g v_perp
@@ -796,19 +796,19 @@ __global__ void k_cheb_start(const double *__restrict__ v, int ldv, const double
                              int ncv, int nb, double g, int tda, float *__restrict__ vp,
                              float *__restrict__ bn, int ldx, bf16 *__restrict__ shi,
                              bf16 *__restrict__ slo, int lds) {
-  const int j = blockIdx.y;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
-    double x = v[(size_t)j * ldv + i];
-    for (int q = 0; q < kdef; ++q) x -= U[(size_t)q * ncv + i] * xo[(size_t)j * kdef + q];
-    vp[(size_t)j * ldx + i] = (float)x;
-    const double b = g * x;
-    bn[(size_t)j * ldx + i] = (float)b;
-    const double u = tda ? b : s[i] * b;
-    bf16 h, l;
-    split_bf16((float)u, h, l);
-    shi[(size_t)j * lds + i] = h;
-    slo[(size_t)j * lds + i] = l;
-  }
+  for (int j = blockIdx.y; j < nb; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
+      double x = v[(size_t)j * ldv + i];
+      for (int q = 0; q < kdef; ++q) x -= U[(size_t)q * ncv + i] * xo[(size_t)j * kdef + q];
+      vp[(size_t)j * ldx + i] = (float)x;
+      const double b = g * x;
+      bn[(size_t)j * ldx + i] = (float)b;
+      const double u = tda ? b : s[i] * b;
+      bf16 h, l;
+      split_bf16((float)u, h, l);
+      shi[(size_t)j * lds + i] = h;
+      slo[(size_t)j * lds + i] = l;
+    }
 }
 
 struct MixedOperator {
@@ -950,7 +950,7 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
   }
   {
     int bx = (s->n_isdf + kdef + 127) / 128;
-    k_split_rows<<<dim3(bx, s->ncv), 128, 0, st>>>(D, s->n_isdf, s->ncv, s->eig_U, kdef,
+    k_split_rows<<<dim3(bx, ygrid(s->ncv)), 128, 0, st>>>(D, s->n_isdf, s->ncv, s->eig_U, kdef,
                                                    s->d_sqrtR, op->A3_hi, op->A3_lo, op->mu_k);
     NGW_CUDA(cudaGetLastError());
   }
@@ -1266,7 +1266,7 @@ int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const dou
   {
     int bx = (ncv + 255) / 256;
     if (bx > 16) bx = 16;
-    k_cheb_start<<<dim3(bx, nb), 256, 0, st>>>(v, ldv, s->eig_U, op->xo, k, s->d_sqrtR, ncv, nb, g[n],
+    k_cheb_start<<<dim3(bx, ygrid(nb)), 256, 0, st>>>(v, ldv, s->eig_U, op->xo, k, s->d_sqrtR, ncv, nb, g[n],
                                               tda, op->vperp, op->bb[0], op->cv_pad, op->S_hi,
                                               op->S_lo, op->cv_pad);
     NGW_CUDA(cudaGetLastError());
@@ -1372,5 +1372,6 @@ extern "C" int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape) {
   shape[4] = op->split1;
   shape[5] = op->ncv; shape[6] = nb; shape[7] = op->n_isdf + op->kdef; shape[8] = op->BN2;
   shape[9] = op->var1; shape[10] = op->var2;
+  shape[11] = 0; shape[12] = 0;
   return NGW_OK;
 }

@@ -18,22 +18,22 @@ static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b)
 __global__ void k_pair_gather_f64(const double *__restrict__ psi, int n_isdf,
                                   const int *__restrict__ cvpair, int ncv,
                                   double *__restrict__ C) {
-  const int cv = blockIdx.y;
-  if (cv >= ncv) return;
-  const int v = cvpair[2 * cv] - 1, c = cvpair[2 * cv + 1] - 1;
-  const double *pv = psi + (size_t)v * n_isdf;
-  const double *pc = psi + (size_t)c * n_isdf;
-  double *out = C + (size_t)cv * n_isdf;
-  if ((n_isdf & 1) == 0) {
-    const int n2 = n_isdf >> 1;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
-      double2 a = reinterpret_cast<const double2 *>(pc)[i];
-      double2 b = reinterpret_cast<const double2 *>(pv)[i];
-      reinterpret_cast<double2 *>(out)[i] = make_double2(a.x * b.x, a.y * b.y);
+  for (int cv = blockIdx.y; cv < ncv; cv += gridDim.y) {
+    const int v = cvpair[2 * cv] - 1, c = cvpair[2 * cv + 1] - 1;
+    const double *pv = psi + (size_t)v * n_isdf;
+    const double *pc = psi + (size_t)c * n_isdf;
+    double *out = C + (size_t)cv * n_isdf;
+    if ((n_isdf & 1) == 0) {
+      const int n2 = n_isdf >> 1;
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+        double2 a = reinterpret_cast<const double2 *>(pc)[i];
+        double2 b = reinterpret_cast<const double2 *>(pv)[i];
+        reinterpret_cast<double2 *>(out)[i] = make_double2(a.x * b.x, a.y * b.y);
+      }
+    } else {
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_isdf; i += gridDim.x * blockDim.x)
+        out[i] = pc[i] * pv[i];
     }
-  } else {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_isdf; i += gridDim.x * blockDim.x)
-      out[i] = pc[i] * pv[i];
   }
 }
 
@@ -43,7 +43,7 @@ void launch_pair_gather_f64(const double *psi, int n_isdf, const int *cvpair, in
   int threads = 128;
   int bx = cdiv((n_isdf + 1) / 2, threads);
   if (bx > 8) bx = 8;
-  dim3 grid(bx, ncv);
+  dim3 grid(bx, ygrid(ncv));
   k_pair_gather_f64<<<grid, threads, 0, st>>>(psi, n_isdf, cvpair, ncv, C);
 }
 
@@ -51,12 +51,12 @@ void launch_pair_gather_f64(const double *psi, int n_isdf, const int *cvpair, in
 __global__ void k_pair_gather_cols(const double *__restrict__ psi, int n_isdf,
                                    const int *__restrict__ b1, const int *__restrict__ b2, int n,
                                    double *__restrict__ out) {
-  const int j = blockIdx.y;
-  if (j >= n) return;
-  const double *p1 = psi + (size_t)(b1[j] - 1) * n_isdf;
-  const double *p2 = psi + (size_t)(b2[j] - 1) * n_isdf;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_isdf; i += gridDim.x * blockDim.x)
-    out[(size_t)j * n_isdf + i] = p1[i] * p2[i];
+  for (int j = blockIdx.y; j < n; j += gridDim.y) {
+    const double *p1 = psi + (size_t)(b1[j] - 1) * n_isdf;
+    const double *p2 = psi + (size_t)(b2[j] - 1) * n_isdf;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_isdf; i += gridDim.x * blockDim.x)
+      out[(size_t)j * n_isdf + i] = p1[i] * p2[i];
+  }
 }
 
 void launch_pair_gather_cols(const double *psi, int n_isdf, const int *b1, const int *b2, int n,
@@ -64,18 +64,18 @@ void launch_pair_gather_cols(const double *psi, int n_isdf, const int *b1, const
   if (n <= 0) return;
   int bx = cdiv(n_isdf, 128);
   if (bx > 8) bx = 8;
-  k_pair_gather_cols<<<dim3(bx, n), 128, 0, st>>>(psi, n_isdf, b1, b2, n, out);
+  k_pair_gather_cols<<<dim3(bx, ygrid(n)), 128, 0, st>>>(psi, n_isdf, b1, b2, n, out);
 }
 
 // ---------------------------------------------------------------------------
 // y = sqrtR * x  (or a copy with TDA)   apply_matvec_lowcomsym.F90:112-128
 __global__ void k_scale_rows(const double *__restrict__ s, const double *__restrict__ x, int ldx,
                              double *__restrict__ y, int ldy, int ncv, int nb, int tamm_d) {
-  const int j = blockIdx.y;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
-    double v = x[(size_t)j * ldx + i];
-    y[(size_t)j * ldy + i] = tamm_d ? v : s[i] * v;
-  }
+  for (int j = blockIdx.y; j < nb; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
+      double v = x[(size_t)j * ldx + i];
+      y[(size_t)j * ldy + i] = tamm_d ? v : s[i] * v;
+    }
 }
 
 void launch_scale_rows(const double *s, const double *x, int ldx, double *y, int ldy, int ncv,
@@ -83,14 +83,14 @@ void launch_scale_rows(const double *s, const double *x, int ldx, double *y, int
   if (nb <= 0) return;
   int bx = cdiv(ncv, 256);
   if (bx > 16) bx = 16;
-  k_scale_rows<<<dim3(bx, nb), 256, 0, st>>>(s, x, ldx, y, ldy, ncv, nb, tamm_d);
+  k_scale_rows<<<dim3(bx, ygrid(nb)), 256, 0, st>>>(s, x, ldx, y, ldy, ncv, nb, tamm_d);
 }
 
 __global__ void k_copy_cols(const double *__restrict__ x, int ldx, double *__restrict__ y, int ldy,
                             int n, int nb) {
-  const int j = blockIdx.y;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    y[(size_t)j * ldy + i] = x[(size_t)j * ldx + i];
+  for (int j = blockIdx.y; j < nb; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+      y[(size_t)j * ldy + i] = x[(size_t)j * ldx + i];
 }
 
 void launch_copy_cols(const double *x, int ldx, double *y, int ldy, int n, int nb,
@@ -98,7 +98,7 @@ void launch_copy_cols(const double *x, int ldx, double *y, int ldy, int n, int n
   if (nb <= 0) return;
   int bx = cdiv(n, 256);
   if (bx > 16) bx = 16;
-  k_copy_cols<<<dim3(bx, nb), 256, 0, st>>>(x, ldx, y, ldy, n, nb);
+  k_copy_cols<<<dim3(bx, ygrid(nb)), 256, 0, st>>>(x, ldx, y, ldy, n, nb);
 }
 
 // Diagonal combine of the ISDF matvec (apply_matvec_lowcomsym.F90:396-412)
@@ -111,25 +111,26 @@ __global__ void k_matvec_combine(const double *__restrict__ s, const double *__r
                                  const double *__restrict__ z, double *__restrict__ y,
                                  const double *__restrict__ vec, int ncv, int nb, int tamm_d,
                                  int horner_k, double pk, double pk1, double *__restrict__ hs) {
-  const int j = blockIdx.y;
-  const size_t base = (size_t)j * ncv;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
-    const double si = s[i];
-    double r;
-    if (tamm_d) {
-      r = (si * si) * h[base + i];
-      r = r + 2.0 * z[base + i];
-    } else {
-      r = (si * si * si) * h[base + i];
-      r = r + 4.0 * si * z[base + i];
+  for (int j = blockIdx.y; j < nb; j += gridDim.y) {
+    const size_t base = (size_t)j * ncv;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
+      const double si = s[i];
+      double r;
+      if (tamm_d) {
+        r = (si * si) * h[base + i];
+        r = r + 2.0 * z[base + i];
+      } else {
+        r = (si * si * si) * h[base + i];
+        r = r + 4.0 * si * z[base + i];
+      }
+      if (horner_k == 1) {
+        r = pk * r + pk1 * vec[base + i];
+      } else if (horner_k > 1) {
+        r = r + pk1 * vec[base + i];
+      }
+      y[base + i] = r;
+      if (hs) hs[base + i] = tamm_d ? r : si * r;
     }
-    if (horner_k == 1) {
-      r = pk * r + pk1 * vec[base + i];
-    } else if (horner_k > 1) {
-      r = r + pk1 * vec[base + i];
-    }
-    y[base + i] = r;
-    if (hs) hs[base + i] = tamm_d ? r : si * r;
   }
 }
 
@@ -139,7 +140,7 @@ void launch_matvec_combine(const double *s, const double *h, const double *z, do
   if (nb <= 0) return;
   int bx = cdiv(ncv, 256);
   if (bx > 16) bx = 16;
-  k_matvec_combine<<<dim3(bx, nb), 256, 0, st>>>(s, h, z, y, vec, ncv, nb, tamm_d, horner_k,
+  k_matvec_combine<<<dim3(bx, ygrid(nb)), 256, 0, st>>>(s, h, z, y, vec, ncv, nb, tamm_d, horner_k,
                                                  pk, pk1, hs_next);
 }
 
@@ -323,20 +324,21 @@ __device__ __forceinline__ cplx contfrac_eval(const double *a, const double *b, 
 __global__ void k_contfrac(const double *__restrict__ a, const double *__restrict__ b, int niter,
                            int nb, const double *__restrict__ zz, int nz,
                            double *__restrict__ spectra) {
-  const int j = blockIdx.y;
   const int iz = blockIdx.x * blockDim.x + threadIdx.x;
-  if (iz >= nz || j >= nb) return;
-  const size_t o = (size_t)j * nz + iz;
-  cplx z = {zz[2 * o], zz[2 * o + 1]};
-  cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, niter, z);
-  spectra[2 * o] = r.re;
-  spectra[2 * o + 1] = r.im;
+  if (iz >= nz) return;
+  for (int j = blockIdx.y; j < nb; j += gridDim.y) {
+    const size_t o = (size_t)j * nz + iz;
+    cplx z = {zz[2 * o], zz[2 * o + 1]};
+    cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, niter, z);
+    spectra[2 * o] = r.re;
+    spectra[2 * o + 1] = r.im;
+  }
 }
 
 void launch_contfrac(const double *a, const double *b, int niter, int nb, const double *zz, int nz,
                      double *spectra, cudaStream_t st) {
   if (nb <= 0 || nz <= 0) return;
-  k_contfrac<<<dim3(cdiv(nz, 128), nb), 128, 0, st>>>(a, b, niter, nb, zz, nz, spectra);
+  k_contfrac<<<dim3(cdiv(nz, 128), ygrid(nb)), 128, 0, st>>>(a, b, niter, nb, zz, nz, spectra);
 }
 
 // Per-chain spectra on the Sigma energy grid:
@@ -348,24 +350,25 @@ __global__ void k_sigma_spectra(const double *__restrict__ a, const double *__re
                                 const int *__restrict__ chain_qp, const double *__restrict__ zz0,
                                 double de, int nen, double ecuts, int nval,
                                 double *__restrict__ S) {
-  const int j = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nchain || i > nen) return;
-  const int n = chain_band[j];
-  const double eta = (n <= nval) ? 1.0 : -1.0;
-  cplx z;
-  if (i == nen) {
-    z.re = 0.0;
-    z.im = 0.0;
-  } else {
-    const double zz = de * (double)i + zz0[chain_qp[j]];
-    z.re = (-zz + e1[n - 1]) * eta;
-    z.im = ecuts;
+  if (i > nen) return;
+  for (int j = blockIdx.y; j < nchain; j += gridDim.y) {
+    const int n = chain_band[j];
+    const double eta = (n <= nval) ? 1.0 : -1.0;
+    cplx z;
+    if (i == nen) {
+      z.re = 0.0;
+      z.im = 0.0;
+    } else {
+      const double zz = de * (double)i + zz0[chain_qp[j]];
+      z.re = (-zz + e1[n - 1]) * eta;
+      z.im = ecuts;
+    }
+    cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, niter, z);
+    const size_t o = (size_t)j * (nen + 1) + i;
+    S[2 * o] = r.re;
+    S[2 * o + 1] = r.im;
   }
-  cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, niter, z);
-  const size_t o = (size_t)j * (nen + 1) + i;
-  S[2 * o] = r.re;
-  S[2 * o + 1] = r.im;
 }
 
 void launch_sigma_spectra(const double *a, const double *b, int niter, int nchain,
@@ -373,7 +376,7 @@ void launch_sigma_spectra(const double *a, const double *b, int niter, int nchai
                           const double *zz0, double de, int nen, double ecuts, int nval,
                           double *S, cudaStream_t st) {
   if (nchain <= 0) return;
-  k_sigma_spectra<<<dim3(cdiv(nen + 1, 128), nchain), 128, 0, st>>>(
+  k_sigma_spectra<<<dim3(cdiv(nen + 1, 128), ygrid(nchain)), 128, 0, st>>>(
       a, b, niter, nchain, e1, chain_band, chain_qp, zz0, de, nen, ecuts, nval, S);
 }
 

@@ -14,6 +14,10 @@ namespace ngw {
 
 void set_error(const char *fmt, ...);
 
+// gridDim.y / gridDim.z are limited to 65535: kernels indexed by pair or chain
+// in y take min(n, 65535) blocks there and stride over the rest.
+inline unsigned ygrid(long long n) { return n < 1 ? 1u : (n < 65535 ? (unsigned)n : 65535u); }
+
 #define NGW_CUDA(call)                                                           \
   do {                                                                           \
     cudaError_t e_ = (call);                                                     \
