@@ -126,6 +126,52 @@ def solve_once(sess, op, qp, poly, wl, sigx, vxc):
     return sig, eqp
 
 
+# Operator dimensions of the large single-molecule workload (60 atoms, 240
+# occupied + 960 empty orbitals, 4800 ISDF points: N_cv = 230,400) and of the
+# largest molecule of the batched workload (140 + 560 orbitals, 1120 points).
+LARGE_OPERATORS = {"large-molecule": (4800, 240, 960), "batched-max": (1120, 140, 560)}
+
+
+def gemm_scan(local, name, nbs, reps=10):
+    """Throughput of the two split-BF16 tcgen05 GEMMs of one matvec at a large
+    operator's dimensions.  The operator is random (orbital values at the
+    points ~ N(0, 0.05^2), M = G G^T * 0.02, sorted random KS energies): the
+    GEMM shapes and the kernels are those of a real operator of that size, the
+    values only feed the timing.  One mixed-precision matvec of 8 vectors
+    builds the split-BF16 operator (one GEMM1 + one GEMM2 launch); the GEMMs
+    are then timed at each chain count with CUDA events
+    (``ngw_profile_mixed_gemms``: one warm-up launch of each, then ``reps``)."""
+    import nanogw_b200 as ngw
+    from nanogw_b200.api import lowcomsym_pairs, sqrt_r
+    n_isdf, nocc, nemp = LARGE_OPERATORS[name]
+    rng = np.random.default_rng(1)
+    nmem = nocc + nemp
+    psi = np.asfortranarray(rng.standard_normal((n_isdf, nmem)) * 0.05)
+    g = rng.standard_normal((n_isdf, n_isdf)) / np.sqrt(n_isdf)
+    m = np.asfortranarray(g @ g.T * 0.02)
+    e1 = np.sort(np.concatenate([rng.uniform(-1.5, -0.5, nocc), rng.uniform(-0.3, 1.0, nemp)]))
+    cv = lowcomsym_pairs(nocc, nmem)
+    _, bf16, _, src = load_peaks()
+    out = {"operator": name, "n_isdf": n_isdf, "ncv": int(len(cv)), "peak_tflops": bf16,
+           "peak_source": f"{src} (bf16 dense, burst)", "values": "random (timing only)", "by_chains": {}}
+    with ngw.Session(local, "mixed") as s:
+        s.set_isdf(psi, m)
+        s.set_pairs(cv, sqrt_r(e1, cv))
+        s.matvec_isdf(rng.standard_normal((len(cv), 8)))
+        for nb in nbs:
+            us1, us2 = s.profile_mixed_gemms(nb, reps=reps)
+            M1, N1, K1, BN1, sp1, M2, N2, K2, BN2, v1, v2, _, _ = s.mixed_gemm_shapes(nb)
+            f1, f2 = 2.0 * M1 * N1 * K1, 2.0 * M2 * N2 * K2
+            out["by_chains"][str(nb)] = {
+                "us_per_launch": [us1, us2],
+                "shapes": [[M1, N1, K1, BN1, sp1, v1], [M2, N2, K2, BN2, 1, v2]],
+                "algorithmic_tflops": [f1 / us1 / 1e6, f2 / us2 / 1e6],
+                "executed_tflops": [3 * f1 / us1 / 1e6, 3 * f2 / us2 / 1e6],
+                "executed_frac": [3 * f1 / us1 / 1e6 / bf16, 3 * f2 / us2 / 1e6 / bf16],
+                "matvec_executed_frac": 3 * (f1 + f2) / (us1 + us2) / 1e6 / bf16}
+    return out
+
+
 def cpu_reference(op, qp, poly, wl, niter_sample):
     """The oracle (CPU restatement of the reference path, numpy/OpenBLAS on all
     host threads) on a bounded sample: one QP state, all band chains,
@@ -152,6 +198,11 @@ def main():
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling case: two mixed Sigma_c requests with --ncu-niter Lanczos steps")
     ap.add_argument("--ncu-niter", type=int, default=3)
+    ap.add_argument("--gemm-scan", default=None, choices=sorted(LARGE_OPERATORS),
+                    help="only time the matvec GEMMs at a large operator's dimensions")
+    ap.add_argument("--scan-chains", default="1024,2048")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the large-operator GEMM line of the default run")
     args = ap.parse_args()
     W = max(3, args.warmup)
     K = args.steps
@@ -170,6 +221,14 @@ def main():
 
     wl = dict(WORKLOAD)
     import nanogw_b200 as ngw
+
+    if args.gemm_scan:
+        if rank == 0:
+            nbs = [int(x) for x in args.scan_chains.split(",")]
+            print(json.dumps(gemm_scan(local, args.gemm_scan, nbs)), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     if args.impl == "reference":
         if rank != 0:
@@ -300,17 +359,29 @@ def main():
         cv_h = pin(cv)
         sr_h = pin(sr)
         e2e_t = []
+        phases = []
         for i in range(2 + max(2, K // 2)):
             t = time.perf_counter()
             sess.set_isdf(psi_h, m_h)
             sess.set_pairs(cv_h, sr_h)
-            solve_once(sess, op, qp, poly, wl, sigx, vxc)
+            t1 = time.perf_counter()
+            sig = sess.calculate_sigma_lanczos(op.e1, op.nval, qp, wl["nen"], wl["deltae"], wl["ecuts"],
+                                               wl["niter"], poly)
+            t2 = time.perf_counter()
+            e1q = op.e1[qp - 1] * RYD
+            sess.qp_newton(sig * RYD, e1q, e1q, wl["deltae"] * RYD, sigx, vxc)
+            t3 = time.perf_counter()
             if i >= 2:
-                e2e_t.append(time.perf_counter() - t)
+                e2e_t.append(t3 - t)
+                phases.append((t1 - t, t2 - t1, t3 - t2))
         h2d = psi_h.nbytes + m_h.nbytes + cv_h.nbytes + sr_h.nbytes + op.e1.nbytes + 4 * nq * 8
         d2h = wl["nen"] * nq * 16 + nq * (8 + 8 + 4)
+        ph = np.median(np.array(phases), axis=0) * 1e3
         e2e = {"value": world * nq / float(np.mean(e2e_t)), "unit": "solves/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "median_ms": {"upload": float(ph[0]), "sigma_incl_operator_build": float(ph[1]),
+                             "qp_newton": float(ph[2])},
+               "step_ms": [round(1e3 * x, 2) for x in e2e_t]}
 
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
@@ -319,6 +390,11 @@ def main():
         cpu = {"value": 1.0 / tcpu, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"1 QP state x {op.nmem} chains x {args.cpu_niter} Lanczos steps, scaled to "
                          f"{wl['niter']} steps (oracle: numpy/OpenBLAS FP64)"}
+
+    # ---- the same GEMM kernels at the large single-molecule operator's size ----
+    large = None
+    if rank == 0 and world == 1 and args.precision == "mixed" and not args.no_large:
+        large = gemm_scan(local, "large-molecule", [2048])
 
     launches_per_step = wl["niter"] * (wl["npoly"] * 3 + 1) + 8
     if rank == 0:
@@ -338,7 +414,8 @@ def main():
                 "qp_err_mev_vs_fp64": qp_err_mev,
                 "setup_ms": {"isdf_fit_and_coulomb_kernel": 1e3 * isdf_build_s,
                              "grid_points": int(op.mol.psi.shape[0]), "n_isdf": int(op.n_isdf)},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "roofline": roof, "roofline_large_operator": large, "cpu_baseline": cpu, "e2e": e2e,
+                "clocks": clk,
                 "gpu_launches": K * launches_per_step}
         print(json.dumps(line), flush=True)
     sess.close()

@@ -3,10 +3,14 @@
 // FP64 GEMMs of the plain path go through cuBLAS (library GEMMs); every other
 // step is a kernel of this library.
 #include <algorithm>
+#include <chrono>
+#include <string>
 #include <cstdarg>
 #include <cstring>
 #include <cmath>
 #include <vector>
+
+#include <cusolverDn.h>
 
 #include "ngw_internal.h"
 
@@ -56,6 +60,7 @@ int scratch(ngw_session *s, int slot, size_t bytes, void **p) {
   if ((int)s->scratch.size() <= slot) s->scratch.resize(slot + 1);
   DBuf &b = s->scratch[slot];
   if (b.bytes < bytes) {
+    bump_generation(s);
     if (b.p) {
       NGW_CUDA(cudaStreamSynchronize(s->stream));
       dfree(s, b.p, b.bytes);
@@ -79,6 +84,31 @@ int check_status(ngw_session *s) {
     set_error("device status %d (%s)", h, h == DEV_TIMEOUT ? "bounded wait timed out" : "index check");
     return h == DEV_TIMEOUT ? NGW_ERR_TIMEOUT : NGW_ERR_CUDA;
   }
+  return NGW_OK;
+}
+
+void bump_generation(ngw_session *s) {
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto &g : s->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  s->graphs.clear();
+  ++s->gen;
+}
+
+int session_cusolver(ngw_session *s, void **handle) {
+  if (!s->cusolver) {
+    cusolverDnHandle_t h = nullptr;
+    if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) {
+      set_error("cusolverDnCreate failed");
+      return NGW_ERR_CUDA;
+    }
+    s->cusolver = h;
+  }
+  if (cusolverDnSetStream((cusolverDnHandle_t)s->cusolver, s->stream) != CUSOLVER_STATUS_SUCCESS) {
+    set_error("cusolverDnSetStream failed");
+    return NGW_ERR_CUDA;
+  }
+  *handle = s->cusolver;
   return NGW_OK;
 }
 
@@ -185,6 +215,35 @@ static int lanczos_dev(ngw_session *s, const PolyPlan &pp, int nb, int niter, do
   return NGW_OK;
 }
 
+// NGW_TIMING=1: host wall-clock of the phases of a call on stderr (the
+// stream is synchronised at each mark, so only for diagnosis).
+struct PhaseTimer {
+  ngw_session *s;
+  bool on;
+  std::chrono::steady_clock::time_point t;
+  std::string line;
+  explicit PhaseTimer(ngw_session *s_) : s(s_) {
+    const char *e = getenv("NGW_TIMING");
+    on = e && e[0] == '1';
+    if (on) {
+      cudaStreamSynchronize(s->stream);
+      t = std::chrono::steady_clock::now();
+    }
+  }
+  void mark(const char *name) {
+    if (!on) return;
+    cudaStreamSynchronize(s->stream);
+    const auto now = std::chrono::steady_clock::now();
+    char buf[96];
+    snprintf(buf, sizeof(buf), " %s=%.2fms", name, std::chrono::duration<double, std::milli>(now - t).count());
+    line += buf;
+    t = now;
+  }
+  ~PhaseTimer() {
+    if (on) fprintf(stderr, "ngw timing:%s\n", line.c_str());
+  }
+};
+
 static int need_op(ngw_session *s) {
   if (!s) {
     set_error("null session");
@@ -216,12 +275,14 @@ static double poly_eval(const std::vector<double> &p, double x) {
 // recurrence only ever sees a spectrum on which p is bounded.
 static int plan_mixed(ngw_session *s, PolyPlan &pp, double lo_in, double hi_in) {
   const int tda = pp.tamm_d;
+  PhaseTimer tm(s);
   if (hi_in > lo_in) {
     pp.c0 = 0.5 * (hi_in + lo_in);
     pp.c1 = 0.5 * (hi_in - lo_in);
     pp.kdef = 0;
   } else {
     if (s->eig_tda != tda) NGW_TRY(compute_top_eigs(s, tda, 64, 240));
+    tm.mark("eigenpairs");
     const std::vector<double> &r = s->eig_vals, &res = s->eig_res;
     const int mm = (int)r.size();
     int k = 0;
@@ -253,7 +314,10 @@ static int plan_mixed(ngw_session *s, PolyPlan &pp, double lo_in, double hi_in) 
     pp.cheb.resize(pp.npoly + 1);
     monomial_to_chebyshev(pp.poly.data(), pp.npoly, pp.c0 - pp.c1, pp.c0 + pp.c1, pp.cheb.data());
   }
-  if (!s->mixed || mixed_kdef(s) != pp.kdef) NGW_TRY(mixed_build_operator(s, pp.kdef, tda));
+  tm.mark("interval");
+  if (!s->mixed || s->mixed_dirty || mixed_kdef(s) != pp.kdef)
+    NGW_TRY(mixed_build_operator(s, pp.kdef, tda));
+  tm.mark("split_operator");
   std::vector<double> pv(pp.kdef);
   for (int j = 0; j < pp.kdef; ++j) pv[j] = tda ? s->eig_vals[j] : poly_eval(pp.poly, s->eig_vals[j]);
   NGW_TRY(mixed_set_deflation_values(s, pv.data()));
@@ -404,6 +468,7 @@ void ngw_session_destroy(ngw_session *s) {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->cublas) cublasDestroy(s->cublas);
+  if (s->cusolver) cusolverDnDestroy((cusolverDnHandle_t)s->cusolver);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -435,28 +500,37 @@ int ngw_set_isdf(ngw_session *s, int n_isdf, int nmem, const double *psi_intp, c
   }
   NGW_CUDA(cudaSetDevice(s->device));
   NGW_CUDA(cudaStreamSynchronize(s->stream));
-  mixed_free(s);
-  if (s->d_psi) dfree(s, s->d_psi, (size_t)s->n_isdf * s->nmem * 8);
-  if (s->d_M) dfree(s, s->d_M, (size_t)s->n_isdf * s->n_isdf * 8);
-  if (s->d_Mxc) dfree(s, s->d_Mxc, (size_t)s->n_isdf * s->n_isdf * 8);
-  if (s->d_C) dfree(s, s->d_C, (size_t)s->n_isdf * s->ncv * 8);
-  s->d_psi = s->d_M = s->d_Mxc = s->d_C = nullptr;
+  // Same shapes: the new values go into the existing buffers, so captured
+  // graphs (which hold buffer addresses) stay valid; every value derived from
+  // the operator (pair products, eigenpairs, split-BF16 operands) is rebuilt.
+  const bool same = s->have_isdf && s->n_isdf == n_isdf && s->nmem == nmem &&
+                    (mxc != nullptr) == (s->d_Mxc != nullptr);
+  if (!same) {
+    bump_generation(s);
+    mixed_free(s);
+    if (s->d_psi) dfree(s, s->d_psi, (size_t)s->n_isdf * s->nmem * 8);
+    if (s->d_M) dfree(s, s->d_M, (size_t)s->n_isdf * s->n_isdf * 8);
+    if (s->d_Mxc) dfree(s, s->d_Mxc, (size_t)s->n_isdf * s->n_isdf * 8);
+    if (s->d_C) dfree(s, s->d_C, (size_t)s->n_isdf * s->ncv * 8);
+    s->d_psi = s->d_M = s->d_Mxc = s->d_C = nullptr;
+    s->n_isdf = n_isdf;
+    s->nmem = nmem;
+    NGW_TRY(dalloc(s, (void **)&s->d_psi, (size_t)n_isdf * nmem * 8));
+    NGW_TRY(dalloc(s, (void **)&s->d_M, (size_t)n_isdf * n_isdf * 8));
+    if (mxc) NGW_TRY(dalloc(s, (void **)&s->d_Mxc, (size_t)n_isdf * n_isdf * 8));
+    if (s->have_pairs) NGW_TRY(dalloc(s, (void **)&s->d_C, (size_t)n_isdf * s->ncv * 8));
+  } else {
+    s->mixed_dirty = true;
+  }
   s->have_C = false;
   s->eig_tda = -1;
-  s->n_isdf = n_isdf;
-  s->nmem = nmem;
-  NGW_TRY(dalloc(s, (void **)&s->d_psi, (size_t)n_isdf * nmem * 8));
-  NGW_TRY(dalloc(s, (void **)&s->d_M, (size_t)n_isdf * n_isdf * 8));
   NGW_CUDA(cudaMemcpyAsync(s->d_psi, psi_intp, (size_t)n_isdf * nmem * 8, cudaMemcpyHostToDevice,
                            s->stream));
   NGW_CUDA(cudaMemcpyAsync(s->d_M, mmtrx, (size_t)n_isdf * n_isdf * 8, cudaMemcpyHostToDevice,
                            s->stream));
-  if (mxc) {
-    NGW_TRY(dalloc(s, (void **)&s->d_Mxc, (size_t)n_isdf * n_isdf * 8));
+  if (mxc)
     NGW_CUDA(cudaMemcpyAsync(s->d_Mxc, mxc, (size_t)n_isdf * n_isdf * 8, cudaMemcpyHostToDevice,
                              s->stream));
-  }
-  if (s->have_pairs) NGW_TRY(dalloc(s, (void **)&s->d_C, (size_t)n_isdf * s->ncv * 8));
   s->have_isdf = true;
   NGW_CUDA(cudaStreamSynchronize(s->stream));
   return NGW_OK;
@@ -481,20 +555,26 @@ int ngw_set_pairs(ngw_session *s, int ncv, const int *cvpair, const double *sqrt
   }
   NGW_CUDA(cudaSetDevice(s->device));
   NGW_CUDA(cudaStreamSynchronize(s->stream));
-  mixed_free(s);
-  if (s->d_cvpair) dfree(s, s->d_cvpair, (size_t)2 * s->ncv * 4);
-  if (s->d_sqrtR) dfree(s, s->d_sqrtR, (size_t)s->ncv * 8);
-  if (s->d_C) dfree(s, s->d_C, (size_t)s->n_isdf * s->ncv * 8);
-  s->d_C = nullptr;
+  const bool same = s->have_pairs && s->ncv == ncv && (!s->have_isdf || s->d_C);
+  if (!same) {
+    bump_generation(s);
+    mixed_free(s);
+    if (s->d_cvpair) dfree(s, s->d_cvpair, (size_t)2 * s->ncv * 4);
+    if (s->d_sqrtR) dfree(s, s->d_sqrtR, (size_t)s->ncv * 8);
+    if (s->d_C) dfree(s, s->d_C, (size_t)s->n_isdf * s->ncv * 8);
+    s->d_C = nullptr;
+    s->ncv = ncv;
+    NGW_TRY(dalloc(s, (void **)&s->d_cvpair, (size_t)2 * ncv * 4));
+    NGW_TRY(dalloc(s, (void **)&s->d_sqrtR, (size_t)ncv * 8));
+    if (s->have_isdf) NGW_TRY(dalloc(s, (void **)&s->d_C, (size_t)s->n_isdf * ncv * 8));
+  } else {
+    s->mixed_dirty = true;
+  }
   s->have_C = false;
   s->eig_tda = -1;
-  s->ncv = ncv;
-  NGW_TRY(dalloc(s, (void **)&s->d_cvpair, (size_t)2 * ncv * 4));
-  NGW_TRY(dalloc(s, (void **)&s->d_sqrtR, (size_t)ncv * 8));
   NGW_CUDA(cudaMemcpyAsync(s->d_cvpair, cvpair, (size_t)2 * ncv * 4, cudaMemcpyHostToDevice,
                            s->stream));
   NGW_CUDA(cudaMemcpyAsync(s->d_sqrtR, sqrtR, (size_t)ncv * 8, cudaMemcpyHostToDevice, s->stream));
-  if (s->have_isdf) NGW_TRY(dalloc(s, (void **)&s->d_C, (size_t)s->n_isdf * ncv * 8));
   s->have_pairs = true;
   NGW_CUDA(cudaStreamSynchronize(s->stream));
   return NGW_OK;
@@ -651,7 +731,13 @@ int ngw_k_integrate_isdf(ngw_session *s, int kflag, const int *rows, int nrow, c
 
 int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e1,
                       double *sigma_c, double *alpha, double *beta) {
+  if (!s) {
+    set_error("ngw_sigma_lanczos: null session");
+    return NGW_ERR_ARG;
+  }
+  PhaseTimer tm(s);
   NGW_TRY(need_op(s));
+  tm.mark("pair_products");
   if (!p || !e1 || !sigma_c || p->nen < 2 || p->niter < 1 || p->nqp < 1 || !p->qp_bands ||
       p->nval < 1 || p->nval >= s->nmem) {
     set_error("ngw_sigma_lanczos: bad arguments");
@@ -680,6 +766,7 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
   double lo = p->cheb_lo, hi = p->cheb_hi;
   PolyPlan pp;
   NGW_TRY(make_plan(s, pp, p->polynomial, p->npoly, tamm_d, lo, hi));
+  tm.mark("plan");
   // chain blocking: whole QP states per block
   int nq_blk = p->nqp;
   if (p->block_chains > 0) nq_blk = std::max(1, std::min(p->nqp, p->block_chains / nbsum));
@@ -753,7 +840,7 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
         (unsigned long long)pp.npoly, (unsigned long long)tamm_d, (unsigned long long)nen,
         (unsigned long long)p->nval, (unsigned long long)nbsum, (unsigned long long)nq,
         (unsigned long long)q0, (unsigned long long)pp.kdef, dbits(p->ecuts), dbits(de),
-        dbits(pp.c0), dbits(pp.c1)};
+        dbits(pp.c0), dbits(pp.c1), s->gen};
     for (double c : pp.poly) key.push_back(dbits(c));
     for (double c : pp.cheb) key.push_back(dbits(c));
     for (const void *ptr : {(const void *)cmn, (const void *)cm, (const void *)P, (const void *)P2,
@@ -767,7 +854,9 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
       extern_mixed_tune(s, tune);
       for (int t : tune) key.push_back((unsigned long long)t);
     }
+    tm.mark("block_setup");
     NGW_TRY(run_graphed(s, key, region));
+    tm.mark("region");
     if (alpha)
       NGW_CUDA(cudaMemcpyAsync(alpha + (size_t)q0 * nbsum * niter, a, (size_t)niter * nb * 8,
                                cudaMemcpyDeviceToHost, s->stream));

@@ -18,56 +18,80 @@
 #include <numeric>
 #include <vector>
 
+#include <cusolverDn.h>
+
 #include "ngw_internal.h"
 
 namespace ngw {
 
 int matvec_f64_dev_pub(ngw_session *s, int nb, double *hs, double *y, int tamm_d);
 
-// Cyclic Jacobi eigen-decomposition of a small dense symmetric matrix
-// (column-major n x n, destroyed).  Eigenvalues to w, eigenvectors as the
-// columns of V.  Quadratically convergent; n <= a few hundred here.
-static void jacobi_eig(std::vector<double> &A, int n, std::vector<double> &w, std::vector<double> &V) {
-  V.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
-  auto a = [&](int i, int j) -> double & { return A[(size_t)j * n + i]; };
-  for (int sweep = 0; sweep < 60; ++sweep) {
-    double off = 0.0, tot = 0.0;
-    for (int j = 0; j < n; ++j)
-      for (int i = 0; i < n; ++i) {
-        const double x = a(i, j) * a(i, j);
-        tot += x;
-        if (i != j) off += x;
-      }
-    if (off <= 1e-30 * tot) break;
-    for (int p = 0; p < n - 1; ++p) {
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = a(p, q);
-        if (std::fabs(apq) < 1e-300) continue;
-        const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
-        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
-        for (int k = 0; k < n; ++k) {          // columns p, q
-          const double akp = a(k, p), akq = a(k, q);
-          a(k, p) = c * akp - sn * akq;
-          a(k, q) = sn * akp + c * akq;
-        }
-        for (int k = 0; k < n; ++k) {          // rows p, q
-          const double apk = a(p, k), aqk = a(q, k);
-          a(p, k) = c * apk - sn * aqk;
-          a(q, k) = sn * apk + c * aqk;
-        }
-        for (int k = 0; k < n; ++k) {
-          double &vp = V[(size_t)p * n + k], &vq = V[(size_t)q * n + k];
-          const double x = vp, y = vq;
-          vp = c * x - sn * y;
-          vq = sn * x + c * y;
-        }
-      }
+// v_next = w / beta with beta = ||w|| already on the device (0 when beta is 0:
+// the run is cut at the first negligible beta after the loop)
+__global__ void k_lanczos_next(const double *__restrict__ w, const double *__restrict__ beta, int ncv,
+                               double *__restrict__ vnext) {
+  const double b = *beta;
+  const double inv = b > 0.0 ? 1.0 / b : 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x)
+    vnext[i] = w[i] * inv;
+}
+
+// Eigen-decomposition of the small symmetric Lanczos matrix T (column-major
+// n x n) on the device with cuSOLVER's divide-and-conquer solver: ascending
+// eigenvalues to w, orthonormal eigenvectors as the columns of V.
+static int sym_eig(ngw_session *s, const std::vector<double> &T, int n, std::vector<double> &w,
+                   std::vector<double> &V) {
+  void *hv = nullptr;
+  NGW_TRY(session_cusolver(s, &hv));
+  cusolverDnHandle_t h = (cusolverDnHandle_t)hv;
+  double *dA = nullptr, *dW = nullptr, *work = nullptr;
+  int *info = nullptr;
+  int lwork = 0, rc = NGW_OK;
+  const size_t ab = (size_t)n * n * 8;
+  do {
+    if ((rc = dalloc(s, (void **)&dA, ab)) || (rc = dalloc(s, (void **)&dW, (size_t)n * 8)) ||
+        (rc = dalloc(s, (void **)&info, 4)))
+      break;
+    if (cudaMemcpyAsync(dA, T.data(), ab, cudaMemcpyHostToDevice, s->stream) != cudaSuccess) {
+      set_error("copy of the Lanczos matrix failed");
+      rc = NGW_ERR_CUDA;
+      break;
     }
-  }
-  w.resize(n);
-  for (int i = 0; i < n; ++i) w[i] = a(i, i);
+    if (cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dA, n, dW,
+                                    &lwork) != CUSOLVER_STATUS_SUCCESS) {
+      set_error("cusolverDnDsyevd_bufferSize failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    if ((rc = dalloc(s, (void **)&work, (size_t)std::max(lwork, 1) * 8))) break;
+    if (cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dA, n, dW, work, lwork,
+                         info) != CUSOLVER_STATUS_SUCCESS) {
+      set_error("cusolverDnDsyevd failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    int hinfo = 0;
+    w.resize(n);
+    V.resize((size_t)n * n);
+    if (cudaMemcpyAsync(w.data(), dW, (size_t)n * 8, cudaMemcpyDeviceToHost, s->stream) ||
+        cudaMemcpyAsync(V.data(), dA, ab, cudaMemcpyDeviceToHost, s->stream) ||
+        cudaMemcpyAsync(&hinfo, info, 4, cudaMemcpyDeviceToHost, s->stream) ||
+        cudaStreamSynchronize(s->stream)) {
+      set_error("copy of the Ritz pairs failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    if (hinfo != 0) {
+      set_error("symmetric eigen-solve of the Lanczos matrix did not converge (info %d)", hinfo);
+      rc = NGW_ERR_NOCONV;
+    }
+  } while (0);
+  cudaStreamSynchronize(s->stream);
+  dfree(s, dA, ab);
+  dfree(s, dW, (size_t)n * 8);
+  dfree(s, info, 4);
+  if (work) dfree(s, work, (size_t)std::max(lwork, 1) * 8);
+  return rc;
 }
 
 // FP64 Lanczos with full (twice-applied) reorthogonalisation on one vector.
@@ -93,32 +117,57 @@ int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
   nrm = std::sqrt(nrm);
   for (double &x : v0) x /= nrm;
   NGW_CUDA(cudaMemcpyAsync(V, v0.data(), (size_t)ncv * 8, cudaMemcpyHostToDevice, s->stream));
-  std::vector<double> alpha(m), beta(m + 1, 0.0);
+  // The loop is asynchronous: alpha_j = <v_j, w> (first Gram-Schmidt pass)
+  // and beta_{j+1} = ||w|| stay on the device and are read back once.
+  double *dab = nullptr;   // alpha (m) then beta (m + 1)
+  NGW_TRY(dalloc(s, (void **)&dab, (size_t)(2 * m + 1) * 8));
+  NGW_CUDA(cudaMemsetAsync(dab, 0, (size_t)(2 * m + 1) * 8, s->stream));
+  double *dalpha = dab, *dbeta = dab + m;
   const double one = 1.0, mone = -1.0, zero = 0.0;
-  int mm = m;
-  for (int j = 0; j < m; ++j) {
+  const int nblk = std::min(148 * 4, (ncv + 255) / 256);
+  int rc = NGW_OK;
+  for (int j = 0; j < m && rc == NGW_OK; ++j) {
     double *vj = V + (size_t)j * ncv;
     launch_scale_rows(s->d_sqrtR, vj, ncv, hs, ncv, ncv, 1, tamm_d, s->stream);
-    NGW_TRY(matvec_f64_dev_pub(s, 1, hs, w, tamm_d));
+    if ((rc = matvec_f64_dev_pub(s, 1, hs, w, tamm_d)) != NGW_OK) break;
     // two passes of classical Gram-Schmidt against all previous vectors
-    for (int pass = 0; pass < 2; ++pass) {
-      NGW_CUBLAS(cublasDgemv(s->cublas, CUBLAS_OP_T, ncv, j + 1, &one, V, ncv, w, 1, &zero, h, 1));
-      if (pass == 0) NGW_CUDA(cudaMemcpyAsync(&alpha[j], h + j, 8, cudaMemcpyDeviceToHost, s->stream));
-      NGW_CUBLAS(cublasDgemv(s->cublas, CUBLAS_OP_N, ncv, j + 1, &mone, V, ncv, h, 1, &one, w, 1));
+    for (int pass = 0; pass < 2 && rc == NGW_OK; ++pass) {
+      if (cublasDgemv(s->cublas, CUBLAS_OP_T, ncv, j + 1, &one, V, ncv, w, 1, &zero, h, 1) ||
+          (pass == 0 && cudaMemcpyAsync(dalpha + j, h + j, 8, cudaMemcpyDeviceToDevice, s->stream)) ||
+          cublasDgemv(s->cublas, CUBLAS_OP_N, ncv, j + 1, &mone, V, ncv, h, 1, &one, w, 1)) {
+        set_error("eigenpair Lanczos: Gram-Schmidt step failed");
+        rc = NGW_ERR_CUDA;
+      }
     }
-    double b = 0.0;
-    NGW_CUBLAS(cublasDnrm2(s->cublas, ncv, w, 1, &b));   // synchronises (host pointer mode)
-    beta[j + 1] = b;
-    if (!(b > 1e-13 * std::fabs(alpha[0]))) {
+    if (rc != NGW_OK) break;
+    cublasSetPointerMode(s->cublas, CUBLAS_POINTER_MODE_DEVICE);
+    const cublasStatus_t st2 = cublasDnrm2(s->cublas, ncv, w, 1, dbeta + j + 1);
+    cublasSetPointerMode(s->cublas, CUBLAS_POINTER_MODE_HOST);
+    if (st2 != CUBLAS_STATUS_SUCCESS) {
+      set_error("eigenpair Lanczos: norm failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    k_lanczos_next<<<nblk, 256, 0, s->stream>>>(w, dbeta + j + 1, ncv, V + (size_t)(j + 1) * ncv);
+  }
+  std::vector<double> alpha(m), beta(m + 1, 0.0);
+  if (rc == NGW_OK &&
+      (cudaGetLastError() != cudaSuccess ||
+       cudaMemcpyAsync(alpha.data(), dalpha, (size_t)m * 8, cudaMemcpyDeviceToHost, s->stream) ||
+       cudaMemcpyAsync(beta.data(), dbeta, (size_t)(m + 1) * 8, cudaMemcpyDeviceToHost, s->stream))) {
+    set_error("eigenpair Lanczos: launch or copy failed");
+    rc = NGW_ERR_CUDA;
+  }
+  cudaStreamSynchronize(s->stream);
+  dfree(s, dab, (size_t)(2 * m + 1) * 8);
+  NGW_TRY(rc);
+  // cut the run at the first negligible beta (invariant subspace found)
+  int mm = m;
+  for (int j = 0; j < m; ++j)
+    if (!(beta[j + 1] > 1e-13 * std::fabs(alpha[0]))) {
       mm = j + 1;
       break;
     }
-    const double inv = 1.0 / b;
-    NGW_CUBLAS(cublasDscal(s->cublas, ncv, &inv, w, 1));
-    NGW_CUDA(cudaMemcpyAsync(V + (size_t)(j + 1) * ncv, w, (size_t)ncv * 8, cudaMemcpyDeviceToDevice,
-                             s->stream));
-  }
-  NGW_CUDA(cudaStreamSynchronize(s->stream));
   // Ritz pairs of the tridiagonal
   std::vector<double> T((size_t)mm * mm, 0.0), ev, Y;
   for (int i = 0; i < mm; ++i) {
@@ -128,7 +177,7 @@ int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
       T[(size_t)i * mm + i + 1] = beta[i + 1];
     }
   }
-  jacobi_eig(T, mm, ev, Y);
+  NGW_TRY(sym_eig(s, T, mm, ev, Y));
   std::vector<int> ord(mm);
   std::iota(ord.begin(), ord.end(), 0);
   std::sort(ord.begin(), ord.end(), [&](int x, int y) { return ev[x] > ev[y]; });
@@ -145,9 +194,13 @@ int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
     for (int r = 0; r < mm; ++r) Yk[(size_t)c * mm + r] = Y[(size_t)ord[c] * mm + r];
   double *dY = nullptr;
   NGW_TRY(dalloc(s, (void **)&dY, (size_t)mm * k * 8));
-  if (s->eig_U) dfree(s, s->eig_U, s->eig_U_bytes);
-  s->eig_U_bytes = (size_t)ncv * std::max(k, 1) * 8;
-  NGW_TRY(dalloc(s, (void **)&s->eig_U, s->eig_U_bytes));
+  const size_t ubytes = (size_t)ncv * std::max(k, 1) * 8;
+  if (!s->eig_U || s->eig_U_bytes != ubytes) {   // captured graphs hold eig_U's address
+    bump_generation(s);
+    if (s->eig_U) dfree(s, s->eig_U, s->eig_U_bytes);
+    s->eig_U_bytes = ubytes;
+    NGW_TRY(dalloc(s, (void **)&s->eig_U, s->eig_U_bytes));
+  }
   NGW_CUDA(cudaMemcpyAsync(dY, Yk.data(), (size_t)mm * k * 8, cudaMemcpyHostToDevice, s->stream));
   if (k > 0)
     NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, ncv, k, mm, &one, V, ncv, dY, mm, &zero,

@@ -34,6 +34,7 @@ int isdf_fit_device(ngw_session *s, int ngrid, int nmem, const double *d_psi, co
   double *P = nullptr, *Q = nullptr, *Ai = nullptr, *Qi = nullptr, *work = nullptr;
   int *ipiv = nullptr, *info = nullptr;
   cusolverDnHandle_t sol = nullptr;
+  void *hv = nullptr;
   int rc = NGW_OK;
   const size_t pb = (size_t)n_isdf * ngrid * 8, ab = (size_t)n_isdf * n_isdf * 8;
   int lwork = 0;
@@ -62,12 +63,8 @@ int isdf_fit_device(ngw_session *s, int ngrid, int nmem, const double *d_psi, co
     }
     k_hadamard<<<2048, 256, 0, s->stream>>>(P, Q, (size_t)n_isdf * ngrid);
     k_hadamard<<<256, 256, 0, s->stream>>>(Ai, Qi, (size_t)n_isdf * n_isdf);
-    if (cusolverDnCreate(&sol) != CUSOLVER_STATUS_SUCCESS) {
-      set_error("cusolverDnCreate failed");
-      rc = NGW_ERR_CUDA;
-      break;
-    }
-    cusolverDnSetStream(sol, s->stream);
+    if ((rc = session_cusolver(s, &hv)) != NGW_OK) break;
+    sol = (cusolverDnHandle_t)hv;
     if (cusolverDnDgetrf_bufferSize(sol, n_isdf, n_isdf, Ai, n_isdf, &lwork) != CUSOLVER_STATUS_SUCCESS ||
         dalloc(s, (void **)&work, (size_t)std::max(lwork, 1) * 8)) {
       set_error("getrf workspace failed");
@@ -95,7 +92,6 @@ int isdf_fit_device(ngw_session *s, int ngrid, int nmem, const double *d_psi, co
     }
   } while (0);
   cudaStreamSynchronize(s->stream);
-  if (sol) cusolverDnDestroy(sol);
   dfree(s, Q, pb);
   dfree(s, Ai, ab);
   dfree(s, Qi, ab);

@@ -87,7 +87,14 @@ struct ngw_session {
     int seen = 0;
   };
   std::vector<GraphEntry> graphs;
+  // bumped whenever a device buffer that captured graphs may reference is
+  // freed or reallocated; part of every graph key
+  unsigned long long gen = 0;
+  // the mixed operator's values are stale (new Psi_intp / M / pairs of the
+  // same shapes were uploaded into the existing buffers)
+  bool mixed_dirty = false;
   void *cublas_ws = nullptr;
+  void *cusolver = nullptr;    // cusolverDnHandle_t, created on first use
   bool use_graphs = true;
   // scratch (grown on demand)
   std::vector<ngw::DBuf> scratch;
@@ -101,6 +108,11 @@ int dalloc(ngw_session *s, void **p, size_t bytes);
 void dfree(ngw_session *s, void *p, size_t bytes);
 int scratch(ngw_session *s, int slot, size_t bytes, void **p);
 int check_status(ngw_session *s);
+// Device buffers of the operator / chains / scratch are about to change: wait
+// for the stream, drop every captured graph and advance the generation.
+void bump_generation(ngw_session *s);
+// session's cuSOLVER dense handle on the session stream (created on first use)
+int session_cusolver(ngw_session *s, void **handle);
 
 // ---- FP64 path kernels (kernels_core.cu) ----
 void launch_pair_gather_f64(const double *psi, int n_isdf, const int *cvpair, int ncv,
