@@ -113,11 +113,31 @@ typedef struct {
   int nbands_sum;          /* bands n summed over: 1..nbands_sum (0 = nmem) */
   int block_chains;        /* chains per device block (0 = all that fit) */
   double cheb_lo, cheb_hi; /* mixed mode: Chebyshev interval (0,0 = auto) */
+  const int *chain_niter;  /* optional per-chain Lanczos lengths 1..niter, nqp x nbands_sum
+                              (chain = iq*nbands_sum + n-1); NULL = niter for every chain */
+  double early_exit_eps;   /* > 0: a chain stops when |b_k| < eps (convergence mask, as
+                              shared/lanczos_spectra.f90:24,58); 0 = never (lowcomsym) */
 } ngw_sigma_params;
+
+/* ngw_lanczos_spectra_isdf with per-chain lengths and a convergence mask:
+ * chain_niter (blksz, 1..niter, NULL = niter) and early_exit_eps (> 0: a
+ * chain stops when |b_k| < eps; its later alpha / beta are 0 and its
+ * continued fraction ends there).  The single-vector reference routine
+ * (lanczos_spectra_isdf, shared/lanczos_spectra.f90:7) is this call with
+ * blksz = 1 and eps = 1e-8 (:24,58); the BLOCK / lowcomsym forms have no exit
+ * (eps = 0, what ngw_lanczos_spectra_isdf does). */
+int ngw_lanczos_spectra_isdf_masked(ngw_session *s, const double *v0, const double *v0_norm, int ld,
+                                    const double *zz, int nz, int niter, const double *polynomial,
+                                    int npoly, int blksz, int tamm_d, const int *chain_niter,
+                                    double early_exit_eps, double *spectra, double *alpha,
+                                    double *beta);
 
 /* Sigma_c(omega) for every QP state: sigma_c complex128 interleaved,
  * (nen x nqp) column-major, in Ry.  e1: KS energies (nmem), Ry.
- * alpha/beta (niter x nchains, chain = iq*nbands_sum + n) optional. */
+ * alpha/beta (niter x nchains, chain = iq*nbands_sum + n) optional; entries
+ * past a chain's length (or its convergence stop) are 0.  With per-chain
+ * lengths the chains of a block run longest first and each step's matvecs
+ * cover only the chains still running. */
 int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e1,
                       double *sigma_c, double *alpha, double *beta);
 

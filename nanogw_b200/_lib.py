@@ -39,6 +39,8 @@ SIGNATURES = {
     "ngw_matvec_isdf": (_I, [_P, _P, _P, _I, _I, _I]),
     "ngw_polynomial_matvec_isdf": (_I, [_P, _P, _I, _P, _P, _I, _I]),
     "ngw_lanczos_spectra_isdf": (_I, [_P, _P, _P, _I, _P, _I, _I, _P, _I, _I, _I, _P, _P, _P]),
+    "ngw_lanczos_spectra_isdf_masked": (_I, [_P, _P, _P, _I, _P, _I, _I, _P, _I, _I, _I, _P, _D, _P, _P,
+                                             _P]),
     "ngw_k_integrate_isdf": (_I, [_P, _I, _P, _I, _P, _I, _P]),
     "ngw_sigma_lanczos": (_I, [_P, _P, _P, _P, _P, _P]),
     "ngw_qp_newton": (_I, [_P, _I, _I, _P, _P, _P, _D, _P, _P, _D, _P, _P, _P]),
@@ -60,6 +62,7 @@ class SigmaParams(ctypes.Structure):
         ("nen", _I), ("deltae", _D), ("ecuts", _D), ("niter", _I), ("npoly", _I),
         ("polynomial", _P), ("tamm_d", _I), ("nval", _I), ("nqp", _I), ("qp_bands", _P),
         ("nbands_sum", _I), ("block_chains", _I), ("cheb_lo", _D), ("cheb_hi", _D),
+        ("chain_niter", _P), ("early_exit_eps", _D),
     ]
 
 

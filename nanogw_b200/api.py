@@ -114,7 +114,11 @@ class Session:
                                                v.shape[0], v.shape[1]))
         return out if np.ndim(vec) == 2 else out[:, 0]
 
-    def lanczos_spectra_isdf(self, v0, v0_norm, zz, niter, polynomial=None, tamm_d=False):
+    def lanczos_spectra_isdf(self, v0, v0_norm, zz, niter, polynomial=None, tamm_d=False,
+                             chain_niter=None, early_exit_eps=0.0):
+        """<v|1/(zz - p(H))|v> per column.  chain_niter: optional per-chain
+        Lanczos lengths; early_exit_eps > 0: a chain stops when |b_k| < eps
+        (the single-vector reference form uses 1e-8)."""
         v = _f64(v0 if np.ndim(v0) == 2 else np.asarray(v0)[:, None])
         nb = v.shape[1]
         nrm = np.ascontiguousarray(np.broadcast_to(np.asarray(v0_norm, dtype=np.float64), (nb,)))
@@ -130,8 +134,16 @@ class Session:
         else:
             poly = np.ascontiguousarray(polynomial, dtype=np.float64)
             npoly = len(poly) - 1
-        check(lib().ngw_lanczos_spectra_isdf(self._h, _p(v), _p(nrm), v.shape[0], _p(z), nz, int(niter),
-                                             _p(poly), npoly, nb, int(tamm_d), _p(spec), _p(a), _p(b)))
+        ln = None if chain_niter is None else np.ascontiguousarray(chain_niter, dtype=np.int32)
+        if ln is None and not early_exit_eps:
+            check(lib().ngw_lanczos_spectra_isdf(self._h, _p(v), _p(nrm), v.shape[0], _p(z), nz,
+                                                 int(niter), _p(poly), npoly, nb, int(tamm_d), _p(spec),
+                                                 _p(a), _p(b)))
+        else:
+            check(lib().ngw_lanczos_spectra_isdf_masked(self._h, _p(v), _p(nrm), v.shape[0], _p(z), nz,
+                                                        int(niter), _p(poly), npoly, nb, int(tamm_d),
+                                                        _p(ln), float(early_exit_eps), _p(spec), _p(a),
+                                                        _p(b)))
         return spec, a, b
 
     def k_integrate_isdf(self, kflag, rows, cols):
@@ -143,8 +155,10 @@ class Session:
 
     def calculate_sigma_lanczos(self, e1, nval, qp_bands, nen, deltae, ecuts, niter, polynomial,
                                 tamm_d=False, nbands_sum=0, block_chains=0, cheb=(0.0, 0.0),
-                                return_ab=False):
-        """Sigma_c(omega) (Ry) for each QP band: complex array (nen, nqp)."""
+                                return_ab=False, chain_niter=None, early_exit_eps=0.0):
+        """Sigma_c(omega) (Ry) for each QP band: complex array (nen, nqp).
+        chain_niter: optional (nqp, nbands_sum) per-chain Lanczos lengths
+        (1..niter); early_exit_eps > 0 stops a chain when |b_k| < eps."""
         e = np.ascontiguousarray(e1, dtype=np.float64)
         qp = np.ascontiguousarray(qp_bands, dtype=np.int32)
         poly = np.ascontiguousarray(polynomial if polynomial is not None else [1.0, 0.0],
@@ -154,7 +168,14 @@ class Session:
                           npoly=len(poly) - 1, polynomial=_p(poly), tamm_d=int(tamm_d),
                           nval=int(nval), nqp=len(qp), qp_bands=_p(qp), nbands_sum=int(nbands_sum),
                           block_chains=int(block_chains), cheb_lo=float(cheb[0]),
-                          cheb_hi=float(cheb[1]))
+                          cheb_hi=float(cheb[1]), chain_niter=None,
+                          early_exit_eps=float(early_exit_eps))
+        ln = None
+        if chain_niter is not None:
+            ln = np.ascontiguousarray(chain_niter, dtype=np.int32).reshape(-1)
+            if ln.size != len(qp) * nbs:
+                raise ValueError("chain_niter must have nqp * nbands_sum entries")
+            prm.chain_niter = _p(ln)
         sig = np.zeros((nen, len(qp)), dtype=np.complex128, order="F")
         a = b = None
         if return_ab:

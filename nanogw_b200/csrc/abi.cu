@@ -122,7 +122,7 @@ static bool all_finite(const double *x, size_t n) {
 enum {
   SL_IN = 0, SL_OUT, SL_HS, SL_T1, SL_T2, SL_Z, SL_VEC, SL_WVEC, SL_TMP, SL_A, SL_B, SL_ZZ,
   SL_SPEC, SL_CMN, SL_CM, SL_P, SL_P2, SL_PN2, SL_PN, SL_CHB, SL_CHQ, SL_E1, SL_ZZ0, SL_SIG,
-  SL_KR, SL_KC, SL_KM, SL_B1, SL_B2, SL_QPW, SL_QPIO, SL_SPECS, SL_NUM
+  SL_KR, SL_KC, SL_KM, SL_B1, SL_B2, SL_QPW, SL_QPIO, SL_SPECS, SL_CLEN, SL_LEN, SL_SLOT, SL_NUM
 };
 
 // ---------------------------------------------------------------------------
@@ -190,21 +190,30 @@ static int apply_poly(ngw_session *s, const PolyPlan &pp, int nb, const double *
 }
 
 // Lanczos recurrence for nb chains whose normalised start vectors are set up
-// by launch_lanczos_init.  Leaves a, b (niter x nb).
+// by launch_lanczos_init.  Leaves a, b (niter x nb).  clen: per-chain lengths
+// (set by launch_lanczos_init, lowered by the convergence mask eps);
+// nact[k] (optional): chains still scheduled at step k -- the chains are
+// ordered longest first, so step k's matvecs and updates cover chains
+// 0 .. nact[k]-1 only.
 static int lanczos_dev(ngw_session *s, const PolyPlan &pp, int nb, int niter, double *V,
-                       double *W, double *hs, double *tmp, double *a, double *b) {
+                       double *W, double *hs, double *tmp, double *a, double *b, int *clen,
+                       double eps, const std::vector<int> *nact) {
   // wvec = p(H) vec
   NGW_TRY(apply_poly(s, pp, nb, V, hs, W));
-  launch_lanczos_first(W, V, s->ncv, nb, a, b, niter, s->stream);
+  launch_lanczos_first(W, V, s->ncv, nb, a, b, niter, clen, eps, s->stream);
   // the scaled copy hs feeds only the FP64 path's first DGEMM
   double *hsn = (s->precision == NGW_PREC_MIXED) ? nullptr : hs;
+  auto active = [&](int k) { return nact ? (*nact)[k] : nb; };
   if (niter >= 2)
-    launch_lanczos_prescale(W, V, s->ncv, nb, 1, b, niter, s->d_sqrtR, hsn, pp.tamm_d, s->stream);
+    launch_lanczos_prescale(W, V, s->ncv, active(1), 1, b, niter, s->d_sqrtR, hsn, pp.tamm_d, clen,
+                            s->stream);
   double *vec = W, *wvec = V;   // roles after the swap
   for (int k = 1; k < niter; ++k) {
-    NGW_TRY(apply_poly(s, pp, nb, vec, hs, tmp));
-    launch_lanczos_step(wvec, vec, tmp, s->ncv, nb, k, a, b, niter, s->d_sqrtR, hsn, pp.tamm_d,
-                        (k + 1 < niter) ? 1 : 0, s->stream);
+    const int nk = active(k);
+    if (nk <= 0) break;
+    NGW_TRY(apply_poly(s, pp, nk, vec, hs, tmp));
+    launch_lanczos_step(wvec, vec, tmp, s->ncv, nk, k, a, b, niter, s->d_sqrtR, hsn, pp.tamm_d,
+                        (k + 1 < niter) ? 1 : 0, clen, eps, s->stream);
     if (k + 1 < niter) {
       double *t = vec;
       vec = wvec;
@@ -641,11 +650,27 @@ int ngw_lanczos_spectra_isdf(ngw_session *s, const double *v0, const double *v0_
                              const double *zz, int nz, int niter, const double *polynomial,
                              int npoly, int blksz, int tamm_d, double *spectra, double *alpha,
                              double *beta) {
+  return ngw_lanczos_spectra_isdf_masked(s, v0, v0_norm, ld, zz, nz, niter, polynomial, npoly, blksz,
+                                         tamm_d, nullptr, 0.0, spectra, alpha, beta);
+}
+
+int ngw_lanczos_spectra_isdf_masked(ngw_session *s, const double *v0, const double *v0_norm, int ld,
+                                    const double *zz, int nz, int niter, const double *polynomial,
+                                    int npoly, int blksz, int tamm_d, const int *chain_niter,
+                                    double early_exit_eps, double *spectra, double *alpha,
+                                    double *beta) {
   NGW_TRY(need_op(s));
-  if (!v0 || !v0_norm || !zz || !spectra || nz <= 0 || niter <= 0 || blksz <= 0 || ld < s->ncv) {
+  if (!v0 || !v0_norm || !zz || !spectra || nz <= 0 || niter <= 0 || blksz <= 0 || ld < s->ncv ||
+      !(early_exit_eps >= 0.0)) {
     set_error("ngw_lanczos_spectra_isdf: bad arguments");
     return NGW_ERR_ARG;
   }
+  if (chain_niter)
+    for (int j = 0; j < blksz; ++j)
+      if (chain_niter[j] < 1 || chain_niter[j] > niter) {
+        set_error("chain_niter[%d] = %d out of 1..niter", j, chain_niter[j]);
+        return NGW_ERR_ARG;
+      }
   NGW_CUDA(cudaSetDevice(s->device));
   const int ncv = s->ncv, nb = blksz;
   PolyPlan pp;
@@ -661,6 +686,12 @@ int ngw_lanczos_spectra_isdf(ngw_session *s, const double *v0, const double *v0_
   NGW_TRY(scratch(s, SL_ZZ, (size_t)nz * nb * 16, (void **)&dzz));
   NGW_TRY(scratch(s, SL_SPEC, (size_t)nz * nb * 16, (void **)&dspec));
   NGW_TRY(scratch(s, SL_PN, (size_t)nb * 8, (void **)&dnorm));
+  int *clen = nullptr, *dlen = nullptr;
+  NGW_TRY(scratch(s, SL_CLEN, (size_t)nb * 4, (void **)&clen));
+  if (chain_niter) {
+    NGW_TRY(scratch(s, SL_LEN, (size_t)nb * 4, (void **)&dlen));
+    NGW_CUDA(cudaMemcpyAsync(dlen, chain_niter, (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
+  }
   if (s->precision == NGW_PREC_MIXED) NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
   NGW_CUDA(cudaMemcpy2DAsync(dv0, (size_t)ncv * 8, v0, (size_t)ld * 8, (size_t)ncv * 8, nb,
                              cudaMemcpyHostToDevice, s->stream));
@@ -668,9 +699,10 @@ int ngw_lanczos_spectra_isdf(ngw_session *s, const double *v0, const double *v0_
   NGW_CUDA(cudaMemcpyAsync(dzz, zz, (size_t)nz * nb * 16, cudaMemcpyHostToDevice, s->stream));
   NGW_CUDA(cudaMemsetAsync(b, 0, (size_t)niter * nb * 8, s->stream));
   NGW_CUDA(cudaMemsetAsync(a, 0, (size_t)niter * nb * 8, s->stream));
-  launch_lanczos_init(dv0, ncv, dnorm, V, hs, s->d_sqrtR, ncv, nb, tamm_d, b, niter, s->stream);
-  NGW_TRY(lanczos_dev(s, pp, nb, niter, V, W, hs, tmp, a, b));
-  launch_contfrac(a, b, niter, nb, dzz, nz, dspec, s->stream);
+  launch_lanczos_init(dv0, ncv, dnorm, V, hs, s->d_sqrtR, ncv, nb, tamm_d, b, niter, dlen, clen,
+                      s->stream);
+  NGW_TRY(lanczos_dev(s, pp, nb, niter, V, W, hs, tmp, a, b, clen, early_exit_eps, nullptr));
+  launch_contfrac(a, b, niter, nb, dzz, nz, dspec, clen, s->stream);
   NGW_CUDA(cudaGetLastError());
   NGW_CUDA(cudaMemcpyAsync(spectra, dspec, (size_t)nz * nb * 16, cudaMemcpyDeviceToHost, s->stream));
   if (alpha)
@@ -753,6 +785,16 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
       set_error("qp band %d out of range", p->qp_bands[i]);
       return NGW_ERR_ARG;
     }
+  if (p->chain_niter)
+    for (int i = 0; i < p->nqp * nbsum; ++i)
+      if (p->chain_niter[i] < 1 || p->chain_niter[i] > p->niter) {
+        set_error("chain_niter[%d] = %d out of 1..niter", i, p->chain_niter[i]);
+        return NGW_ERR_ARG;
+      }
+  if (!(p->early_exit_eps >= 0.0)) {
+    set_error("early_exit_eps must be >= 0");
+    return NGW_ERR_ARG;
+  }
   if (!all_finite(e1, s->nmem)) {
     set_error("non-finite energies");
     return NGW_ERR_NONFINITE;
@@ -791,6 +833,10 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
   NGW_TRY(scratch(s, SL_CHB, (size_t)2 * nb_max * 4, (void **)&chb));
   NGW_TRY(scratch(s, SL_CHQ, (size_t)2 * nb_max * 4, (void **)&chq));
   NGW_TRY(scratch(s, SL_VEC, (size_t)ncv * nb_max * 8, (void **)&V));
+  int *clen, *dlen, *dslot;
+  NGW_TRY(scratch(s, SL_CLEN, (size_t)nb_max * 4, (void **)&clen));
+  NGW_TRY(scratch(s, SL_LEN, (size_t)nb_max * 4, (void **)&dlen));
+  NGW_TRY(scratch(s, SL_SLOT, (size_t)nb_max * 4, (void **)&dslot));
   if (s->precision == NGW_PREC_MIXED) NGW_TRY(mixed_prepare_chains(s, nb_max, 0, 0, 0));
   NGW_CUDA(cudaMemcpyAsync(de1, e1, (size_t)s->nmem * 8, cudaMemcpyHostToDevice, s->stream));
   // energy grid origin per QP state: en0 = e1(m) - deltae/2, step deltae/(nen-1)
@@ -799,21 +845,39 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
   const double de = p->deltae / (double)(nen - 1);
   NGW_CUDA(cudaMemcpyAsync(zz0, hz0.data(), (size_t)p->nqp * 8, cudaMemcpyHostToDevice, s->stream));
   const double one = 1.0, zero = 0.0;
-  std::vector<int> hb(2 * nb_max), hq(2 * nb_max);
+  std::vector<int> hb(2 * nb_max), hq(2 * nb_max), hl(nb_max), hslot(nb_max), order(nb_max);
+  std::vector<int> nact;
   for (int q0 = 0; q0 < p->nqp; q0 += nq_blk) {
     const int nq = std::min(nq_blk, p->nqp - q0);
     const int nb = nq * nbsum;
-    // chain (iq, n): band1 = m (QP band), band2 = n; chain_qp = block-local QP index
-    for (int iq = 0; iq < nq; ++iq)
-      for (int jn = 0; jn < nbsum; ++jn) {
-        const int j = iq * nbsum + jn;
-        hb[j] = p->qp_bands[q0 + iq];
-        hb[nb + j] = jn + 1;
-        hq[j] = q0 + iq;
+    // chain o = (iq, n) of the block, o = iq*nbsum + n-1: band1 = m (QP band),
+    // band2 = n.  With per-chain lengths the chains run longest first (stable
+    // order): position j holds chain order[j], slot[o] is o's position.
+    for (int o = 0; o < nb; ++o) order[o] = o;
+    const int *len = p->chain_niter ? p->chain_niter + (size_t)q0 * nbsum : nullptr;
+    if (len)
+      std::stable_sort(order.begin(), order.begin() + nb, [&](int x, int y) { return len[x] > len[y]; });
+    for (int j = 0; j < nb; ++j) {
+      const int o = order[j], iq = o / nbsum, jn = o % nbsum;
+      hb[j] = p->qp_bands[q0 + iq];
+      hb[nb + j] = jn + 1;
+      hq[j] = q0 + iq;
+      hl[j] = len ? len[o] : niter;
+      hslot[o] = j;
+    }
+    nact.assign(niter, nb);
+    if (len)
+      for (int k = 0; k < niter; ++k) {
+        int c = 0;
+        while (c < nb && hl[c] > k) ++c;
+        nact[k] = c;
       }
     NGW_CUDA(cudaMemcpyAsync(chb, hb.data(), (size_t)2 * nb * 4, cudaMemcpyHostToDevice, s->stream));
     NGW_CUDA(cudaMemcpyAsync(chq, hq.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
+    NGW_CUDA(cudaMemcpyAsync(dlen, hl.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
+    NGW_CUDA(cudaMemcpyAsync(dslot, hslot.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
     NGW_CUDA(cudaStreamSynchronize(s->stream));
+    const double eps = p->early_exit_eps;
     auto region = [&]() -> int {
       // start vectors  P = sqrtR * C^T M (psi_m psi_n)   (F90z:578-709), FP64
       launch_pair_gather_cols(s->d_psi, n, chb, chb + nb, nb, cmn, s->stream);
@@ -826,12 +890,13 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
       NGW_CUDA(cudaMemsetAsync(b, 0, (size_t)niter * nb * 8, s->stream));
       // pnorm = sqrt(pnorm2), v0 = P / pnorm   (F90z:707-709, lanczos_spectra_lowcomsym.F90:68-70)
       launch_sqrt_vec(pn2, pn, nb, s->stream);
-      launch_lanczos_init(P2, ncv, pn, V, hs, s->d_sqrtR, ncv, nb, tamm_d, b, niter, s->stream);
-      NGW_TRY(lanczos_dev(s, pp, nb, niter, V, W, hs, tmp, a, b));
+      launch_lanczos_init(P2, ncv, pn, V, hs, s->d_sqrtR, ncv, nb, tamm_d, b, niter, dlen, clen,
+                          s->stream);
+      NGW_TRY(lanczos_dev(s, pp, nb, niter, V, W, hs, tmp, a, b, clen, eps, len ? &nact : nullptr));
       launch_sigma_spectra(a, b, niter, nb, de1, chb + nb, chq, zz0, de, nen, p->ecuts, p->nval, S,
-                           s->stream);
+                           clen, s->stream);
       launch_sigma_reduce(S, pn2, de1, chb + nb, zz0 + q0, de, nen, p->ecuts, p->nval, nbsum, nq,
-                          tamm_d, sig + (size_t)2 * q0 * nen, 0, s->stream);
+                          tamm_d, sig + (size_t)2 * q0 * nen, 0, dslot, s->stream);
       NGW_CUDA(cudaGetLastError());
       return NGW_OK;
     };
@@ -840,14 +905,16 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
         (unsigned long long)pp.npoly, (unsigned long long)tamm_d, (unsigned long long)nen,
         (unsigned long long)p->nval, (unsigned long long)nbsum, (unsigned long long)nq,
         (unsigned long long)q0, (unsigned long long)pp.kdef, dbits(p->ecuts), dbits(de),
-        dbits(pp.c0), dbits(pp.c1), s->gen};
+        dbits(pp.c0), dbits(pp.c1), s->gen, dbits(eps), (unsigned long long)(len != nullptr)};
+    if (len) key.insert(key.end(), nact.begin(), nact.end());
     for (double c : pp.poly) key.push_back(dbits(c));
     for (double c : pp.cheb) key.push_back(dbits(c));
     for (const void *ptr : {(const void *)cmn, (const void *)cm, (const void *)P, (const void *)P2,
                             (const void *)pn2, (const void *)pn, (const void *)V, (const void *)W,
                             (const void *)hs, (const void *)tmp, (const void *)a, (const void *)b,
                             (const void *)S, (const void *)chb, (const void *)chq, (const void *)de1,
-                            (const void *)zz0, (const void *)sig, (const void *)s->mixed})
+                            (const void *)zz0, (const void *)sig, (const void *)s->mixed,
+                            (const void *)clen, (const void *)dlen, (const void *)dslot})
       key.push_back((unsigned long long)(uintptr_t)ptr);
     if (s->mixed) {
       int tune[4];
@@ -857,12 +924,18 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
     tm.mark("block_setup");
     NGW_TRY(run_graphed(s, key, region));
     tm.mark("region");
-    if (alpha)
-      NGW_CUDA(cudaMemcpyAsync(alpha + (size_t)q0 * nbsum * niter, a, (size_t)niter * nb * 8,
-                               cudaMemcpyDeviceToHost, s->stream));
-    if (beta)
-      NGW_CUDA(cudaMemcpyAsync(beta + (size_t)q0 * nbsum * niter, b, (size_t)niter * nb * 8,
-                               cudaMemcpyDeviceToHost, s->stream));
+    // alpha / beta back in chain order
+    for (int w = 0; w < 2; ++w) {
+      double *dst = w == 0 ? alpha : beta;
+      if (!dst) continue;
+      std::vector<double> h((size_t)niter * nb);
+      NGW_CUDA(cudaMemcpyAsync(h.data(), w == 0 ? a : b, (size_t)niter * nb * 8, cudaMemcpyDeviceToHost,
+                               s->stream));
+      NGW_CUDA(cudaStreamSynchronize(s->stream));
+      for (int o = 0; o < nb; ++o)
+        std::memcpy(dst + ((size_t)q0 * nbsum + o) * niter, h.data() + (size_t)hslot[o] * niter,
+                    (size_t)niter * 8);
+    }
   }
   NGW_CUDA(cudaMemcpyAsync(sigma_c, sig, (size_t)p->nqp * nen * 16, cudaMemcpyDeviceToHost,
                            s->stream));

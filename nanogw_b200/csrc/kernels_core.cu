@@ -168,11 +168,15 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
 constexpr int LNT = 256;
 
 // vec = v0 / v0_norm ; b(1) = 1 ; hs = sqrtR * vec (TDA: vec)
-// (lanczos_spectra_lowcomsym.F90:68-72)
+// (lanczos_spectra_lowcomsym.F90:68-72).  clen (optional) receives each
+// chain's length: len[j] (per-chain lengths) or niter, clamped to 1..niter.
+// The step kernels leave a chain alone from step clen[j] on, and lower clen[j]
+// when its recurrence breaks down (convergence mask, below).
 __global__ void k_lanczos_init(const double *__restrict__ v0, int ld,
                                const double *__restrict__ v0_norm, double *__restrict__ vec,
                                double *__restrict__ hs, const double *__restrict__ s, int ncv,
-                               int tamm_d, double *__restrict__ b_elmt, int niter) {
+                               int tamm_d, double *__restrict__ b_elmt, int niter,
+                               const int *__restrict__ len, int *__restrict__ clen) {
   const int j = blockIdx.x;
   const double nrm = v0_norm[j];
   for (int i = threadIdx.x; i < ncv; i += blockDim.x) {
@@ -180,14 +184,18 @@ __global__ void k_lanczos_init(const double *__restrict__ v0, int ld,
     vec[(size_t)j * ncv + i] = v;
     hs[(size_t)j * ncv + i] = tamm_d ? v : s[i] * v;
   }
-  if (threadIdx.x == 0) b_elmt[(size_t)j * niter] = 1.0;
+  if (threadIdx.x == 0) {
+    b_elmt[(size_t)j * niter] = 1.0;
+    if (clen) clen[j] = len ? min(max(len[j], 1), niter) : niter;
+  }
 }
 
 void launch_lanczos_init(const double *v0, int ld, const double *v0_norm, double *vec, double *hs,
                          const double *s, int ncv, int nb, int tamm_d, double *b_elmt, int niter,
-                         cudaStream_t st) {
+                         const int *len, int *clen, cudaStream_t st) {
   if (nb <= 0) return;
-  k_lanczos_init<<<nb, LNT, 0, st>>>(v0, ld, v0_norm, vec, hs, s, ncv, tamm_d, b_elmt, niter);
+  k_lanczos_init<<<nb, LNT, 0, st>>>(v0, ld, v0_norm, vec, hs, s, ncv, tamm_d, b_elmt, niter, len,
+                                     clen);
 }
 
 // Rescale for the next step and hand the next matvec its input:
@@ -204,10 +212,15 @@ __device__ __forceinline__ void prescale_chain(double *w, double *v, int ncv, do
 }
 
 // a(1) = <w, v> ; w = w - a(1) v ; b(2) = ||w||   (lanczos_spectra_lowcomsym.F90:104-116)
+// Convergence mask (eps > 0): the chain stops when |b(k)| < eps, as the
+// single-vector reference does (shared/lanczos_spectra.f90:24,58: its later
+// a/b stay unset; here they stay 0 and the continued fraction ends at clen).
 __global__ void k_lanczos_first(double *__restrict__ w, const double *__restrict__ v, int ncv,
-                                double *__restrict__ a, double *__restrict__ b, int niter) {
+                                double *__restrict__ a, double *__restrict__ b, int niter,
+                                int *__restrict__ clen, double eps) {
   __shared__ double sh[33];
   const int j = blockIdx.x;
+  const int L = clen ? clen[j] : niter;
   double *wj = w + (size_t)j * ncv;
   const double *vj = v + (size_t)j * ncv;
   double acc = 0.0;
@@ -222,31 +235,36 @@ __global__ void k_lanczos_first(double *__restrict__ w, const double *__restrict
   const double bb = block_sum<LNT>(acc, sh);
   if (threadIdx.x == 0) {
     a[(size_t)j * niter] = a1;
-    if (niter >= 2) b[(size_t)j * niter + 1] = sqrt(bb);
+    if (L >= 2) {
+      const double b2 = sqrt(bb);
+      b[(size_t)j * niter + 1] = b2;
+      if (clen && eps > 0.0 && b2 < eps) clen[j] = 1;
+    }
   }
 }
 
 void launch_lanczos_first(double *w, const double *v, int ncv, int nb, double *a, double *b,
-                          int niter, cudaStream_t st) {
+                          int niter, int *clen, double eps, cudaStream_t st) {
   if (nb <= 0) return;
-  k_lanczos_first<<<nb, LNT, 0, st>>>(w, v, ncv, a, b, niter);
+  k_lanczos_first<<<nb, LNT, 0, st>>>(w, v, ncv, a, b, niter, clen, eps);
 }
 
 __global__ void k_lanczos_prescale(double *__restrict__ w, double *__restrict__ v, int ncv, int k,
                                    const double *__restrict__ b, int niter,
                                    const double *__restrict__ s, double *__restrict__ hs,
-                                   int tamm_d) {
+                                   int tamm_d, const int *__restrict__ clen) {
   const int j = blockIdx.x;
+  if (clen && k >= clen[j]) return;     // finished or stopped chain
   const double bk = b[(size_t)j * niter + k];
   prescale_chain(w + (size_t)j * ncv, v + (size_t)j * ncv, ncv, bk, s,
                  hs ? hs + (size_t)j * ncv : nullptr, tamm_d);
 }
 
 void launch_lanczos_prescale(double *w, double *v, int ncv, int nb, int k, const double *b,
-                             int niter, const double *s, double *hs, int tamm_d,
+                             int niter, const double *s, double *hs, int tamm_d, const int *clen,
                              cudaStream_t st) {
   if (nb <= 0) return;
-  k_lanczos_prescale<<<nb, LNT, 0, st>>>(w, v, ncv, k, b, niter, s, hs, tamm_d);
+  k_lanczos_prescale<<<nb, LNT, 0, st>>>(w, v, ncv, k, b, niter, s, hs, tamm_d, clen);
 }
 
 // Step k (0-based, k >= 1):  w = w + t ; a(k) = <w, v> ;
@@ -256,9 +274,11 @@ __global__ void k_lanczos_step(double *__restrict__ w, double *__restrict__ v,
                                const double *__restrict__ t, int ncv, int k,
                                double *__restrict__ a, double *__restrict__ b, int niter,
                                const double *__restrict__ s, double *__restrict__ hs, int tamm_d,
-                               int prescale_next) {
+                               int prescale_next, int *__restrict__ clen, double eps) {
   __shared__ double sh[33];
   const int j = blockIdx.x;
+  const int L = clen ? clen[j] : niter;
+  if (k >= L) return;                    // finished or stopped chain: vectors left as they are
   double *wj = w + (size_t)j * ncv;
   double *vj = v + (size_t)j * ncv;
   const double *tj = t + (size_t)j * ncv;
@@ -270,7 +290,7 @@ __global__ void k_lanczos_step(double *__restrict__ w, double *__restrict__ v,
   }
   const double ak = block_sum<LNT>(acc, sh);
   if (threadIdx.x == 0) a[(size_t)j * niter + k] = ak;
-  if (k + 1 < niter) {
+  if (k + 1 < L) {
     acc = 0.0;
     for (int i = threadIdx.x; i < ncv; i += blockDim.x) {
       double wi = wj[i] - ak * vj[i];
@@ -278,16 +298,22 @@ __global__ void k_lanczos_step(double *__restrict__ w, double *__restrict__ v,
       acc += wi * wi;
     }
     const double bk1 = sqrt(block_sum<LNT>(acc, sh));
-    if (threadIdx.x == 0) b[(size_t)j * niter + k + 1] = bk1;
-    if (prescale_next) prescale_chain(wj, vj, ncv, bk1, s, hs ? hs + (size_t)j * ncv : nullptr, tamm_d);
+    const bool stop = clen && eps > 0.0 && bk1 < eps;
+    if (threadIdx.x == 0) {
+      b[(size_t)j * niter + k + 1] = bk1;
+      if (stop) clen[j] = k + 1;
+    }
+    if (prescale_next && !stop)
+      prescale_chain(wj, vj, ncv, bk1, s, hs ? hs + (size_t)j * ncv : nullptr, tamm_d);
   }
 }
 
 void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb, int k, double *a,
                          double *b, int niter, const double *s, double *hs, int tamm_d,
-                         int prescale_next, cudaStream_t st) {
+                         int prescale_next, int *clen, double eps, cudaStream_t st) {
   if (nb <= 0) return;
-  k_lanczos_step<<<nb, LNT, 0, st>>>(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next);
+  k_lanczos_step<<<nb, LNT, 0, st>>>(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next, clen,
+                                     eps);
 }
 
 // ---------------------------------------------------------------------------
@@ -323,22 +349,22 @@ __device__ __forceinline__ cplx contfrac_eval(const double *a, const double *b, 
 
 __global__ void k_contfrac(const double *__restrict__ a, const double *__restrict__ b, int niter,
                            int nb, const double *__restrict__ zz, int nz,
-                           double *__restrict__ spectra) {
+                           double *__restrict__ spectra, const int *__restrict__ clen) {
   const int iz = blockIdx.x * blockDim.x + threadIdx.x;
   if (iz >= nz) return;
   for (int j = blockIdx.y; j < nb; j += gridDim.y) {
     const size_t o = (size_t)j * nz + iz;
     cplx z = {zz[2 * o], zz[2 * o + 1]};
-    cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, niter, z);
+    cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, clen ? clen[j] : niter, z);
     spectra[2 * o] = r.re;
     spectra[2 * o + 1] = r.im;
   }
 }
 
 void launch_contfrac(const double *a, const double *b, int niter, int nb, const double *zz, int nz,
-                     double *spectra, cudaStream_t st) {
+                     double *spectra, const int *clen, cudaStream_t st) {
   if (nb <= 0 || nz <= 0) return;
-  k_contfrac<<<dim3(cdiv(nz, 128), ygrid(nb)), 128, 0, st>>>(a, b, niter, nb, zz, nz, spectra);
+  k_contfrac<<<dim3(cdiv(nz, 128), ygrid(nb)), 128, 0, st>>>(a, b, niter, nb, zz, nz, spectra, clen);
 }
 
 // Per-chain spectra on the Sigma energy grid:
@@ -349,7 +375,7 @@ __global__ void k_sigma_spectra(const double *__restrict__ a, const double *__re
                                 const int *__restrict__ chain_band,
                                 const int *__restrict__ chain_qp, const double *__restrict__ zz0,
                                 double de, int nen, double ecuts, int nval,
-                                double *__restrict__ S) {
+                                double *__restrict__ S, const int *__restrict__ clen) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i > nen) return;
   for (int j = blockIdx.y; j < nchain; j += gridDim.y) {
@@ -364,7 +390,7 @@ __global__ void k_sigma_spectra(const double *__restrict__ a, const double *__re
       z.re = (-zz + e1[n - 1]) * eta;
       z.im = ecuts;
     }
-    cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, niter, z);
+    cplx r = contfrac_eval(a + (size_t)j * niter, b + (size_t)j * niter, clen ? clen[j] : niter, z);
     const size_t o = (size_t)j * (nen + 1) + i;
     S[2 * o] = r.re;
     S[2 * o + 1] = r.im;
@@ -374,22 +400,23 @@ __global__ void k_sigma_spectra(const double *__restrict__ a, const double *__re
 void launch_sigma_spectra(const double *a, const double *b, int niter, int nchain,
                           const double *e1, const int *chain_band, const int *chain_qp,
                           const double *zz0, double de, int nen, double ecuts, int nval,
-                          double *S, cudaStream_t st) {
+                          double *S, const int *clen, cudaStream_t st) {
   if (nchain <= 0) return;
   k_sigma_spectra<<<dim3(cdiv(nen + 1, 128), ygrid(nchain)), 128, 0, st>>>(
-      a, b, niter, nchain, e1, chain_band, chain_qp, zz0, de, nen, ecuts, nval, S);
+      a, b, niter, nchain, e1, chain_band, chain_qp, zz0, de, nen, ecuts, nval, S, clen);
 }
 
 // Sigma_c(i, iq) (+)= sum_n in band order of
 //   non-TDA: (S_n(0) - S_n(ezz)) * eta_n * 2 * pnorm2_n / ezz
 //   TDA:     -S_n(ezz) * eta_n * sqrt(2) * pnorm2_n   (sqrt(2) in single precision, as 2.0**0.5)
-// (calculate_sigma_lanczos_lowcomsym.F90:736-745).  Chains of QP iq are
-// iq*nbsum .. iq*nbsum + nbsum-1 of this block.
+// (calculate_sigma_lanczos_lowcomsym.F90:736-745).  The chain of (QP iq,
+// band nn) is slot[iq*nbsum + nn] of this block (iq*nbsum + nn without slot).
 __global__ void k_sigma_reduce(const double *__restrict__ S, const double *__restrict__ pnorm2,
                                const double *__restrict__ e1, const int *__restrict__ chain_band,
                                const double *__restrict__ zz0, double de, int nen, double ecuts,
                                int nval, int nbsum, int nqp, int tamm_d,
-                               double *__restrict__ sigma, int accumulate) {
+                               double *__restrict__ sigma, int accumulate,
+                               const int *__restrict__ slot) {
   const int iq = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= nqp || i >= nen) return;
@@ -401,7 +428,7 @@ __global__ void k_sigma_reduce(const double *__restrict__ S, const double *__res
     acc.im = sigma[2 * ((size_t)iq * nen + i) + 1];
   }
   for (int nn = 0; nn < nbsum; ++nn) {
-    const int j = iq * nbsum + nn;
+    const int j = slot ? slot[iq * nbsum + nn] : iq * nbsum + nn;
     const int n = chain_band[j];
     const double eta = (n <= nval) ? 1.0 : -1.0;
     const size_t o = (size_t)j * (nen + 1);
@@ -426,11 +453,11 @@ __global__ void k_sigma_reduce(const double *__restrict__ S, const double *__res
 void launch_sigma_reduce(const double *S, const double *pnorm2, const double *e1,
                          const int *chain_band, const double *zz0, double de, int nen,
                          double ecuts, int nval, int nbsum, int nqp, int tamm_d, double *sigma,
-                         int accumulate, cudaStream_t st) {
+                         int accumulate, const int *slot, cudaStream_t st) {
   if (nqp <= 0) return;
   k_sigma_reduce<<<dim3(cdiv(nen, 128), nqp), 128, 0, st>>>(S, pnorm2, e1, chain_band, zz0, de,
                                                             nen, ecuts, nval, nbsum, nqp, tamm_d,
-                                                            sigma, accumulate);
+                                                            sigma, accumulate, slot);
 }
 
 // P = P * sqrtR (non-TDA) ; pnorm2 = <P, P>   (calculate_sigma_lanczos_lowcomsym.F90:696-705)

@@ -128,25 +128,25 @@ void launch_copy_cols(const double *x, int ldx, double *y, int ldy, int n, int n
                       cudaStream_t st);
 void launch_lanczos_init(const double *v0, int ld, const double *v0_norm, double *vec,
                          double *hs, const double *s, int ncv, int nb, int tamm_d,
-                         double *b_elmt, int niter, cudaStream_t st);
+                         double *b_elmt, int niter, const int *len, int *clen, cudaStream_t st);
 void launch_lanczos_first(double *w, const double *v, int ncv, int nb, double *a, double *b,
-                          int niter, cudaStream_t st);
+                          int niter, int *clen, double eps, cudaStream_t st);
 void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb, int k,
                          double *a, double *b, int niter, const double *s, double *hs,
-                         int tamm_d, int prescale_next, cudaStream_t st);
+                         int tamm_d, int prescale_next, int *clen, double eps, cudaStream_t st);
 void launch_lanczos_prescale(double *w, double *v, int ncv, int nb, int k, const double *b,
-                             int niter, const double *s, double *hs, int tamm_d,
+                             int niter, const double *s, double *hs, int tamm_d, const int *clen,
                              cudaStream_t st);
 void launch_contfrac(const double *a, const double *b, int niter, int nb, const double *zz,
-                     int nz, double *spectra, cudaStream_t st);
+                     int nz, double *spectra, const int *clen, cudaStream_t st);
 void launch_sigma_spectra(const double *a, const double *b, int niter, int nchain,
                           const double *e1, const int *chain_band, const int *chain_qp,
                           const double *zz0, double de, int nen, double ecuts, int nval,
-                          double *S, cudaStream_t st);
+                          double *S, const int *clen, cudaStream_t st);
 void launch_sigma_reduce(const double *S, const double *pnorm2, const double *e1,
                          const int *chain_band, const double *zz0, double de, int nen,
                          double ecuts, int nval, int nbsum, int nqp, int tamm_d,
-                         double *sigma, int accumulate, cudaStream_t st);
+                         double *sigma, int accumulate, const int *slot, cudaStream_t st);
 void launch_norms(const double *P, int ncv, int nb, const double *s, int tamm_d, double *P_out,
                   double *pnorm2, cudaStream_t st);
 void launch_qp_newton_ws(int nqp, int nen, const double *sig, const double *e1, const double *e0,

@@ -57,21 +57,26 @@ def polynomial_matvec_isdf(vec, polynomial, cmtrx, mmtrx, sqrtR, matvec=None):
     return hvec
 
 
-def lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=None):
+def lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=None, lengths=None,
+                       return_lengths=False):
     """Lanczos alpha/beta for a block of independent chains.
 
     Follows ``shared/lanczos_spectra_lowcomsym.F90:67-166`` exactly (no
-    reorthogonalisation; ``b(1) = 1``; the ``k+1 <= niter`` guard).  With
-    ``early_exit_eps`` the chain stops when ``|b_k| < eps`` as in
-    ``shared/lanczos_spectra.f90:57-58`` (single chain only); the unset
-    tail is returned as zeros (the reference leaves it uninitialised).
-    Returns (a, b) with shape (niter, blksz).
+    reorthogonalisation; ``b(1) = 1``; the ``k+1 <= niter`` guard).
+    ``lengths`` (optional, per chain) runs chain j for lengths[j] steps: the
+    same loop with niter = lengths[j].  With ``early_exit_eps`` a chain stops
+    at the top of step k when ``|b_k| < eps``, as the single-vector routine
+    does (``shared/lanczos_spectra.f90:57-58``); the tail the reference leaves
+    uninitialised is zero here and the chain's effective length is k.
+    Returns (a, b) with shape (niter, blksz) [, effective lengths].
     """
     v0 = np.asarray(v0, dtype=np.float64)
     if v0.ndim == 1:
         v0 = v0[:, None]
     blksz = v0.shape[1]
     v0_norm = np.broadcast_to(np.asarray(v0_norm, dtype=np.float64), (blksz,))
+    L = np.full(blksz, niter) if lengths is None else np.clip(np.asarray(lengths), 1, niter)
+    leff = L.copy()
     a = np.zeros((niter, blksz))
     b = np.zeros((niter, blksz))
     vec = v0 / v0_norm[None, :]
@@ -80,27 +85,38 @@ def lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=None):
     a[0] = np.einsum("ij,ij->j", wvec, vec)
     wvec = wvec - a[0][None, :] * vec
     if niter >= 2:
-        b[1] = np.sqrt(np.einsum("ij,ij->j", wvec, wvec))
+        b[1] = np.where(L >= 2, np.sqrt(np.einsum("ij,ij->j", wvec, wvec)), 0.0)
     for k in range(1, niter):
-        if early_exit_eps is not None and np.all(np.abs(b[k]) < early_exit_eps):
+        act = k < leff
+        if early_exit_eps is not None:
+            stop = act & (np.abs(b[k]) < early_exit_eps)
+            leff[stop] = k
+            act &= ~stop
+        sel = np.nonzero(act)[0]
+        if len(sel) == 0:
             break
-        wvec = wvec / b[k][None, :]
-        vec = -vec * b[k][None, :]
-        vec, wvec = wvec, vec
-        tmp = apply_h(vec)
-        wvec = wvec + tmp
-        a[k] = np.einsum("ij,ij->j", wvec, vec)
-        if k + 1 < niter:
-            wvec = wvec - a[k][None, :] * vec
-            b[k + 1] = np.sqrt(np.einsum("ij,ij->j", wvec, wvec))
+        w = wvec[:, sel] / b[k, sel][None, :]
+        v = -vec[:, sel] * b[k, sel][None, :]
+        v, w = w, v
+        w = w + apply_h(v)
+        a[k, sel] = np.einsum("ij,ij->j", w, v)
+        more = k + 1 < L[sel]
+        if more.any():
+            w[:, more] = w[:, more] - a[k, sel][more][None, :] * v[:, more]
+            b[k + 1, sel[more]] = np.sqrt(np.einsum("ij,ij->j", w[:, more], w[:, more]))
+        vec[:, sel] = v
+        wvec[:, sel] = w
+    if return_lengths:
+        return a, b, leff
     return a, b
 
 
-def continued_fraction(a, b, zz):
+def continued_fraction(a, b, zz, lengths=None):
     """S(z) = <v|(z-H)^-1|v> from the Lanczos coefficients.
 
     Follows ``shared/lanczos_spectra_lowcomsym.F90:175-188``:
     S = 0; for j = niter..1: S = (j==1 ? 1 : b_j^2) / (z - a_j - S).
+    ``lengths`` (optional): chain j uses its first lengths[j] coefficients.
     a, b: (niter, blksz); zz: (nz, blksz) complex.  Returns (nz, blksz).
     """
     a = np.asarray(a)
@@ -115,7 +131,8 @@ def continued_fraction(a, b, zz):
     s = np.zeros(np.broadcast_shapes(zz.shape, (1, a.shape[1])), dtype=np.complex128)
     for j in range(niter - 1, -1, -1):
         num = 1.0 if j == 0 else b[j] * b[j]
-        s = num / (zz - a[j][None, :] - s)
+        nxt = num / (zz - a[j][None, :] - s)
+        s = nxt if lengths is None else np.where((j < np.asarray(lengths))[None, :], nxt, s)
     return s
 
 
@@ -133,10 +150,12 @@ def perturbed(apply_h, rel, seed=1):
 
 
 def lanczos_spectra_isdf(v0, v0_norm, zz, niter, polynomial, cmtrx, mmtrx, sqrtR,
-                         tamm_d=False, perturb=0.0):
+                         tamm_d=False, perturb=0.0, lengths=None, early_exit_eps=None,
+                         return_lengths=False):
     """``lanczos_spectra_isdf_lowcomsym`` (``shared/lanczos_spectra_lowcomsym.F90:7-190``):
-    the spectra <P|1/(zz-p(H))|P> for a block of start vectors.
-    Returns (spectra (nz, blksz), a, b)."""
+    the spectra <P|1/(zz-p(H))|P> for a block of start vectors; per-chain
+    lengths and the single-vector form's exit (``shared/lanczos_spectra.f90:57-58``)
+    as in ``lanczos_recurrence``.  Returns (spectra (nz, blksz), a, b[, lengths])."""
     mv = lambda x: matvec_isdf(x, cmtrx, mmtrx, sqrtR, tamm_d=tamm_d)   # noqa: E731
     if perturb:
         mv = perturbed(mv, perturb)
@@ -145,8 +164,12 @@ def lanczos_spectra_isdf(v0, v0_norm, zz, niter, polynomial, cmtrx, mmtrx, sqrtR
     else:
         def apply_h(x):
             return polynomial_matvec_isdf(x, polynomial, cmtrx, mmtrx, sqrtR, matvec=mv)
-    a, b = lanczos_recurrence(apply_h, v0, v0_norm, niter)
-    return continued_fraction(a, b, zz), a, b
+    a, b, leff = lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=early_exit_eps,
+                                    lengths=lengths, return_lengths=True)
+    spec = continued_fraction(a, b, zz, lengths=leff)
+    if return_lengths:
+        return spec, a, b, leff
+    return spec, a, b
 
 
 def dense_lanczos_spectra(H, v0, zz, niter):
