@@ -131,7 +131,8 @@ def continued_fraction(a, b, zz, lengths=None):
     s = np.zeros(np.broadcast_shapes(zz.shape, (1, a.shape[1])), dtype=np.complex128)
     for j in range(niter - 1, -1, -1):
         num = 1.0 if j == 0 else b[j] * b[j]
-        nxt = num / (zz - a[j][None, :] - s)
+        with np.errstate(divide="ignore", invalid="ignore"):   # masked-out tails may divide 0/0
+            nxt = num / (zz - a[j][None, :] - s)
         s = nxt if lengths is None else np.where((j < np.asarray(lengths))[None, :], nxt, s)
     return s
 
