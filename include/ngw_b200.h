@@ -141,6 +141,19 @@ int ngw_lanczos_spectra_isdf_masked(ngw_session *s, const double *v0, const doub
 int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e1,
                       double *sigma_c, double *alpha, double *beta);
 
+/* Batched Sigma_c of several molecules, one per session (sessions on one
+ * device, each with its operator set): entry i solves params[i] with KS
+ * energies e1[i] into sigma_c[i], exactly as ngw_sigma_lanczos would (same
+ * kernels and tiles, so the results are bit-identical).  The device work of
+ * all entries is one CUDA graph -- entry i a branch on session i's stream,
+ * forked from and joined into session 0's stream -- captured on the second
+ * call with the same shapes and replayed by one launch afterwards, so the
+ * chains of small molecules overlap on the GPU.  Each entry's chains must fit
+ * one block (block_chains 0 or >= nqp * nbands_sum).  Configuration 2 of the
+ * benchmarks (uneven molecules, per-chain lengths) runs through this call. */
+int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_sigma_params *params,
+                            const double *const *e1, double *const *sigma_c);
+
 /* QP Newton solve on the device (eV in, eV out), one state per column:
  * sigma_c (nen x nqp complex, eV), e1/e0/sigx/vxc (nqp) eV.
  * Grid: x_i = e1 - deltae/2 + deltae/(nen-1)*(i-1).  Tolerance xacc (eV). */

@@ -5,6 +5,6 @@ k_integrate_isdf, calculate_sigma_lanczos) through the C ABI in
 ``include/ngw_b200.h``; the Python classes here are a thin mirror of it.
 """
 from ._lib import NGWError, NGW_PREC_FP64, NGW_PREC_MIXED  # noqa: F401
-from .api import RYD, Session, lowcomsym_pairs, sqrt_r  # noqa: F401
+from .api import RYD, Session, lowcomsym_pairs, sigma_lanczos_batch, sqrt_r  # noqa: F401
 
-__all__ = ["Session", "NGWError", "RYD", "lowcomsym_pairs", "sqrt_r"]
+__all__ = ["Session", "NGWError", "RYD", "lowcomsym_pairs", "sigma_lanczos_batch", "sqrt_r"]

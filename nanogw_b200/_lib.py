@@ -43,6 +43,7 @@ SIGNATURES = {
                                              _P]),
     "ngw_k_integrate_isdf": (_I, [_P, _I, _P, _I, _P, _I, _P]),
     "ngw_sigma_lanczos": (_I, [_P, _P, _P, _P, _P, _P]),
+    "ngw_sigma_lanczos_batch": (_I, [_P, _I, _P, _P, _P]),
     "ngw_qp_newton": (_I, [_P, _I, _I, _P, _P, _P, _D, _P, _P, _D, _P, _P, _P]),
     "ngw_qp_newton_noalloc": (_I, [_I, _I, _P, _P, _P, _D, _P, _P, _D, _P, _P, _P, _P]),
     "ngw_profile_mixed_gemms": (_I, [_P, _I, _I, _P, _P]),

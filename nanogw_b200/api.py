@@ -153,12 +153,10 @@ class Session:
         check(lib().ngw_k_integrate_isdf(self._h, int(kflag), _p(r), len(r), _p(c), len(c), _p(out)))
         return out
 
-    def calculate_sigma_lanczos(self, e1, nval, qp_bands, nen, deltae, ecuts, niter, polynomial,
-                                tamm_d=False, nbands_sum=0, block_chains=0, cheb=(0.0, 0.0),
-                                return_ab=False, chain_niter=None, early_exit_eps=0.0):
-        """Sigma_c(omega) (Ry) for each QP band: complex array (nen, nqp).
-        chain_niter: optional (nqp, nbands_sum) per-chain Lanczos lengths
-        (1..niter); early_exit_eps > 0 stops a chain when |b_k| < eps."""
+    def _sigma_params(self, e1, nval, qp_bands, nen, deltae, ecuts, niter, polynomial, tamm_d=False,
+                      nbands_sum=0, block_chains=0, cheb=(0.0, 0.0), chain_niter=None,
+                      early_exit_eps=0.0):
+        """ngw_sigma_params for one request, with the arrays it points to."""
         e = np.ascontiguousarray(e1, dtype=np.float64)
         qp = np.ascontiguousarray(qp_bands, dtype=np.int32)
         poly = np.ascontiguousarray(polynomial if polynomial is not None else [1.0, 0.0],
@@ -177,10 +175,21 @@ class Session:
                 raise ValueError("chain_niter must have nqp * nbands_sum entries")
             prm.chain_niter = _p(ln)
         sig = np.zeros((nen, len(qp)), dtype=np.complex128, order="F")
+        return prm, e, sig, (qp, poly, ln), nbs
+
+    def calculate_sigma_lanczos(self, e1, nval, qp_bands, nen, deltae, ecuts, niter, polynomial,
+                                tamm_d=False, nbands_sum=0, block_chains=0, cheb=(0.0, 0.0),
+                                return_ab=False, chain_niter=None, early_exit_eps=0.0):
+        """Sigma_c(omega) (Ry) for each QP band: complex array (nen, nqp).
+        chain_niter: optional (nqp, nbands_sum) per-chain Lanczos lengths
+        (1..niter); early_exit_eps > 0 stops a chain when |b_k| < eps."""
+        prm, e, sig, keep, nbs = self._sigma_params(e1, nval, qp_bands, nen, deltae, ecuts, niter,
+                                                    polynomial, tamm_d, nbands_sum, block_chains,
+                                                    cheb, chain_niter, early_exit_eps)
         a = b = None
         if return_ab:
-            a = np.zeros((niter, nbs * len(qp)), order="F")
-            b = np.zeros((niter, nbs * len(qp)), order="F")
+            a = np.zeros((niter, nbs * sig.shape[1]), order="F")
+            b = np.zeros((niter, nbs * sig.shape[1]), order="F")
         check(lib().ngw_sigma_lanczos(self._h, ctypes.byref(prm), _p(e), _p(sig), _p(a), _p(b)))
         if return_ab:
             return sig, a, b
@@ -244,3 +253,20 @@ class Session:
         check(lib().ngw_build_coulomb_kernel(self._h, ngrid, n_isdf, _p(zt), _p(g), int(nfft), float(h),
                                              float(trunc), _p(m)))
         return m
+
+
+def sigma_lanczos_batch(sessions, requests):
+    """Sigma_c of several molecules in one graph launch (``ngw_sigma_lanczos_batch``).
+    sessions: Session objects (one molecule each, same device); requests: one
+    dict of ``calculate_sigma_lanczos`` arguments per session (no return_ab).
+    Returns the list of Sigma_c arrays, each bit-identical to the single call."""
+    if len(sessions) != len(requests) or not sessions:
+        raise ValueError("one request per session")
+    built = [s._sigma_params(**r) for s, r in zip(sessions, requests)]
+    n = len(sessions)
+    params = (SigmaParams * n)(*[b[0] for b in built])
+    hs = (ctypes.c_void_p * n)(*[s._h for s in sessions])
+    e1s = (ctypes.c_void_p * n)(*[_p(b[1]) for b in built])
+    sigs = (ctypes.c_void_p * n)(*[_p(b[2]) for b in built])
+    check(lib().ngw_sigma_lanczos_batch(hs, n, params, e1s, sigs))
+    return [b[2] for b in built]

@@ -409,11 +409,239 @@ static unsigned long long dbits(double x) {
   return u;
 }
 
+// ---------------------------------------------------------------------------
+// Sigma_c driver (SIGMA/calculate_sigma_lanczos_lowcomsym.F90z:516-779), split
+// into the host preparation, one device region per chain block (run through
+// the graph cache) and the download, so that a batch of sessions can record
+// their regions as branches of one graph.
+struct SigmaJob {
+  ngw_session *s = nullptr;
+  const ngw_sigma_params *p = nullptr;
+  const double *e1 = nullptr;
+  int nbsum = 0, ncv = 0, n = 0, nen = 0, niter = 0, tamm_d = 0, nq_blk = 0, nb_max = 0;
+  PolyPlan pp;
+  double de = 0.0;
+  double *de1, *zz0, *sig, *cmn, *cm, *P, *P2, *pn2, *pn, *V, *W, *hs, *tmp, *a, *b, *S;
+  int *chb, *chq, *clen, *dlen, *dslot;
+  // current block
+  int q0 = 0, nq = 0, nb = 0;
+  const int *len = nullptr;
+  std::vector<int> hb, hq, hl, hslot, order, nact;
+};
+
+static int sigma_prepare(SigmaJob &J, ngw_session *s, const ngw_sigma_params *p, const double *e1) {
+  NGW_TRY(need_op(s));
+  if (!p || !e1 || p->nen < 2 || p->niter < 1 || p->nqp < 1 || !p->qp_bands || p->nval < 1 ||
+      p->nval >= s->nmem) {
+    set_error("ngw_sigma_lanczos: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  const int nbsum = p->nbands_sum > 0 ? p->nbands_sum : s->nmem;
+  if (nbsum > s->nmem) {
+    set_error("nbands_sum > nmem");
+    return NGW_ERR_ARG;
+  }
+  for (int i = 0; i < p->nqp; ++i)
+    if (p->qp_bands[i] < 1 || p->qp_bands[i] > s->nmem) {
+      set_error("qp band %d out of range", p->qp_bands[i]);
+      return NGW_ERR_ARG;
+    }
+  if (p->chain_niter)
+    for (int i = 0; i < p->nqp * nbsum; ++i)
+      if (p->chain_niter[i] < 1 || p->chain_niter[i] > p->niter) {
+        set_error("chain_niter[%d] = %d out of 1..niter", i, p->chain_niter[i]);
+        return NGW_ERR_ARG;
+      }
+  if (!(p->early_exit_eps >= 0.0)) {
+    set_error("early_exit_eps must be >= 0");
+    return NGW_ERR_ARG;
+  }
+  if (!all_finite(e1, s->nmem)) {
+    set_error("non-finite energies");
+    return NGW_ERR_NONFINITE;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  J.s = s;
+  J.p = p;
+  J.e1 = e1;
+  J.nbsum = nbsum;
+  J.ncv = s->ncv;
+  J.n = s->n_isdf;
+  J.nen = p->nen;
+  J.niter = p->niter;
+  J.tamm_d = p->tamm_d ? 1 : 0;
+  // Chebyshev interval of the mixed form: from the operator's eigenpairs
+  // unless given (cheb_lo < cheb_hi)
+  NGW_TRY(make_plan(s, J.pp, p->polynomial, p->npoly, J.tamm_d, p->cheb_lo, p->cheb_hi));
+  // chain blocking: whole QP states per block
+  J.nq_blk = p->nqp;
+  if (p->block_chains > 0) J.nq_blk = std::max(1, std::min(p->nqp, p->block_chains / nbsum));
+  const int nb_max = J.nq_blk * nbsum, ncv = J.ncv, n = J.n, nen = J.nen, niter = J.niter;
+  J.nb_max = nb_max;
+  NGW_TRY(scratch(s, SL_E1, (size_t)s->nmem * 8, (void **)&J.de1));
+  NGW_TRY(scratch(s, SL_ZZ0, (size_t)p->nqp * 8, (void **)&J.zz0));
+  NGW_TRY(scratch(s, SL_SIG, (size_t)p->nqp * nen * 16, (void **)&J.sig));
+  NGW_TRY(scratch(s, SL_CMN, (size_t)n * nb_max * 8, (void **)&J.cmn));
+  NGW_TRY(scratch(s, SL_CM, (size_t)n * nb_max * 8, (void **)&J.cm));
+  NGW_TRY(scratch(s, SL_P, (size_t)ncv * nb_max * 8, (void **)&J.P));
+  NGW_TRY(scratch(s, SL_P2, (size_t)ncv * nb_max * 8, (void **)&J.P2));
+  NGW_TRY(scratch(s, SL_PN2, (size_t)nb_max * 8, (void **)&J.pn2));
+  NGW_TRY(scratch(s, SL_PN, (size_t)nb_max * 8, (void **)&J.pn));
+  NGW_TRY(scratch(s, SL_WVEC, (size_t)ncv * nb_max * 8, (void **)&J.W));
+  NGW_TRY(scratch(s, SL_HS, (size_t)ncv * nb_max * 8, (void **)&J.hs));
+  NGW_TRY(scratch(s, SL_TMP, (size_t)ncv * nb_max * 8, (void **)&J.tmp));
+  NGW_TRY(scratch(s, SL_A, (size_t)niter * nb_max * 8, (void **)&J.a));
+  NGW_TRY(scratch(s, SL_B, (size_t)niter * nb_max * 8, (void **)&J.b));
+  NGW_TRY(scratch(s, SL_SPECS, (size_t)(nen + 1) * nb_max * 16, (void **)&J.S));
+  NGW_TRY(scratch(s, SL_CHB, (size_t)2 * nb_max * 4, (void **)&J.chb));
+  NGW_TRY(scratch(s, SL_CHQ, (size_t)2 * nb_max * 4, (void **)&J.chq));
+  NGW_TRY(scratch(s, SL_VEC, (size_t)ncv * nb_max * 8, (void **)&J.V));
+  NGW_TRY(scratch(s, SL_CLEN, (size_t)nb_max * 4, (void **)&J.clen));
+  NGW_TRY(scratch(s, SL_LEN, (size_t)nb_max * 4, (void **)&J.dlen));
+  NGW_TRY(scratch(s, SL_SLOT, (size_t)nb_max * 4, (void **)&J.dslot));
+  if (s->precision == NGW_PREC_MIXED) NGW_TRY(mixed_prepare_chains(s, nb_max, 0, 0, 0));
+  NGW_CUDA(cudaMemcpyAsync(J.de1, e1, (size_t)s->nmem * 8, cudaMemcpyHostToDevice, s->stream));
+  // energy grid origin per QP state: en0 = e1(m) - deltae/2, step deltae/(nen-1)
+  std::vector<double> hz0(p->nqp);
+  for (int i = 0; i < p->nqp; ++i) hz0[i] = e1[p->qp_bands[i] - 1] - p->deltae * 0.5;
+  J.de = p->deltae / (double)(nen - 1);
+  NGW_CUDA(cudaMemcpyAsync(J.zz0, hz0.data(), (size_t)p->nqp * 8, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  J.hb.assign(2 * nb_max, 0);
+  J.hq.assign(2 * nb_max, 0);
+  J.hl.assign(nb_max, 0);
+  J.hslot.assign(nb_max, 0);
+  J.order.assign(nb_max, 0);
+  return NGW_OK;
+}
+
+// Chain tables of the block starting at QP state q0.  Chain o = (iq, n) of the
+// block, o = iq*nbsum + n-1: band1 = m (QP band), band2 = n.  With per-chain
+// lengths the chains run longest first (stable order): position j holds chain
+// order[j], slot[o] is o's position, nact[k] the chains still running at step k.
+static int sigma_block_setup(SigmaJob &J, int q0) {
+  ngw_session *s = J.s;
+  const ngw_sigma_params *p = J.p;
+  const int nbsum = J.nbsum, niter = J.niter;
+  J.q0 = q0;
+  J.nq = std::min(J.nq_blk, p->nqp - q0);
+  const int nb = J.nb = J.nq * nbsum;
+  for (int o = 0; o < nb; ++o) J.order[o] = o;
+  const int *len = J.len = p->chain_niter ? p->chain_niter + (size_t)q0 * nbsum : nullptr;
+  if (len)
+    std::stable_sort(J.order.begin(), J.order.begin() + nb, [&](int x, int y) { return len[x] > len[y]; });
+  for (int j = 0; j < nb; ++j) {
+    const int o = J.order[j], iq = o / nbsum, jn = o % nbsum;
+    J.hb[j] = p->qp_bands[q0 + iq];
+    J.hb[nb + j] = jn + 1;
+    J.hq[j] = q0 + iq;
+    J.hl[j] = len ? len[o] : niter;
+    J.hslot[o] = j;
+  }
+  J.nact.assign(niter, nb);
+  if (len)
+    for (int k = 0; k < niter; ++k) {
+      int c = 0;
+      while (c < nb && J.hl[c] > k) ++c;
+      J.nact[k] = c;
+    }
+  NGW_CUDA(cudaMemcpyAsync(J.chb, J.hb.data(), (size_t)2 * nb * 4, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(J.chq, J.hq.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(J.dlen, J.hl.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaMemcpyAsync(J.dslot, J.hslot.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return NGW_OK;
+}
+
+// The device work of one block, launch-only (graph-capturable).
+static int sigma_region(SigmaJob &J) {
+  ngw_session *s = J.s;
+  const ngw_sigma_params *p = J.p;
+  const int n = J.n, ncv = J.ncv, nb = J.nb, niter = J.niter, tamm_d = J.tamm_d;
+  const double one = 1.0, zero = 0.0;
+  // start vectors  P = sqrtR * C^T M (psi_m psi_n)   (F90z:578-709), FP64
+  launch_pair_gather_cols(s->d_psi, n, J.chb, J.chb + nb, nb, J.cmn, s->stream);
+  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, n, nb, n, &one, s->d_M, n, J.cmn, n, &zero,
+                         J.cm, n));
+  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, ncv, nb, n, &one, s->d_C, n, J.cm, n, &zero,
+                         J.P, ncv));
+  launch_norms(J.P, ncv, nb, s->d_sqrtR, tamm_d, J.P2, J.pn2, s->stream);
+  NGW_CUDA(cudaMemsetAsync(J.a, 0, (size_t)niter * nb * 8, s->stream));
+  NGW_CUDA(cudaMemsetAsync(J.b, 0, (size_t)niter * nb * 8, s->stream));
+  // pnorm = sqrt(pnorm2), v0 = P / pnorm   (F90z:707-709, lanczos_spectra_lowcomsym.F90:68-70)
+  launch_sqrt_vec(J.pn2, J.pn, nb, s->stream);
+  launch_lanczos_init(J.P2, ncv, J.pn, J.V, J.hs, s->d_sqrtR, ncv, nb, tamm_d, J.b, niter, J.dlen, J.clen,
+                      s->stream);
+  NGW_TRY(lanczos_dev(s, J.pp, nb, niter, J.V, J.W, J.hs, J.tmp, J.a, J.b, J.clen, p->early_exit_eps,
+                      J.len ? &J.nact : nullptr));
+  launch_sigma_spectra(J.a, J.b, niter, nb, J.de1, J.chb + nb, J.chq, J.zz0, J.de, J.nen, p->ecuts, p->nval,
+                       J.S, J.clen, s->stream);
+  launch_sigma_reduce(J.S, J.pn2, J.de1, J.chb + nb, J.zz0 + J.q0, J.de, J.nen, p->ecuts, p->nval, J.nbsum,
+                      J.nq, tamm_d, J.sig + (size_t)2 * J.q0 * J.nen, 0, J.dslot, s->stream);
+  NGW_CUDA(cudaGetLastError());
+  return NGW_OK;
+}
+
+// Graph key of the current block: every shape, scalar and device address the
+// region's launches capture.
+static void sigma_key(const SigmaJob &J, std::vector<unsigned long long> &key) {
+  ngw_session *s = J.s;
+  const ngw_sigma_params *p = J.p;
+  const unsigned long long head[] = {
+      (unsigned long long)s->precision, (unsigned long long)J.nb, (unsigned long long)J.niter,
+      (unsigned long long)J.pp.npoly, (unsigned long long)J.tamm_d, (unsigned long long)J.nen,
+      (unsigned long long)p->nval, (unsigned long long)J.nbsum, (unsigned long long)J.nq,
+      (unsigned long long)J.q0, (unsigned long long)J.pp.kdef, dbits(p->ecuts), dbits(J.de),
+      dbits(J.pp.c0), dbits(J.pp.c1), s->gen, dbits(p->early_exit_eps),
+      (unsigned long long)(J.len != nullptr)};
+  key.insert(key.end(), std::begin(head), std::end(head));
+  if (J.len) key.insert(key.end(), J.nact.begin(), J.nact.end());
+  for (double c : J.pp.poly) key.push_back(dbits(c));
+  for (double c : J.pp.cheb) key.push_back(dbits(c));
+  for (const void *ptr : {(const void *)J.cmn, (const void *)J.cm, (const void *)J.P, (const void *)J.P2,
+                          (const void *)J.pn2, (const void *)J.pn, (const void *)J.V, (const void *)J.W,
+                          (const void *)J.hs, (const void *)J.tmp, (const void *)J.a, (const void *)J.b,
+                          (const void *)J.S, (const void *)J.chb, (const void *)J.chq, (const void *)J.de1,
+                          (const void *)J.zz0, (const void *)J.sig, (const void *)s->mixed,
+                          (const void *)J.clen, (const void *)J.dlen, (const void *)J.dslot})
+    key.push_back((unsigned long long)(uintptr_t)ptr);
+  if (s->mixed) {
+    int tune[4];
+    extern_mixed_tune(s, tune);
+    for (int t : tune) key.push_back((unsigned long long)t);
+  }
+}
+
+// alpha / beta of the current block back in chain order
+static int sigma_block_ab(SigmaJob &J, double *alpha, double *beta) {
+  ngw_session *s = J.s;
+  for (int w = 0; w < 2; ++w) {
+    double *dst = w == 0 ? alpha : beta;
+    if (!dst) continue;
+    std::vector<double> h((size_t)J.niter * J.nb);
+    NGW_CUDA(cudaMemcpyAsync(h.data(), w == 0 ? J.a : J.b, (size_t)J.niter * J.nb * 8,
+                             cudaMemcpyDeviceToHost, s->stream));
+    NGW_CUDA(cudaStreamSynchronize(s->stream));
+    for (int o = 0; o < J.nb; ++o)
+      std::memcpy(dst + ((size_t)J.q0 * J.nbsum + o) * J.niter, h.data() + (size_t)J.hslot[o] * J.niter,
+                  (size_t)J.niter * 8);
+  }
+  return NGW_OK;
+}
+
+static int sigma_finish(SigmaJob &J, double *sigma_c) {
+  ngw_session *s = J.s;
+  NGW_CUDA(cudaMemcpyAsync(sigma_c, J.sig, (size_t)J.p->nqp * J.nen * 16, cudaMemcpyDeviceToHost, s->stream));
+  NGW_CUDA(cudaStreamSynchronize(s->stream));
+  return check_status(s);
+}
+
 }  // namespace ngw
 
 using namespace ngw;
 
 extern "C" {
+
 
 int ngw_version(void) { return 100; }
 
@@ -768,179 +996,82 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
     return NGW_ERR_ARG;
   }
   PhaseTimer tm(s);
-  NGW_TRY(need_op(s));
-  tm.mark("pair_products");
-  if (!p || !e1 || !sigma_c || p->nen < 2 || p->niter < 1 || p->nqp < 1 || !p->qp_bands ||
-      p->nval < 1 || p->nval >= s->nmem) {
-    set_error("ngw_sigma_lanczos: bad arguments");
+  SigmaJob J;
+  NGW_TRY(sigma_prepare(J, s, p, e1));
+  tm.mark("plan");
+  for (int q0 = 0; q0 < p->nqp; q0 += J.nq_blk) {
+    NGW_TRY(sigma_block_setup(J, q0));
+    std::vector<unsigned long long> key;
+    sigma_key(J, key);
+    tm.mark("block_setup");
+    NGW_TRY(run_graphed(s, key, [&]() { return sigma_region(J); }));
+    tm.mark("region");
+    NGW_TRY(sigma_block_ab(J, alpha, beta));
+  }
+  return sigma_finish(J, sigma_c);
+}
+
+int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_sigma_params *params,
+                            const double *const *e1, double *const *sigma_c) {
+  if (!sessions || count < 1 || !params || !e1 || !sigma_c) {
+    set_error("ngw_sigma_lanczos_batch: bad arguments");
     return NGW_ERR_ARG;
   }
-  const int nbsum = p->nbands_sum > 0 ? p->nbands_sum : s->nmem;
-  if (nbsum > s->nmem) {
-    set_error("nbands_sum > nmem");
-    return NGW_ERR_ARG;
-  }
-  for (int i = 0; i < p->nqp; ++i)
-    if (p->qp_bands[i] < 1 || p->qp_bands[i] > s->nmem) {
-      set_error("qp band %d out of range", p->qp_bands[i]);
+  for (int i = 0; i < count; ++i) {
+    if (!sessions[i] || !e1[i] || !sigma_c[i]) {
+      set_error("ngw_sigma_lanczos_batch: entry %d is null", i);
       return NGW_ERR_ARG;
     }
-  if (p->chain_niter)
-    for (int i = 0; i < p->nqp * nbsum; ++i)
-      if (p->chain_niter[i] < 1 || p->chain_niter[i] > p->niter) {
-        set_error("chain_niter[%d] = %d out of 1..niter", i, p->chain_niter[i]);
+    if (sessions[i]->device != sessions[0]->device) {
+      set_error("ngw_sigma_lanczos_batch: sessions on different devices");
+      return NGW_ERR_ARG;
+    }
+    for (int k = 0; k < i; ++k)
+      if (sessions[k] == sessions[i]) {
+        set_error("ngw_sigma_lanczos_batch: session %d appears twice", i);
         return NGW_ERR_ARG;
       }
-  if (!(p->early_exit_eps >= 0.0)) {
-    set_error("early_exit_eps must be >= 0");
-    return NGW_ERR_ARG;
   }
-  if (!all_finite(e1, s->nmem)) {
-    set_error("non-finite energies");
-    return NGW_ERR_NONFINITE;
-  }
-  NGW_CUDA(cudaSetDevice(s->device));
-  const int ncv = s->ncv, n = s->n_isdf, nen = p->nen, niter = p->niter;
-  const int tamm_d = p->tamm_d ? 1 : 0;
-  // Chebyshev interval (mixed): [0, 1.02 lambda_max(C)] unless given; C is
-  // positive definite, and the interval must contain its whole spectrum for the
-  // Clenshaw recurrence to be stable (the reference's fit range need not).
-  double lo = p->cheb_lo, hi = p->cheb_hi;
-  PolyPlan pp;
-  NGW_TRY(make_plan(s, pp, p->polynomial, p->npoly, tamm_d, lo, hi));
-  tm.mark("plan");
-  // chain blocking: whole QP states per block
-  int nq_blk = p->nqp;
-  if (p->block_chains > 0) nq_blk = std::max(1, std::min(p->nqp, p->block_chains / nbsum));
-  const int nb_max = nq_blk * nbsum;
-  double *de1, *zz0, *sig, *cmn, *cm, *P, *P2, *pn2, *pn, *V, *W, *hs, *tmp, *a, *b, *S;
-  int *chb, *chq;
-  NGW_TRY(scratch(s, SL_E1, (size_t)s->nmem * 8, (void **)&de1));
-  NGW_TRY(scratch(s, SL_ZZ0, (size_t)p->nqp * 8, (void **)&zz0));
-  NGW_TRY(scratch(s, SL_SIG, (size_t)p->nqp * nen * 16, (void **)&sig));
-  NGW_TRY(scratch(s, SL_CMN, (size_t)n * nb_max * 8, (void **)&cmn));
-  NGW_TRY(scratch(s, SL_CM, (size_t)n * nb_max * 8, (void **)&cm));
-  NGW_TRY(scratch(s, SL_P, (size_t)ncv * nb_max * 8, (void **)&P));
-  NGW_TRY(scratch(s, SL_P2, (size_t)ncv * nb_max * 8, (void **)&P2));
-  NGW_TRY(scratch(s, SL_PN2, (size_t)nb_max * 8, (void **)&pn2));
-  NGW_TRY(scratch(s, SL_PN, (size_t)nb_max * 8, (void **)&pn));
-  NGW_TRY(scratch(s, SL_WVEC, (size_t)ncv * nb_max * 8, (void **)&W));
-  NGW_TRY(scratch(s, SL_HS, (size_t)ncv * nb_max * 8, (void **)&hs));
-  NGW_TRY(scratch(s, SL_TMP, (size_t)ncv * nb_max * 8, (void **)&tmp));
-  NGW_TRY(scratch(s, SL_A, (size_t)niter * nb_max * 8, (void **)&a));
-  NGW_TRY(scratch(s, SL_B, (size_t)niter * nb_max * 8, (void **)&b));
-  NGW_TRY(scratch(s, SL_SPECS, (size_t)(nen + 1) * nb_max * 16, (void **)&S));
-  NGW_TRY(scratch(s, SL_CHB, (size_t)2 * nb_max * 4, (void **)&chb));
-  NGW_TRY(scratch(s, SL_CHQ, (size_t)2 * nb_max * 4, (void **)&chq));
-  NGW_TRY(scratch(s, SL_VEC, (size_t)ncv * nb_max * 8, (void **)&V));
-  int *clen, *dlen, *dslot;
-  NGW_TRY(scratch(s, SL_CLEN, (size_t)nb_max * 4, (void **)&clen));
-  NGW_TRY(scratch(s, SL_LEN, (size_t)nb_max * 4, (void **)&dlen));
-  NGW_TRY(scratch(s, SL_SLOT, (size_t)nb_max * 4, (void **)&dslot));
-  if (s->precision == NGW_PREC_MIXED) NGW_TRY(mixed_prepare_chains(s, nb_max, 0, 0, 0));
-  NGW_CUDA(cudaMemcpyAsync(de1, e1, (size_t)s->nmem * 8, cudaMemcpyHostToDevice, s->stream));
-  // energy grid origin per QP state: en0 = e1(m) - deltae/2, step deltae/(nen-1)
-  std::vector<double> hz0(p->nqp);
-  for (int i = 0; i < p->nqp; ++i) hz0[i] = e1[p->qp_bands[i] - 1] - p->deltae * 0.5;
-  const double de = p->deltae / (double)(nen - 1);
-  NGW_CUDA(cudaMemcpyAsync(zz0, hz0.data(), (size_t)p->nqp * 8, cudaMemcpyHostToDevice, s->stream));
-  const double one = 1.0, zero = 0.0;
-  std::vector<int> hb(2 * nb_max), hq(2 * nb_max), hl(nb_max), hslot(nb_max), order(nb_max);
-  std::vector<int> nact;
-  for (int q0 = 0; q0 < p->nqp; q0 += nq_blk) {
-    const int nq = std::min(nq_blk, p->nqp - q0);
-    const int nb = nq * nbsum;
-    // chain o = (iq, n) of the block, o = iq*nbsum + n-1: band1 = m (QP band),
-    // band2 = n.  With per-chain lengths the chains run longest first (stable
-    // order): position j holds chain order[j], slot[o] is o's position.
-    for (int o = 0; o < nb; ++o) order[o] = o;
-    const int *len = p->chain_niter ? p->chain_niter + (size_t)q0 * nbsum : nullptr;
-    if (len)
-      std::stable_sort(order.begin(), order.begin() + nb, [&](int x, int y) { return len[x] > len[y]; });
-    for (int j = 0; j < nb; ++j) {
-      const int o = order[j], iq = o / nbsum, jn = o % nbsum;
-      hb[j] = p->qp_bands[q0 + iq];
-      hb[nb + j] = jn + 1;
-      hq[j] = q0 + iq;
-      hl[j] = len ? len[o] : niter;
-      hslot[o] = j;
+  std::vector<SigmaJob> jobs(count);
+  for (int i = 0; i < count; ++i) {
+    NGW_TRY(sigma_prepare(jobs[i], sessions[i], &params[i], e1[i]));
+    if (jobs[i].nq_blk < params[i].nqp) {
+      set_error("ngw_sigma_lanczos_batch: entry %d needs %d chain blocks (one per entry allowed)", i,
+                (params[i].nqp + jobs[i].nq_blk - 1) / jobs[i].nq_blk);
+      return NGW_ERR_ARG;
     }
-    nact.assign(niter, nb);
-    if (len)
-      for (int k = 0; k < niter; ++k) {
-        int c = 0;
-        while (c < nb && hl[c] > k) ++c;
-        nact[k] = c;
+    NGW_TRY(sigma_block_setup(jobs[i], 0));
+  }
+  ngw_session *s0 = sessions[0];
+  // one graph for the whole batch: entry i is a branch on its session's
+  // stream, forked from and joined back into session 0's stream
+  std::vector<unsigned long long> key = {0xBA7C4ull, (unsigned long long)count};
+  for (int i = 0; i < count; ++i) {
+    key.push_back((unsigned long long)(uintptr_t)sessions[i]);
+    key.push_back((unsigned long long)(uintptr_t)sessions[i]->cublas_ws);
+    sigma_key(jobs[i], key);
+  }
+  std::vector<cudaEvent_t> ev(count + 1, nullptr);
+  for (auto &e : ev) NGW_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  auto region = [&]() -> int {
+    NGW_CUDA(cudaEventRecord(ev[count], s0->stream));
+    for (int i = 0; i < count; ++i) {
+      ngw_session *si = sessions[i];
+      if (si->stream != s0->stream) NGW_CUDA(cudaStreamWaitEvent(si->stream, ev[count], 0));
+      NGW_TRY(sigma_region(jobs[i]));
+      if (si->stream != s0->stream) {
+        NGW_CUDA(cudaEventRecord(ev[i], si->stream));
+        NGW_CUDA(cudaStreamWaitEvent(s0->stream, ev[i], 0));
       }
-    NGW_CUDA(cudaMemcpyAsync(chb, hb.data(), (size_t)2 * nb * 4, cudaMemcpyHostToDevice, s->stream));
-    NGW_CUDA(cudaMemcpyAsync(chq, hq.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
-    NGW_CUDA(cudaMemcpyAsync(dlen, hl.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
-    NGW_CUDA(cudaMemcpyAsync(dslot, hslot.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
-    NGW_CUDA(cudaStreamSynchronize(s->stream));
-    const double eps = p->early_exit_eps;
-    auto region = [&]() -> int {
-      // start vectors  P = sqrtR * C^T M (psi_m psi_n)   (F90z:578-709), FP64
-      launch_pair_gather_cols(s->d_psi, n, chb, chb + nb, nb, cmn, s->stream);
-      NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, n, nb, n, &one, s->d_M, n, cmn, n,
-                             &zero, cm, n));
-      NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, ncv, nb, n, &one, s->d_C, n, cm, n,
-                             &zero, P, ncv));
-      launch_norms(P, ncv, nb, s->d_sqrtR, tamm_d, P2, pn2, s->stream);
-      NGW_CUDA(cudaMemsetAsync(a, 0, (size_t)niter * nb * 8, s->stream));
-      NGW_CUDA(cudaMemsetAsync(b, 0, (size_t)niter * nb * 8, s->stream));
-      // pnorm = sqrt(pnorm2), v0 = P / pnorm   (F90z:707-709, lanczos_spectra_lowcomsym.F90:68-70)
-      launch_sqrt_vec(pn2, pn, nb, s->stream);
-      launch_lanczos_init(P2, ncv, pn, V, hs, s->d_sqrtR, ncv, nb, tamm_d, b, niter, dlen, clen,
-                          s->stream);
-      NGW_TRY(lanczos_dev(s, pp, nb, niter, V, W, hs, tmp, a, b, clen, eps, len ? &nact : nullptr));
-      launch_sigma_spectra(a, b, niter, nb, de1, chb + nb, chq, zz0, de, nen, p->ecuts, p->nval, S,
-                           clen, s->stream);
-      launch_sigma_reduce(S, pn2, de1, chb + nb, zz0 + q0, de, nen, p->ecuts, p->nval, nbsum, nq,
-                          tamm_d, sig + (size_t)2 * q0 * nen, 0, dslot, s->stream);
-      NGW_CUDA(cudaGetLastError());
-      return NGW_OK;
-    };
-    std::vector<unsigned long long> key = {
-        (unsigned long long)s->precision, (unsigned long long)nb, (unsigned long long)niter,
-        (unsigned long long)pp.npoly, (unsigned long long)tamm_d, (unsigned long long)nen,
-        (unsigned long long)p->nval, (unsigned long long)nbsum, (unsigned long long)nq,
-        (unsigned long long)q0, (unsigned long long)pp.kdef, dbits(p->ecuts), dbits(de),
-        dbits(pp.c0), dbits(pp.c1), s->gen, dbits(eps), (unsigned long long)(len != nullptr)};
-    if (len) key.insert(key.end(), nact.begin(), nact.end());
-    for (double c : pp.poly) key.push_back(dbits(c));
-    for (double c : pp.cheb) key.push_back(dbits(c));
-    for (const void *ptr : {(const void *)cmn, (const void *)cm, (const void *)P, (const void *)P2,
-                            (const void *)pn2, (const void *)pn, (const void *)V, (const void *)W,
-                            (const void *)hs, (const void *)tmp, (const void *)a, (const void *)b,
-                            (const void *)S, (const void *)chb, (const void *)chq, (const void *)de1,
-                            (const void *)zz0, (const void *)sig, (const void *)s->mixed,
-                            (const void *)clen, (const void *)dlen, (const void *)dslot})
-      key.push_back((unsigned long long)(uintptr_t)ptr);
-    if (s->mixed) {
-      int tune[4];
-      extern_mixed_tune(s, tune);
-      for (int t : tune) key.push_back((unsigned long long)t);
     }
-    tm.mark("block_setup");
-    NGW_TRY(run_graphed(s, key, region));
-    tm.mark("region");
-    // alpha / beta back in chain order
-    for (int w = 0; w < 2; ++w) {
-      double *dst = w == 0 ? alpha : beta;
-      if (!dst) continue;
-      std::vector<double> h((size_t)niter * nb);
-      NGW_CUDA(cudaMemcpyAsync(h.data(), w == 0 ? a : b, (size_t)niter * nb * 8, cudaMemcpyDeviceToHost,
-                               s->stream));
-      NGW_CUDA(cudaStreamSynchronize(s->stream));
-      for (int o = 0; o < nb; ++o)
-        std::memcpy(dst + ((size_t)q0 * nbsum + o) * niter, h.data() + (size_t)hslot[o] * niter,
-                    (size_t)niter * 8);
-    }
-  }
-  NGW_CUDA(cudaMemcpyAsync(sigma_c, sig, (size_t)p->nqp * nen * 16, cudaMemcpyDeviceToHost,
-                           s->stream));
-  NGW_CUDA(cudaStreamSynchronize(s->stream));
-  return check_status(s);
+    return NGW_OK;
+  };
+  const int rc = run_graphed(s0, key, region);
+  if (rc == NGW_OK) NGW_CUDA(cudaStreamSynchronize(s0->stream));
+  for (auto &e : ev) cudaEventDestroy(e);
+  NGW_TRY(rc);
+  for (int i = 0; i < count; ++i) NGW_TRY(sigma_finish(jobs[i], sigma_c[i]));
+  return NGW_OK;
 }
 
 int ngw_qp_newton(ngw_session *s, int nqp, int nen, const double *sigma_c_ev, const double *e1_ev,
