@@ -132,6 +132,121 @@ def solve_once(sess, op, qp, poly, wl, sigx, vxc):
 LARGE_OPERATORS = {"large-molecule": (4800, 240, 960), "batched-max": (1120, 140, 560)}
 
 
+def random_operator(n_isdf, nocc, nemp, seed):
+    """Random ISDF operator of given dimensions (timing only): orbital values at
+    the points ~ N(0, 0.05^2), M = G G^T * 0.02, sorted random KS energies (Ry)
+    in the ranges of the synthetic molecules."""
+    rng = np.random.default_rng(seed)
+    nmem = nocc + nemp
+    psi = np.asfortranarray(rng.standard_normal((n_isdf, nmem)) * 0.05)
+    g = rng.standard_normal((n_isdf, n_isdf)) / np.sqrt(n_isdf)
+    m = np.asfortranarray(g @ g.T * 0.02)
+    e1 = np.sort(np.concatenate([rng.uniform(-1.5, -0.5, nocc), rng.uniform(-0.3, 1.0, nemp)]))
+    return psi, m, e1
+
+
+def batched_workload(local, nmol, nqp, seed=2024, nocc_range=(20, 140)):
+    """Uneven molecules in one batch (the batched configuration: n_occ in
+    nocc_range, n_empty = 3-4 n_occ, n_isdf = 8 n_occ, per-chain Lanczos
+    lengths 100-300 seeded per chain), random operators of those dimensions.
+    Times one ngw_sigma_lanczos_batch call (graph replay) against the same
+    solves issued one molecule after another, both mixed precision."""
+    import nanogw_b200 as ngw
+    from nanogw_b200.api import lowcomsym_pairs, sqrt_r
+    from nanogw_b200.polyfit import sigma_polynomial
+    rng = np.random.default_rng(seed)
+    sessions, reqs, dims = [], [], []
+    for i in range(nmol):
+        nocc = int(rng.integers(nocc_range[0], nocc_range[1] + 1))
+        nemp = int(nocc * rng.uniform(3.0, 4.0))
+        n_isdf = 8 * nocc
+        psi, m, e1 = random_operator(n_isdf, nocc, nemp, seed + 1 + i)
+        s = ngw.Session(local, "mixed")
+        s.set_isdf(psi, m)
+        cv = lowcomsym_pairs(nocc, nocc + nemp)
+        s.set_pairs(cv, sqrt_r(e1, cv))
+        poly, _, _ = sigma_polynomial(e1, nocc, nocc + nemp, 12)
+        nq = min(nqp, nocc + nemp)
+        qp = np.arange(nocc - nq // 2 + 1, nocc - nq // 2 + 1 + nq, dtype=np.int32)
+        lens = rng.integers(100, 301, size=(nq, nocc + nemp))
+        reqs.append(dict(e1=e1, nval=nocc, qp_bands=qp, nen=400, deltae=4.0, ecuts=0.02, niter=300,
+                         polynomial=poly, chain_niter=lens))
+        sessions.append(s)
+        dims.append({"n_occ": nocc, "n_empty": nemp, "n_isdf": n_isdf, "ncv": int(len(cv)),
+                     "chains": int(nq * (nocc + nemp)), "chain_steps": int(lens.sum())})
+    import torch
+    solves = sum(len(r["qp_bands"]) for r in reqs)
+    for s, r in zip(sessions, reqs):          # tunes every shape, warms the per-session graphs
+        for _ in range(2):
+            s.calculate_sigma_lanczos(**r)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for s, r in zip(sessions, reqs):
+        s.calculate_sigma_lanczos(**r)
+    seq = time.perf_counter() - t
+    for _ in range(2):                        # eager + capture of the batch graph
+        ngw.sigma_lanczos_batch(sessions, reqs)
+    t = time.perf_counter()
+    ngw.sigma_lanczos_batch(sessions, reqs)
+    bat = time.perf_counter() - t
+    for s in sessions:
+        s.close()
+    return {"workload": f"{nmol} uneven molecules, {nqp} QP states each, per-chain lengths 100-300",
+            "values": "random operators of the molecules' dimensions (timing only)",
+            "solves": solves, "batched_solves_per_s": solves / bat, "sequential_solves_per_s": solves / seq,
+            "batched_s": bat, "sequential_s": seq, "molecules": dims}
+
+
+def serving_workload(local, nreq, workers, seed=77, nocc_range=(8, 48), load=0.8):
+    """A stream of Sigma_c requests (the serving configuration with n_occ
+    log-uniform in nocc_range, n_empty = 4 n_occ, n_isdf = 8 n_occ, 4-16 QP
+    states, 100-300 Lanczos steps) on random operators of those dimensions.
+    Closed loop (all requests queued at t = 0) in mixed precision and in the
+    plain FP64 per-request form give the throughputs; Poisson arrivals at
+    ``load`` x the mixed closed-loop rate give p50/p99 latency."""
+    from nanogw_b200.polyfit import sigma_polynomial
+    from nanogw_b200.serving import SigmaRequest, SigmaServer
+    rng = np.random.default_rng(seed)
+    base = []
+    for i in range(nreq):
+        nocc = int(round(np.exp(rng.uniform(np.log(nocc_range[0]), np.log(nocc_range[1])))))
+        nemp = 4 * nocc
+        psi, m, e1 = random_operator(8 * nocc, nocc, nemp, seed + 1 + i)
+        nq = int(rng.integers(4, 17))
+        qp = np.arange(nocc - nq // 2 + 1, nocc - nq // 2 + 1 + nq, dtype=np.int32)
+        poly, _, _ = sigma_polynomial(e1, nocc, nocc + nemp, 12)
+        base.append(dict(rid=i, mol_id=1000 + i, psi_intp=psi, mmtrx=m, e1=e1, nval=nocc, qp_bands=qp,
+                         polynomial=poly, niter=int(rng.integers(100, 301)), nen=400, deltae=4.0))
+
+    passes = iter(range(1, 100))
+
+    def make(arrivals=None):
+        # a new molecule id on every pass: each request uploads its operator
+        off = next(passes) * 100000
+        return [SigmaRequest(**dict(b, mol_id=b["mol_id"] + off),
+                             arrival=0.0 if arrivals is None else float(arrivals[i]))
+                for i, b in enumerate(base)]
+
+    out = {"workload": f"{nreq} requests, n_occ log-uniform {nocc_range[0]}-{nocc_range[1]}, "
+                       f"4-16 QP states, 100-300 Lanczos steps",
+           "values": "random operators of the requests' dimensions (timing only)", "workers": workers}
+    srv = SigmaServer(device=local, workers=workers, precision="mixed")
+    srv.run(make(), realtime=False)                 # warm-up: tunes every shape
+    closed = srv.run(make(), realtime=False)
+    rate = load * closed["requests"] / closed["wall_s"]
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    live = srv.run(make(arrivals), realtime=True)
+    srv.close()
+    f64 = SigmaServer(device=local, workers=workers, precision="fp64")
+    f64_closed = f64.run(make(), realtime=False)
+    f64.close()
+    out.update({"mixed_solves_per_s": closed["solves_per_s"], "fp64_solves_per_s": f64_closed["solves_per_s"],
+                "speedup_vs_fp64": closed["solves_per_s"] / f64_closed["solves_per_s"],
+                "arrival_rate_per_s": rate, "p50_ms": live["p50_ms"], "p99_ms": live["p99_ms"],
+                "live_solves_per_s": live["solves_per_s"], "solves": closed["solves"]})
+    return out
+
+
 def gemm_scan(local, name, nbs, reps=10):
     """Throughput of the two split-BF16 tcgen05 GEMMs of one matvec at a large
     operator's dimensions.  The operator is random (orbital values at the
@@ -203,6 +318,11 @@ def main():
     ap.add_argument("--scan-chains", default="1024,2048")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the large-operator GEMM line of the default run")
+    ap.add_argument("--workload", default="12atom", choices=["12atom", "batched", "serving"],
+                    help="batched: uneven molecules in one graph launch; serving: request stream")
+    ap.add_argument("--batched-qp", type=int, default=2)
+    ap.add_argument("--serving-requests", type=int, default=24)
+    ap.add_argument("--serving-workers", type=int, default=2)
     args = ap.parse_args()
     W = max(3, args.warmup)
     K = args.steps
@@ -221,6 +341,17 @@ def main():
 
     wl = dict(WORKLOAD)
     import nanogw_b200 as ngw
+
+    if args.workload != "12atom":
+        if rank == 0:
+            if args.workload == "batched":
+                res = batched_workload(local, 8, args.batched_qp)
+            else:
+                res = serving_workload(local, args.serving_requests, args.serving_workers)
+            print(json.dumps(res), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     if args.gemm_scan:
         if rank == 0:
