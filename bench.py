@@ -36,6 +36,9 @@ WORKLOAD = dict(name="12-atom molecule, 30 occ + 90 empty, 600 ISDF points, 150 
                 h=0.35, n_occ=30, n_empty=90, n_isdf=600, niter=150, n_qp=6, nen=400,
                 deltae=4.0, ecuts=0.02, npoly=12, seed=11)
 METRIC = "Sigma_c solves/s"
+# DRAM bytes (read + write) of one in-situ GEMM1 + GEMM2 pair of the 12-atom
+# workload from an ncu capture, by tile choice "bn1,var1,split1,bn2,var2"
+MEASURED_TRAFFIC = {"80,3,3,64,4": 15.37e6 + 28.84e6}
 RYD = 13.60569193
 
 
@@ -471,8 +474,18 @@ def main():
         flops = 2.0 * M1 * N1 * K1 + 2.0 * M2 * N2 * K2
         achieved = flops / ((us1 + us2) * 1e-6) / 1e12
         hbm, bf16, bf16s, src = load_peaks()
+        tiles = f"{BN1},{v1},{sp1},{BN2},{v2}"
+        # algorithmic bytes of the pair: split-BF16 operands (4 B per element
+        # for hi + lo), GEMM1 output, GEMM2's Clenshaw vectors (3 FP32 reads,
+        # FP32 + hi/lo writes)
+        alg_bytes = (4.0 * (M1 * K1 + N1 * K1) + 4.0 * M1 * N1 + 4.0 * (M2 * K2 + N2 * K2)
+                     + 20.0 * M2 * N2)
         roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                "frac": achieved / bf16, "traffic": None,
+                "frac": achieved / bf16, "traffic": MEASURED_TRAFFIC.get(tiles),
+                "traffic_note": "ncu dram__bytes_read+write of one GEMM1 + GEMM2 pair in situ "
+                                "(--ncu-case); null when the tuned tiles differ from the "
+                                "profiled ones",
+                "algorithmic_bytes_per_matvec": alg_bytes,
                 "kernel": "k_tc_gemm (GEMM1 + GEMM2 of one matvec)",
                 "us_per_launch": [us1, us2], "shapes": [[M1, N1, K1, BN1, sp1, v1], [M2, N2, K2, BN2, 1, v2]],
                 "tiles_env": f"{BN1},{v1},{sp1},{BN2},{v2},{r1},{r2}",
