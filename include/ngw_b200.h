@@ -35,6 +35,9 @@
  *   ngw_build_fxc_kernel          -- f_xc block, shared/isdf_parallel_sym_UltraLowMem.F90:809-839
  *   ngw_build_isdf_kernel         -- ISDF fit + both kernel blocks on the device,
  *                                    shared/isdf_parallel_sym_UltraLowMem.F90:439-889
+ *   ngw_fock_exchange             -- Zfock_exchange          SIGMA/fock_exchange.F90z:2
+ *   ngw_vxc_matrix                -- Zvxc / Zvxcmtxel        SIGMA/vxc.F90z:2,
+ *                                    shared/vxcmtxel.F90z:2
  */
 #ifndef NGW_B200_H
 #define NGW_B200_H
@@ -225,6 +228,26 @@ int ngw_build_isdf_kernel(ngw_session *s, int ngrid, int nmem, const double *psi
                           const int *grid_idx, int n_isdf, const int *intp, int mv, int nfft,
                           double h, double trunc, const double *rho, double *psi_intp,
                           double *mmtrx, double *mxc);
+
+/* Bare exchange matrix Sigma_x (Ry) between the Sigma bands, finite system,
+ * one spin, C1 (SIGMA/fock_exchange.F90z:16-228):
+ *   K_x(m1, m2) = -(ntrans / h^3) sum_{n <= maxv} occ_n <psi_m1 | psi_n V_c[psi_n psi_m2]>
+ * with V_c the FFT-Poisson solve of ngw_build_coulomb_kernel (box nfft, spacing
+ * h, truncation radius trunc) and maxv the highest band with occ > 0.01.
+ * psi (ngrid x nmem) orbitals on the grid (sum psi^2 ntrans = 1), grid_idx
+ * (3 x ngrid), occ (nmem) occupations per spin, sig_bands (nsig, 1-based).
+ * kx out: (nsig x nsig), symmetric. */
+int ngw_fock_exchange(ngw_session *s, int ngrid, int nmem, const double *psi, const int *grid_idx,
+                      int nfft, double h, double trunc, const double *occ, int nsig,
+                      const int *sig_bands, int ntrans, double *kx);
+
+/* V_xc matrix elements (Ry) of the LDA (Slater exchange + Perdew-Zunger
+ * correlation, x2 to Rydberg as shared/xc_module.F90:523-829) between the
+ * Sigma bands: V(m1, m2) = ntrans <psi_m1 | v(rho) | psi_m2>
+ * (SIGMA/vxc.F90z:147-165, shared/vxcmtxel.F90z).  rho (ngrid) > 0.
+ * vxc out (nsig x nsig); vx (optional) the exchange part alone. */
+int ngw_vxc_matrix(ngw_session *s, int ngrid, int nmem, const double *psi, const double *rho, int nsig,
+                   const int *sig_bands, int ntrans, double *vxc, double *vx);
 
 #ifdef __cplusplus
 }

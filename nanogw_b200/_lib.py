@@ -54,6 +54,8 @@ SIGNATURES = {
     "ngw_build_coulomb_kernel": (_I, [_P, _I, _I, _P, _P, _I, _D, _D, _P]),
     "ngw_build_fxc_kernel": (_I, [_P, _I, _I, _P, _P, _D, _P, _P]),
     "ngw_build_isdf_kernel": (_I, [_P, _I, _I, _P, _P, _I, _P, _I, _I, _D, _D, _P, _P, _P, _P]),
+    "ngw_fock_exchange": (_I, [_P, _I, _I, _P, _P, _I, _D, _D, _P, _I, _P, _I, _P]),
+    "ngw_vxc_matrix": (_I, [_P, _I, _I, _P, _P, _I, _P, _I, _P, _P]),
 }
 
 

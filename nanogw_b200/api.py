@@ -245,6 +245,29 @@ class Session:
                                           _p(mx)))
         return pi, m, mx
 
+    def fock_exchange(self, psi, grid_idx, nfft, h, trunc, occ, sig_bands, ntrans=1):
+        """Bare exchange matrix Sigma_x (Ry) between ``sig_bands`` (1-based)."""
+        ps = _f64(psi)
+        g = np.ascontiguousarray(grid_idx, dtype=np.int32)
+        oc = np.ascontiguousarray(occ, dtype=np.float64)
+        sb = np.ascontiguousarray(sig_bands, dtype=np.int32)
+        kx = np.zeros((len(sb), len(sb)), order="F")
+        check(lib().ngw_fock_exchange(self._h, ps.shape[0], ps.shape[1], _p(ps), _p(g), int(nfft),
+                                      float(h), float(trunc), _p(oc), len(sb), _p(sb), int(ntrans),
+                                      _p(kx)))
+        return kx
+
+    def vxc_matrix(self, psi, rho, sig_bands, ntrans=1):
+        """(V_xc, V_x) matrices (Ry) of the LDA between ``sig_bands``."""
+        ps = _f64(psi)
+        r = np.ascontiguousarray(rho, dtype=np.float64)
+        sb = np.ascontiguousarray(sig_bands, dtype=np.int32)
+        v = np.zeros((len(sb), len(sb)), order="F")
+        vx = np.zeros((len(sb), len(sb)), order="F")
+        check(lib().ngw_vxc_matrix(self._h, ps.shape[0], ps.shape[1], _p(ps), _p(r), len(sb), _p(sb),
+                                   int(ntrans), _p(v), _p(vx)))
+        return v, vx
+
     def build_coulomb_kernel(self, zeta, grid_idx, nfft, h, trunc):
         zt = _f64(zeta)
         g = np.ascontiguousarray(grid_idx, dtype=np.int32)

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "ngw_internal.h"
+#include "xc_lda.cuh"
 
 namespace ngw {
 
@@ -79,24 +80,26 @@ __global__ void k_mul_coulomb(cufftDoubleComplex *__restrict__ f, const double *
 }
 
 
-// M = (ntrans / hcub) zeta^T (v_c zeta) from a device-resident zeta
-// (ngrid x n_isdf, column-major) and grid coordinates (3 x ngrid).
-int coulomb_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const int *dg, int nfft,
-                 double h, double trunc, double *dm) {
+// v_c * rho for ncol columns (ngrid x ncol, column-major, ld ngrid) on the
+// device: each column packed into the zero-padded FFT box, D2Z, multiplied by
+// the truncated Coulomb kernel, Z2D, unpacked with 1/nfft^3
+// (shared/fft_module.F90z:122-177).  Columns go through in batches of boxes
+// that stay under ~2 GB.
+int poisson_apply(ngw_session *s, int ngrid, int ncol, const double *drho, const int *dg, int nfft,
+                  double h, double trunc, double *dv) {
   const int n = nfft;
   const size_t bsz = (size_t)n * n * n;
   const size_t csz = (size_t)n * n * (n / 2 + 1);
-  // batch so that the boxes stay under ~2 GB
   int batch = (int)std::max<size_t>(1, (size_t)(2ull << 30) / (bsz * 8 + csz * 16));
-  if (batch > n_isdf) batch = n_isdf;
-  double *dvz = nullptr, *box = nullptr, *vtab = nullptr;
+  if (batch > ncol) batch = ncol;
+  double *box = nullptr, *vtab = nullptr;
   cufftDoubleComplex *spec = nullptr;
   int rc = NGW_OK;
   cufftHandle pf = 0, pb = 0;
   bool have_pf = false, have_pb = false;
   do {
-    if (dalloc(s, (void **)&dvz, (size_t)ngrid * n_isdf * 8) || dalloc(s, (void **)&box, bsz * batch * 8) ||
-        dalloc(s, (void **)&spec, csz * batch * 16) || dalloc(s, (void **)&vtab, csz * 8)) {
+    if (dalloc(s, (void **)&box, bsz * batch * 8) || dalloc(s, (void **)&spec, csz * batch * 16) ||
+        dalloc(s, (void **)&vtab, csz * 8)) {
       rc = NGW_ERR_OOM;
       break;
     }
@@ -118,12 +121,12 @@ int coulomb_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const 
     cufftSetStream(pf, s->stream);
     cufftSetStream(pb, s->stream);
     const double scale = 1.0 / ((double)n * (double)n * (double)n);
-    for (int c0 = 0; c0 < n_isdf && rc == NGW_OK; c0 += batch) {
-      const int nc = std::min(batch, n_isdf - c0);
+    for (int c0 = 0; c0 < ncol && rc == NGW_OK; c0 += batch) {
+      const int nc = std::min(batch, ncol - c0);
       cudaMemsetAsync(box, 0, bsz * batch * 8, s->stream);
       int bx = (ngrid + 255) / 256;
       if (bx > 256) bx = 256;
-      k_pack<<<dim3(bx, nc), 256, 0, s->stream>>>(dz + (size_t)c0 * ngrid, ngrid, ngrid, dg, n, box, nc);
+      k_pack<<<dim3(bx, nc), 256, 0, s->stream>>>(drho + (size_t)c0 * ngrid, ngrid, ngrid, dg, n, box, nc);
       if (cufftExecD2Z(pf, box, spec) != CUFFT_SUCCESS) {
         set_error("cufftExecD2Z failed");
         rc = NGW_ERR_CUDA;
@@ -135,8 +138,7 @@ int coulomb_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const 
         rc = NGW_ERR_CUDA;
         break;
       }
-      k_unpack<<<dim3(bx, nc), 256, 0, s->stream>>>(box, ngrid, dg, n, scale, dvz + (size_t)c0 * ngrid,
-                                                    ngrid);
+      k_unpack<<<dim3(bx, nc), 256, 0, s->stream>>>(box, ngrid, dg, n, scale, dv + (size_t)c0 * ngrid, ngrid);
     }
     if (rc != NGW_OK) break;
     if (cudaGetLastError() != cudaSuccess) {
@@ -144,6 +146,28 @@ int coulomb_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const 
       rc = NGW_ERR_CUDA;
       break;
     }
+  } while (0);
+  cudaStreamSynchronize(s->stream);
+  if (have_pf) cufftDestroy(pf);
+  if (have_pb) cufftDestroy(pb);
+  dfree(s, box, bsz * batch * 8);
+  dfree(s, spec, csz * batch * 16);
+  dfree(s, vtab, csz * 8);
+  return rc;
+}
+
+// M = (ntrans / hcub) zeta^T (v_c zeta) from a device-resident zeta
+// (ngrid x n_isdf, column-major) and grid coordinates (3 x ngrid).
+int coulomb_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const int *dg, int nfft,
+                 double h, double trunc, double *dm) {
+  double *dvz = nullptr;
+  int rc = NGW_OK;
+  do {
+    if (dalloc(s, (void **)&dvz, (size_t)ngrid * n_isdf * 8)) {
+      rc = NGW_ERR_OOM;
+      break;
+    }
+    if ((rc = poisson_apply(s, ngrid, n_isdf, dz, dg, nfft, h, trunc, dvz)) != NGW_OK) break;
     const double nf = 1.0 / (h * h * h);
     const double zero = 0.0;
     if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n_isdf, n_isdf, ngrid, &nf, dz, ngrid, dvz, ngrid,
@@ -154,12 +178,7 @@ int coulomb_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const 
     }
   } while (0);
   cudaStreamSynchronize(s->stream);
-  if (have_pf) cufftDestroy(pf);
-  if (have_pb) cufftDestroy(pb);
   dfree(s, dvz, (size_t)ngrid * n_isdf * 8);
-  dfree(s, box, bsz * batch * 8);
-  dfree(s, spec, csz * batch * 16);
-  dfree(s, vtab, csz * 8);
   return rc;
 }
 
@@ -215,20 +234,6 @@ extern "C" int ngw_build_coulomb_kernel(ngw_session *s, int ngrid, int n_isdf, c
 // and f_c libxc's finite difference of the Perdew-Zunger potential
 // (LIB/libxc/src/lda.c:153-182, delta_rho = 1e-8, centred unless rho < 2 delta).
 namespace ngw {
-
-__device__ __forceinline__ double pz_vc(double rho) {
-  const double gamma = -0.1423, beta1 = 1.0529, beta2 = 0.3334;
-  const double a = 0.0311, b = -0.048, c = 0.0020, d = -0.0116;
-  const double rs = cbrt(3.0 / (4.0 * M_PI * rho));
-  if (rs >= 1.0) {
-    const double srs = sqrt(rs);
-    const double den = 1.0 + beta1 * srs + beta2 * rs;
-    const double ec = gamma / den;
-    return ec * (1.0 + 7.0 / 6.0 * beta1 * srs + 4.0 / 3.0 * beta2 * rs) / den;
-  }
-  const double lrs = log(rs);
-  return a * lrs + (b - a / 3.0) + 2.0 / 3.0 * c * rs * lrs + (2.0 * d - c) * rs / 3.0;
-}
 
 __global__ void k_fxc_lda(const double *__restrict__ rho, int n, double *__restrict__ fxc) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {

@@ -87,6 +87,19 @@ def build_operator(mol, n_isdf, session, qp_bands=(), seed=0, max_cvt_iter=10000
     return op
 
 
+def exchange_and_vxc(mol, session, qp_bands):
+    """Diagonal Sigma_x and V_xc (Ry) of the QP bands on the device
+    (``ngw_fock_exchange``, ``ngw_vxc_matrix``): closed shell, occupation 1 per
+    spin for the nval lowest bands, truncated Coulomb radius 2 rmax."""
+    occ = np.zeros(mol.nmem)
+    occ[: mol.nval] = 1.0
+    qp = np.asarray(qp_bands, dtype=np.int32)
+    nfft = fft_box_size(mol.rmax, mol.h)
+    kx = session.fock_exchange(mol.psi, mol.grid_idx, nfft, mol.h, 2.0 * mol.rmax, occ, qp)
+    vxc, _ = session.vxc_matrix(mol.psi, mol.rho, qp)
+    return np.diag(kx).copy(), np.diag(vxc).copy()
+
+
 def qp_bands_near_gap(nval, nqp):
     """The nqp bands nearest the gap: nqp/2 highest occupied, the rest lowest empty."""
     nocc = nqp // 2
