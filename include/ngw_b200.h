@@ -35,6 +35,8 @@
  *   ngw_build_fxc_kernel          -- f_xc block, shared/isdf_parallel_sym_UltraLowMem.F90:809-839
  *   ngw_build_isdf_kernel         -- ISDF fit + both kernel blocks on the device,
  *                                    shared/isdf_parallel_sym_UltraLowMem.F90:439-889
+ *   ngw_parsec_read / _write      -- parsec_wfn              shared/parsec_wfn.F90:20 (file
+ *                                    records :80-320,663-700)
  *   ngw_fock_exchange             -- Zfock_exchange          SIGMA/fock_exchange.F90z:2
  *   ngw_vxc_matrix                -- Zvxc / Zvxcmtxel        SIGMA/vxc.F90z:2,
  *                                    shared/vxcmtxel.F90z:2
@@ -228,6 +230,28 @@ int ngw_build_isdf_kernel(ngw_session *s, int ngrid, int nmem, const double *psi
                           const int *grid_idx, int n_isdf, const int *intp, int mv, int nfft,
                           double h, double trunc, const double *rho, double *psi_intp,
                           double *mmtrx, double *mxc);
+
+/* PARSEC wavefunction file (parsec.dat), finite system, real orbitals, one
+ * spin channel, in the record order shared/parsec_wfn.F90 reads.  Arrays
+ * are in file order (the reader's density reordering is ngw_shell_sort's
+ * job): gtable (3 x nwedge) integer grid coordinates, rho (nwedge), irep /
+ * e0 (Ry) / occ (nstate), iord (nwfn, 1-based state of each stored
+ * wavefunction), wfn (nwedge x nwfn), trans (3 x 3 x ntrans), chi
+ * (ntrans x ntrans).  Read: ngw_parsec_read_header fills the sizes, the
+ * caller allocates, ngw_parsec_read fills the arrays.  Periodic, complex or
+ * spin-polarised files return NGW_ERR_ARG. */
+typedef struct {
+  char datelabel[27];
+  int nspin, lcplx, per, ndim, nwedge, ntrans, nstate, nwfn;
+  double step;
+  double shift[3];
+} ngw_parsec_header;
+int ngw_parsec_read_header(const char *path, ngw_parsec_header *h);
+int ngw_parsec_read(const char *path, ngw_parsec_header *h, int *gtable, double *rho, int *irep,
+                    double *e0, double *occ, int *iord, double *wfn, double *trans, int *chi);
+int ngw_parsec_write(const char *path, const ngw_parsec_header *h, const int *gtable,
+                     const double *rho, const int *irep, const double *e0, const double *occ,
+                     const int *iord, const double *wfn, const double *trans, const int *chi);
 
 /* Bare exchange matrix Sigma_x (Ry) between the Sigma bands, finite system,
  * one spin, C1 (SIGMA/fock_exchange.F90z:16-228):

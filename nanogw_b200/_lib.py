@@ -55,6 +55,9 @@ SIGNATURES = {
     "ngw_build_fxc_kernel": (_I, [_P, _I, _I, _P, _P, _D, _P, _P]),
     "ngw_build_isdf_kernel": (_I, [_P, _I, _I, _P, _P, _I, _P, _I, _I, _D, _D, _P, _P, _P, _P]),
     "ngw_fock_exchange": (_I, [_P, _I, _I, _P, _P, _I, _D, _D, _P, _I, _P, _I, _P]),
+    "ngw_parsec_read_header": (_I, [ctypes.c_char_p, _P]),
+    "ngw_parsec_read": (_I, [ctypes.c_char_p, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "ngw_parsec_write": (_I, [ctypes.c_char_p, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ngw_vxc_matrix": (_I, [_P, _I, _I, _P, _P, _I, _P, _I, _P, _P]),
 }
 
@@ -66,6 +69,15 @@ class SigmaParams(ctypes.Structure):
         ("polynomial", _P), ("tamm_d", _I), ("nval", _I), ("nqp", _I), ("qp_bands", _P),
         ("nbands_sum", _I), ("block_chains", _I), ("cheb_lo", _D), ("cheb_hi", _D),
         ("chain_niter", _P), ("early_exit_eps", _D),
+    ]
+
+
+class ParsecHeader(ctypes.Structure):
+    """Mirror of ``ngw_parsec_header``."""
+    _fields_ = [
+        ("datelabel", ctypes.c_char * 27), ("nspin", _I), ("lcplx", _I), ("per", _I), ("ndim", _I),
+        ("nwedge", _I), ("ntrans", _I), ("nstate", _I), ("nwfn", _I), ("step", _D),
+        ("shift", _D * 3),
     ]
 
 
