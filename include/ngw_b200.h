@@ -28,6 +28,7 @@
  *   ngw_qp_newton                 -- QP part of printsigma  SIGMA/printsigma.F90:97-125
  *                                    (newtonr SIGMA/newtonr.f90:18)
  *   ngw_cvt / ngw_dedup_points    -- cvt shared/cvt.F90:8 and SIGMA/sigma.F90:377-461
+ *   ngw_cvt_device                -- cvt shared/cvt.F90:8, iterations on the device
  *   ngw_shell_sort                -- quicksort shared/quicksort.f90:19
  *   ngw_build_coulomb_kernel      -- Mmtrx build, shared/isdf_parallel_sym_UltraLowMem.F90:687-889
  *                                    (dpoisson shared/fft_module.F90z:122,
@@ -201,6 +202,12 @@ int ngw_shell_sort(int n, const double *arr, int *idx);
  * intp (n_intp) 1-based grid indices.  Bit-exact with the reference loops. */
 int ngw_cvt(int ngrid, const double *grid, const double *rho, int n_intp, double *pts,
             int max_iter, int *intp, int *iters);
+/* ngw_cvt with the O(N_grid x N_mu) work of every iteration on the device
+ * (nearest centres, weighted centroids, nearest grid points) and the
+ * order-dependent snap on the host; results bit-identical to ngw_cvt
+ * (separately rounded products and sums, the same summation orders). */
+int ngw_cvt_device(ngw_session *s, int ngrid, const double *grid, const double *rho, int n_intp,
+                   double *pts, int max_iter, int *intp, int *iters);
 /* de-duplicate CVT points by density (C1): returns the kept count in *nout */
 int ngw_dedup_points(int n, const int *intp, const double *rho, int *out, int *nout);
 /* Coulomb ISDF kernel: M = ntrans/hcub * zeta^T (v_c zeta) on the device.

@@ -50,6 +50,7 @@ SIGNATURES = {
     "ngw_mixed_gemm_shapes": (_I, [_P, _I, _P]),
     "ngw_shell_sort": (_I, [_I, _P, _P]),
     "ngw_cvt": (_I, [_I, _P, _P, _I, _P, _I, _P, _P]),
+    "ngw_cvt_device": (_I, [_P, _I, _P, _P, _I, _P, _I, _P, _P]),
     "ngw_dedup_points": (_I, [_I, _P, _P, _P, _P]),
     "ngw_build_coulomb_kernel": (_I, [_P, _I, _I, _P, _P, _I, _D, _D, _P]),
     "ngw_build_fxc_kernel": (_I, [_P, _I, _I, _P, _P, _D, _P, _P]),

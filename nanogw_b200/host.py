@@ -17,15 +17,21 @@ def shell_sort(arr):
     return idx
 
 
-def cvt(grid, rho, init_pts, max_iter=100000):
-    """CVT interpolation points (``shared/cvt.F90``): returns (intp 1-based, points, iterations)."""
+def cvt(grid, rho, init_pts, max_iter=100000, session=None):
+    """CVT interpolation points (``shared/cvt.F90``): returns (intp 1-based, points, iterations).
+    With a ``Session`` the iterations run on its device (``ngw_cvt_device``,
+    bit-identical to the host form)."""
     g = np.ascontiguousarray(grid, dtype=np.float64)
     r = np.ascontiguousarray(rho, dtype=np.float64)
     p = np.array(init_pts, dtype=np.float64, order="C", copy=True)
     n = p.shape[0]
     intp = np.zeros(n, dtype=np.int32)
     it = np.zeros(1, dtype=np.int32)
-    check(lib().ngw_cvt(g.shape[0], _ptr(g), _ptr(r), n, _ptr(p), int(max_iter), _ptr(intp), _ptr(it)))
+    if session is None:
+        check(lib().ngw_cvt(g.shape[0], _ptr(g), _ptr(r), n, _ptr(p), int(max_iter), _ptr(intp), _ptr(it)))
+    else:
+        check(lib().ngw_cvt_device(session._h, g.shape[0], _ptr(g), _ptr(r), n, _ptr(p), int(max_iter),
+                                   _ptr(intp), _ptr(it)))
     return intp, p, int(it[0])
 
 

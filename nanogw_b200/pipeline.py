@@ -1,7 +1,8 @@
 """Setup pipeline: molecule -> ISDF points -> Psi_intp, zeta -> Coulomb kernel M.
 
 Order follows ``SIGMA/sigma.F90:318-738``: CVT point selection on the
-density (``shared/cvt.F90``), density de-duplication (``sigma.F90:377-461``),
+density (``shared/cvt.F90``; iterations on the device, bit-identical to the
+host restatement), density de-duplication (``sigma.F90:377-461``),
 the ISDF fit of the interpolation vectors zeta
 (``shared/isdf_parallel_sym_UltraLowMem.F90:439-667``) and the Coulomb block
 ``M = ntrans/hcub zeta^T v_c zeta`` built on the device
@@ -67,7 +68,8 @@ def build_operator(mol, n_isdf, session, qp_bands=(), seed=0, max_cvt_iter=10000
                    keep_zeta=False, device_fit=True, with_fxc=False):
     grid = mol.grid
     init = synth.cvt_initial_points(grid, n_isdf, seed if seed else mol.seed)
-    intp, _, iters = host.cvt(grid, mol.rho, init, max_cvt_iter)
+    # CVT iterations on the session's device (bit-identical to the host form)
+    intp, _, iters = host.cvt(grid, mol.rho, init, max_cvt_iter, session=session if device_fit else None)
     intp = host.dedup_points(intp, mol.rho)
     mv = max([mol.nval] + [int(b) for b in qp_bands])
     nfft = fft_box_size(mol.rmax, mol.h)

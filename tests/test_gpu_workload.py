@@ -52,3 +52,24 @@ def test_cvt_points_match_oracle(workload):
     intp, _, _ = ocvt.cvt(mol.grid, mol.rho, init)
     intp = ocvt.dedup_points(intp, mol.rho)
     assert np.array_equal(intp, op.intp)
+
+
+def test_device_cvt_bit_identical(workload):
+    """ngw_cvt_device (iterations on the GPU) equals the host ngw_cvt bit for
+    bit at full size: points, indices and iteration count."""
+    import time
+    from nanogw_b200 import host
+    mol, op, qp, poly = workload
+    init = synth.cvt_initial_points(mol.grid, 600, 11)
+    t = time.perf_counter()
+    ih, ph, nh = host.cvt(mol.grid, mol.rho, init)
+    th = time.perf_counter() - t
+    with ngw.Session(0) as s:
+        host.cvt(mol.grid[:5000], mol.rho[:5000], init[:50], 3, session=s)   # warm the kernels
+        t = time.perf_counter()
+        idv, pdv, ndv = host.cvt(mol.grid, mol.rho, init, session=s)
+        td = time.perf_counter() - t
+    print(f"CVT host {th:.3f} s, device {td:.3f} s, {nh} iterations")
+    assert nh == ndv
+    assert np.array_equal(ih, idv)
+    assert np.array_equal(ph, pdv)
