@@ -20,7 +20,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels_core.cu", "gemm_tc.cu", "deflate.cu", "abi.cu", "poisson.cu", "noalloc.cu", "isdf_fit.cu",
-              "exchange.cu", "cvt_device.cu"]
+              "exchange.cu", "cvt_device.cu", "fft3d.cu"]
 CXX_SOURCES = ["host_setup.cpp", "parsec_io.cpp"]
 
 

@@ -12,6 +12,8 @@
 #include <cufft.h>
 
 #include <cmath>
+#include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "ngw_internal.h"
@@ -80,6 +82,19 @@ __global__ void k_mul_coulomb(cufftDoubleComplex *__restrict__ f, const double *
 }
 
 
+int fft_coulomb_boxes(ngw_session *s, int n, int ncol, double *box, double2 *spec, const double *vtab);
+
+// NGW_FFT=cufft selects cuFFT for the 3-D transforms (timing comparison);
+// the default is the library's own FFT.
+static bool use_cufft() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("NGW_FFT");
+    v = (e && std::string(e) == "cufft") ? 1 : 0;
+  }
+  return v == 1;
+}
+
 // v_c * rho for ncol columns (ngrid x ncol, column-major, ld ngrid) on the
 // device: each column packed into the zero-padded FFT box, D2Z, multiplied by
 // the truncated Coulomb kernel, Z2D, unpacked with 1/nfft^3
@@ -105,6 +120,25 @@ int poisson_apply(ngw_session *s, int ngrid, int ncol, const double *drho, const
     }
     const double b = 2.0 * M_PI / ((double)n * h);
     k_coulomb_table<<<1024, 256, 0, s->stream>>>(vtab, n, b, trunc);
+    if (!use_cufft()) {
+      // the library's own batched 3-D FFT (fft3d.cu)
+      const double scale = 1.0 / ((double)n * (double)n * (double)n);
+      int bx = (ngrid + 255) / 256;
+      if (bx > 256) bx = 256;
+      for (int c0 = 0; c0 < ncol && rc == NGW_OK; c0 += batch) {
+        const int nc = std::min(batch, ncol - c0);
+        cudaMemsetAsync(box, 0, bsz * nc * 8, s->stream);
+        k_pack<<<dim3(bx, nc), 256, 0, s->stream>>>(drho + (size_t)c0 * ngrid, ngrid, ngrid, dg, n, box, nc);
+        rc = fft_coulomb_boxes(s, n, nc, box, reinterpret_cast<double2 *>(spec), vtab);
+        if (rc != NGW_OK) break;
+        k_unpack<<<dim3(bx, nc), 256, 0, s->stream>>>(box, ngrid, dg, n, scale, dv + (size_t)c0 * ngrid, ngrid);
+      }
+      if (rc == NGW_OK && cudaGetLastError() != cudaSuccess) {
+        set_error("Poisson kernels failed to launch");
+        rc = NGW_ERR_CUDA;
+      }
+      break;
+    }
     int dims[3] = {n, n, n};
     if (cufftPlanMany(&pf, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, batch) != CUFFT_SUCCESS) {
       set_error("cufftPlanMany D2Z failed");
