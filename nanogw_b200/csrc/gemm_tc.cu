@@ -30,8 +30,12 @@
 #include <utility>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "ngw_internal.h"
 #include "tc_gemm.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace ngw {
 
@@ -83,7 +87,7 @@ constexpr int NTHREADS = 256;
 
 // Epilogue loads for one 16-column chunk, issued before any arithmetic so the
 // global-memory latencies overlap.
-template <int BN, int STAGES, int MINB, bool FUSED>
+template <int BN, int STAGES, int MINB, bool FUSED, bool CRED = false>
 __global__ void __launch_bounds__(NTHREADS, MINB)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
               const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
@@ -203,7 +207,47 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
   const int ch_begin = wg == 0 ? 0 : NCH0;
   const int ch_end = wg == 0 ? NCH0 : NCH;
 
-  if (ep.kind == EPI_SPLIT) {
+  if (CRED && ep.kind == EPI_SPLIT) {
+    // Split-K inside a thread-block cluster (the nsplit CTAs of this tile):
+    // every CTA stages its FP32 partial tile in its own shared memory (the
+    // pipeline stages are free now), then CTA r sums the column slice r over
+    // the cluster's CTAs in split order through distributed shared memory
+    // and writes the split-BF16 result -- the same sums, in the same order,
+    // as k_splitk_reduce, without the global round trip and the extra launch.
+    float *part = reinterpret_cast<float *>(smem);
+    for (int ch = 2 * ch_begin; ch < 2 * ch_end; ++ch) {
+      const int c = ch * 8;
+      float v[8];
+      if (have) {
+        tc::tmem_ld8(trow + c, v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = 0.f;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) part[(c + j) * BM + mloc] = v[j];
+    }
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    const int ns = ga.nsplit;
+    const int rank = (int)cl.block_rank();
+    const int cpr = (BN + ns - 1) / ns;
+    const int c_lo = rank * cpr, c_hi = min(BN, c_lo + cpr);
+    const int row = threadIdx.x % BM;
+    const int mm = m0 + row;
+    for (int c = c_lo + (int)threadIdx.x / BM; c < c_hi; c += NTHREADS / BM) {
+      float acc = 0.f;
+      for (int q = 0; q < ns; ++q) acc += cl.map_shared_rank(part, q)[c * BM + row];
+      const int n = n0 + c;
+      if (mm < ep.Mv && n < ep.Nv) {
+        bf16 hi, lo;
+        split_bf16(acc, hi, lo);
+        ep.out_hi[(size_t)n * ep.ldo + mm] = hi;
+        ep.out_lo[(size_t)n * ep.ldo + mm] = lo;
+      }
+    }
+    cl.sync();   // no CTA leaves while another still reads its shared memory
+  } else if (ep.kind == EPI_SPLIT) {
     const bool partial = ga.nsplit > 1;
     const int tile = blockIdx.y * gridDim.x + blockIdx.x;
     float *wsl = partial ? ep.ws + ((size_t)tile * ga.nsplit + split) * (size_t)(BN * BM) : nullptr;
@@ -630,6 +674,42 @@ static int launch_tc(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUt
   return NGW_OK;
 }
 
+// Cluster-reduced split-K launch: the nsplit CTAs of a tile form one cluster.
+template <int BN, int STAGES, int MINB>
+static int launch_tc_cluster(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
+                             const CUtensorMap &b_lo, int tiles_m, int tiles_n, const GemmArgs &ga,
+                             const EpiParams &ep, int *status, cudaStream_t st) {
+  constexpr size_t smem = (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) * 2 + 1024;
+  static_assert((size_t)BN * BM * 4 <= smem - 1024, "partial tile must fit the stage buffers");
+  static bool attr = false;
+  if (!attr) {
+    NGW_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, MINB, true, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  if (ga.nsplit < 2 || ga.nsplit > 8) {
+    set_error("cluster split-K needs 2..8 splits (got %d)", ga.nsplit);
+    return NGW_ERR_ARG;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(tiles_m, tiles_n, ga.nsplit);
+  cfg.blockDim = dim3(NTHREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attrs[2];
+  attrs[0].id = cudaLaunchAttributeClusterDimension;
+  attrs[0].val.clusterDim.x = 1;
+  attrs[0].val.clusterDim.y = 1;
+  attrs[0].val.clusterDim.z = ga.nsplit;
+  attrs[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attrs[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attrs;
+  cfg.numAttrs = pdl_enabled() ? 2 : 1;
+  NGW_CUDA(cudaLaunchKernelEx(&cfg, k_tc_gemm<BN, STAGES, MINB, true, true>, a_hi, a_lo, b_hi, b_lo, ga, ep,
+                              status));
+  return NGW_OK;
+}
+
 template <int BN, int STAGES>
 static int launch_tc_p(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
                        const CUtensorMap &b_lo, int tiles_m, int tiles_n, const GemmArgs &ga,
@@ -651,6 +731,8 @@ static int launch_tc_p(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const C
 }
 
 static bool has_persistent(int BN) { return BN <= 160; }
+// variants 5 / 6: fused stages with the split-K sum inside a cluster, 1 / 2 CTAs per SM
+static bool is_cluster_var(int var) { return var == 5 || var == 6; }
 static bool has_fused(int BN) { return BN <= 128; }
 static bool has_fused2(int BN) { return BN <= 64; }
 
@@ -702,6 +784,26 @@ static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorM
     }
   }
 #undef NGW_TCF
+#define NGW_TCC(BNV, ST, MB) \
+  return launch_tc_cluster<BNV, ST, MB>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st)
+  if (var == 5) {
+    switch (BN) {
+      case 32: NGW_TCC(32, 5, 1);
+      case 48: NGW_TCC(48, 4, 1);
+      case 64: NGW_TCC(64, 4, 1);
+      case 80: NGW_TCC(80, 4, 1);
+      case 96: NGW_TCC(96, 3, 1);
+      case 128: NGW_TCC(128, 3, 1);
+    }
+  }
+  if (var == 6) {
+    switch (BN) {
+      case 32: NGW_TCC(32, 2, 2);
+      case 48: NGW_TCC(48, 2, 2);
+      case 64: NGW_TCC(64, 2, 2);
+    }
+  }
+#undef NGW_TCC
   if (var == 0) {
     switch (BN) {
       case 32: NGW_TC(32, 8, 1);
@@ -1060,17 +1162,19 @@ static int autotune(ngw_session *s, int nb) {
     if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
     const int waste = round_up(nb, bn) - nb;
     if (waste * 8 > nb && bn != kBNs[0]) continue;     // at most 12.5% padding
-    for (int var = 0; var < 5; ++var) {
+    for (int var = 0; var < 7; ++var) {
       if (var == 1 && !has_shallow(bn)) continue;
       if (var == 2 && !has_persistent(bn)) continue;
-      if (var == 3 && !has_fused(bn)) continue;
-      if (var == 4 && !has_fused2(bn)) continue;
-      c2.push_back({bn, var});
+      if ((var == 3 || var == 5) && !has_fused(bn)) continue;
+      if ((var == 4 || var == 6) && !has_fused2(bn)) continue;
+      if (!is_cluster_var(var)) c2.push_back({bn, var});
       const int tiles = tiles_m1 * ((nb + bn - 1) / bn);
       const int tkb = (var >= 2) ? total_kb1 / 3 : total_kb1;
       for (int sp : {1, 2, 3, 4, 6, 8, 12, 16}) {
         if (sp > 1 && tkb / sp < 3) break;
-        if ((size_t)tiles * sp * bn * BM * sizeof(float) > op->ws_bytes && sp > 1) break;
+        if (is_cluster_var(var) && (sp < 2 || sp > 8)) continue;
+        if (!is_cluster_var(var) && (size_t)tiles * sp * bn * BM * sizeof(float) > op->ws_bytes && sp > 1)
+          break;
         if (tiles * sp > 4 * 148) break;
         c1.push_back({bn, var, sp});
       }
@@ -1246,7 +1350,7 @@ static int run_gemm1(ngw_session *s, int nb) {
   const int tiles_n = (nb + op->BN1 - 1) / op->BN1;
   NGW_TRY(dispatch_tc(op->BN1, op->var1, op->tA1hi, op->tA1lo, op->tShi, op->tSlo, tiles_m, tiles_n,
                       ga, ep, s->d_status, s->stream));
-  if (op->split1 > 1) {
+  if (op->split1 > 1 && !is_cluster_var(op->var1)) {
     const size_t total = (size_t)ep.Mv * nb;
     int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
     NGW_CUDA(launch_pdl(k_splitk_reduce, dim3(blocks), dim3(256), 0, s->stream, (const float *)op->ws,
