@@ -281,11 +281,11 @@ def gemm_scan(local, name, nbs, reps=10):
         s.matvec_isdf(rng.standard_normal((len(cv), 8)))
         for nb in nbs:
             us1, us2 = s.profile_mixed_gemms(nb, reps=reps)
-            M1, N1, K1, BN1, sp1, M2, N2, K2, BN2, v1, v2, _, _ = s.mixed_gemm_shapes(nb)
+            M1, N1, K1, BN1, sp1, M2, N2, K2, BN2, v1, v2, sp2, _ = s.mixed_gemm_shapes(nb)
             f1, f2 = 2.0 * M1 * N1 * K1, 2.0 * M2 * N2 * K2
             out["by_chains"][str(nb)] = {
                 "us_per_launch": [us1, us2],
-                "shapes": [[M1, N1, K1, BN1, sp1, v1], [M2, N2, K2, BN2, 1, v2]],
+                "shapes": [[M1, N1, K1, BN1, sp1, v1], [M2, N2, K2, BN2, sp2, v2]],
                 "algorithmic_tflops": [f1 / us1 / 1e6, f2 / us2 / 1e6],
                 "executed_tflops": [3 * f1 / us1 / 1e6, 3 * f2 / us2 / 1e6],
                 "executed_frac": [3 * f1 / us1 / 1e6 / bf16, 3 * f2 / us2 / 1e6 / bf16],
@@ -496,11 +496,11 @@ def main():
     roof = None
     if args.precision == "mixed":
         us1, us2 = sess.profile_mixed_gemms(nb, reps=50)
-        M1, N1, K1, BN1, sp1, M2, N2, K2, BN2, v1, v2, r1, r2 = sess.mixed_gemm_shapes(nb)
+        M1, N1, K1, BN1, sp1, M2, N2, K2, BN2, v1, v2, sp2, _ = sess.mixed_gemm_shapes(nb)
         flops = 2.0 * M1 * N1 * K1 + 2.0 * M2 * N2 * K2
         achieved = flops / ((us1 + us2) * 1e-6) / 1e12
         hbm, bf16, bf16s, src = load_peaks()
-        tiles = f"{BN1},{v1},{sp1},{BN2},{v2}"
+        tiles = f"{BN1},{v1},{sp1},{BN2},{v2}" + (f",{sp2}" if sp2 > 1 else "")
         # algorithmic bytes of the pair: split-BF16 operands (4 B per element
         # for hi + lo), GEMM1 output, GEMM2's Clenshaw vectors (3 FP32 reads,
         # FP32 + hi/lo writes)
@@ -513,8 +513,8 @@ def main():
                                 "profiled ones",
                 "algorithmic_bytes_per_matvec": alg_bytes,
                 "kernel": "k_tc_gemm (GEMM1 + GEMM2 of one matvec)",
-                "us_per_launch": [us1, us2], "shapes": [[M1, N1, K1, BN1, sp1, v1], [M2, N2, K2, BN2, 1, v2]],
-                "tiles_env": f"{BN1},{v1},{sp1},{BN2},{v2},{r1},{r2}",
+                "us_per_launch": [us1, us2], "shapes": [[M1, N1, K1, BN1, sp1, v1], [M2, N2, K2, BN2, sp2, v2]],
+                "tiles_env": tiles,
                 "peak_source": f"{src} (bf16 dense, burst)",
                 "executed_bf16_frac": 3.0 * achieved / bf16}
 

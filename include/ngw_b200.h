@@ -191,8 +191,8 @@ int ngw_qp_newton_noalloc(int nqp, int nen, const double *sigma_c_ev, const doub
  * session stream.  No reference counterpart: used by the benchmark. */
 int ngw_profile_mixed_gemms(ngw_session *s, int nb, int reps, double *us_gemm1, double *us_gemm2);
 /* shape[13] = {M1, N1, K1, BN1, splitK1, M2, N2, K2, BN2, variant1, variant2,
- * order1, order2} of the two GEMMs (valid sizes, N tile, split-K, kernel
- * variant, tile order: 0 = M tiles fastest, 1 = N tiles fastest). */
+ * splitK2, 0} of the two GEMMs (valid sizes, N tile, split-K, kernel
+ * variant; split-K > 1 of GEMM2 only with the cluster variants 5 / 6). */
 int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape);
 
 /* ---- setup path ---- */

@@ -207,13 +207,14 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
   const int ch_begin = wg == 0 ? 0 : NCH0;
   const int ch_end = wg == 0 ? NCH0 : NCH;
 
-  if (CRED && ep.kind == EPI_SPLIT) {
+  if (CRED) {
     // Split-K inside a thread-block cluster (the nsplit CTAs of this tile):
     // every CTA stages its FP32 partial tile in its own shared memory (the
     // pipeline stages are free now), then CTA r sums the column slice r over
     // the cluster's CTAs in split order through distributed shared memory
-    // and writes the split-BF16 result -- the same sums, in the same order,
-    // as k_splitk_reduce, without the global round trip and the extra launch.
+    // and finishes those columns with the epilogue: the split-BF16 result
+    // (the same sums, in the same order, as k_splitk_reduce, without the
+    // global round trip and the extra launch) or the Clenshaw step.
     float *part = reinterpret_cast<float *>(smem);
     for (int ch = 2 * ch_begin; ch < 2 * ch_end; ++ch) {
       const int c = ch * 8;
@@ -239,11 +240,35 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
       float acc = 0.f;
       for (int q = 0; q < ns; ++q) acc += cl.map_shared_rank(part, q)[c * BM + row];
       const int n = n0 + c;
-      if (mm < ep.Mv && n < ep.Nv) {
+      if (mm >= ep.Mv || n >= ep.Nv) continue;
+      if (ep.kind == EPI_SPLIT) {
         bf16 hi, lo;
         split_bf16(acc, hi, lo);
         ep.out_hi[(size_t)n * ep.ldo + mm] = hi;
         ep.out_lo[(size_t)n * ep.ldo + mm] = lo;
+      } else {
+        // the Clenshaw step of the EPI_CLENSHAW branch below, for one element
+        const double si = ep.s[mm];
+        const double s2 = si * si;
+        const double sc = ep.tda ? 1.0 : si;
+        const size_t o_ = (size_t)n * ep.ldx + mm;
+        const double x = (double)__ldg(ep.x + o_);
+        const double b2v = ep.b2 ? (double)__ldg(ep.b2 + o_) : 0.0;
+        const double vv = ep.v ? (double)__ldg(ep.v + o_) : 0.0;
+        const double y = ep.tda ? (s2 * x + 2.0 * (double)acc) : (s2 * s2 * x + 4.0 * si * (double)acc);
+        const double o = ep.gamma * vv + ep.alpha * (y - ep.c0 * x) - ep.beta * b2v;
+        if (ep.out32) ep.out32[(size_t)n * ep.ldx + mm] = (float)o;
+        if (ep.out64) {
+          double od = o;
+          for (int q = 0; q < ep.kdef; ++q) od += ep.Up[(size_t)q * ep.Mv + mm] * ep.xo[(size_t)n * ep.kdef + q];
+          ep.out64[(size_t)n * ep.ldv + mm] = od;
+        }
+        if (ep.s_hi) {
+          bf16 hi, lo;
+          split_bf16((float)(sc * o), hi, lo);
+          ep.s_hi[(size_t)n * ep.lds + mm] = hi;
+          ep.s_lo[(size_t)n * ep.lds + mm] = lo;
+        }
       }
     }
     cl.sync();   // no CTA leaves while another still reads its shared memory
@@ -926,7 +951,7 @@ struct MixedOperator {
   // chain buffers
   int nb_cap = 0, nb_pad = 0;
   // tile choice (autotuned per chain count): N tile, kernel variant, split-K
-  int BN1 = 128, var1 = 0, split1 = 1, BN2 = 128, var2 = 0;
+  int BN1 = 128, var1 = 0, split1 = 1, BN2 = 128, var2 = 0, split2 = 1;
   int tuned_nb = -1, maps_bn1 = -1, maps_bn2 = -1;
   size_t ws_bytes = 0;
   bf16 *S_hi = nullptr, *S_lo = nullptr, *T_hi = nullptr, *T_lo = nullptr;
@@ -976,7 +1001,7 @@ void extern_mixed_tune(ngw_session *s, int *tune) {
   MixedOperator *op = s->mixed;
   tune[0] = op->BN1 * 16 + op->var1;
   tune[1] = op->split1;
-  tune[2] = op->BN2 * 16 + op->var2;
+  tune[2] = (op->BN2 * 16 + op->var2) * 16 + op->split2;
   tune[3] = op->nb_cap;
 }
 
@@ -1153,7 +1178,7 @@ static int autotune(ngw_session *s, int nb) {
     return NGW_OK;
   };
   struct C1 { int bn, var, sp; };
-  struct C2 { int bn, var; };
+  struct C2 { int bn, var, sp; };
   std::vector<C1> c1;
   std::vector<C2> c2;
   const int total_kb1 = 3 * (op->cv_pad / BK);
@@ -1167,7 +1192,13 @@ static int autotune(ngw_session *s, int nb) {
       if (var == 2 && !has_persistent(bn)) continue;
       if ((var == 3 || var == 5) && !has_fused(bn)) continue;
       if ((var == 4 || var == 6) && !has_fused2(bn)) continue;
-      if (!is_cluster_var(var)) c2.push_back({bn, var});
+      if (!is_cluster_var(var)) {
+        c2.push_back({bn, var, 1});
+      } else {
+        const int kb2 = op->mu_k / BK;   // GEMM2 k-blocks (fused stages)
+        for (int sp : {2, 3, 4})
+          if (kb2 / sp >= 2) c2.push_back({bn, var, sp});
+      }
       const int tiles = tiles_m1 * ((nb + bn - 1) / bn);
       const int tkb = (var >= 2) ? total_kb1 / 3 : total_kb1;
       for (int sp : {1, 2, 3, 4, 6, 8, 12, 16}) {
@@ -1186,6 +1217,7 @@ static int autotune(ngw_session *s, int nb) {
     if (c.var == 0 && c.bn == 64) fix2 = c;
   op->BN2 = fix2.bn;
   op->var2 = fix2.var;
+  op->split2 = fix2.sp;
   float best1 = 1e30f, best2 = 1e30f;
   C1 b1 = c1.front();
   for (const C1 &c : c1) {
@@ -1210,12 +1242,13 @@ static int autotune(ngw_session *s, int nb) {
   for (const C2 &c : c2) {
     op->BN2 = c.bn;
     op->var2 = c.var;
+    op->split2 = c.sp;
     NGW_TRY(encode_chain_maps(op, op->BN1, c.bn));
     float ms = 0;
     NGW_TRY(time_pair(&ms));
     if (verbose)
-      fprintf(stderr, "tune gemm2 bn=%d var=%d (+gemm1 %d/%d/%d): %.2f us\n", c.bn, c.var, op->BN1,
-              op->var1, op->split1, 1e3f * ms);
+      fprintf(stderr, "tune gemm2 bn=%d var=%d split=%d (+gemm1 %d/%d/%d): %.2f us\n", c.bn, c.var, c.sp,
+              op->BN1, op->var1, op->split1, 1e3f * ms);
     if (ms < best2) {
       best2 = ms;
       b2 = c;
@@ -1225,6 +1258,7 @@ static int autotune(ngw_session *s, int nb) {
   cudaEventDestroy(e1);
   op->BN2 = b2.bn;
   op->var2 = b2.var;
+  op->split2 = b2.sp;
   NGW_TRY(encode_chain_maps(op, op->BN1, op->BN2));
   // buffers used for timing held scratch values: clear the operands again
   NGW_CUDA(cudaMemsetAsync(op->T_hi, 0, (size_t)op->nb_pad * op->mu_k * sizeof(bf16), s->stream));
@@ -1245,7 +1279,7 @@ struct TuneKey {
   }
 };
 struct TuneVal {
-  int bn1, var1, split1, bn2, var2;
+  int bn1, var1, split1, bn2, var2, split2;
 };
 static std::mutex g_tune_mu;
 static std::map<TuneKey, TuneVal> g_tune;
@@ -1295,18 +1329,20 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
     op->BN2 = bn2;
     op->var1 = op->var2 = 0;
     op->split1 = split1 > 0 ? split1 : 1;
+    op->split2 = 1;
     op->tuned_nb = -2;
     return encode_chain_maps(op, bn1, bn2);
   }
-  // NGW_TILES="bn1,var1,split1,bn2,var2" fixes the tiles (reproducible profiling)
+  // NGW_TILES="bn1,var1,split1,bn2,var2[,split2]" fixes the tiles (reproducible profiling)
   if (const char *env = getenv("NGW_TILES")) {
-    int t[5];
-    if (sscanf(env, "%d,%d,%d,%d,%d", &t[0], &t[1], &t[2], &t[3], &t[4]) == 5) {
+    int t[6] = {0, 0, 0, 0, 0, 1};
+    if (sscanf(env, "%d,%d,%d,%d,%d,%d", &t[0], &t[1], &t[2], &t[3], &t[4], &t[5]) >= 5) {
       op->BN1 = t[0];
       op->var1 = t[1];
       op->split1 = t[2];
       op->BN2 = t[3];
       op->var2 = t[4];
+      op->split2 = t[5] > 0 ? t[5] : 1;
       op->tuned_nb = nb;
       return encode_chain_maps(op, t[0], t[3]);
     }
@@ -1321,11 +1357,12 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
       op->split1 = it->second.split1;
       op->BN2 = it->second.bn2;
       op->var2 = it->second.var2;
+      op->split2 = it->second.split2;
       op->tuned_nb = nb;
       return encode_chain_maps(op, op->BN1, op->BN2);
     }
     NGW_TRY(autotune(s, nb));
-    g_tune[key] = TuneVal{op->BN1, op->var1, op->split1, op->BN2, op->var2};
+    g_tune[key] = TuneVal{op->BN1, op->var1, op->split1, op->BN2, op->var2, op->split2};
   }
   return NGW_OK;
 }
@@ -1367,7 +1404,7 @@ static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, co
   GemmArgs ga;
   ga.num_kb = op->mu_k / BK;
   ga.nseg = 3;
-  ga.nsplit = 1;
+  ga.nsplit = is_cluster_var(op->var2) ? op->split2 : 1;
   EpiParams ep;
   std::memset(&ep, 0, sizeof(ep));
   ep.kind = EPI_CLENSHAW;
@@ -1529,6 +1566,6 @@ extern "C" int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape) {
   shape[4] = op->split1;
   shape[5] = op->ncv; shape[6] = nb; shape[7] = op->n_isdf + op->kdef; shape[8] = op->BN2;
   shape[9] = op->var1; shape[10] = op->var2;
-  shape[11] = 0; shape[12] = 0;
+  shape[11] = op->split2; shape[12] = 0;
   return NGW_OK;
 }

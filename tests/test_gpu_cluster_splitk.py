@@ -41,3 +41,38 @@ def test_cluster_split_k_bit_identical(tmp_path, plain, cluster):
     a = _run(tmp_path, plain)
     b = _run(tmp_path, cluster)
     assert np.array_equal(a, b)
+
+
+QP_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, {root!r})
+import nanogw_b200 as ngw
+from tests._system import make_small_system
+from oracle import sigma as OS
+S = make_small_system()
+qp = np.array([S.nval - 1, S.nval, S.nval + 1, S.nval + 2], dtype=np.int32)
+nen, deltae, ecuts, niter = 81, 2.0, 0.02, 24
+with ngw.Session(0, "mixed") as s:
+    s.set_isdf(S.psi_intp, S.M)
+    s.set_pairs(S.cvpair, S.sqrtR)
+    got = s.calculate_sigma_lanczos(S.e1, S.nval, qp, nen, deltae, ecuts, niter, S.poly)
+    sh = s.mixed_gemm_shapes(len(qp) * S.nmem)
+refs = np.stack([OS.sigma_c_state(S.psi_intp, S.M, S.e1, S.nval, int(m), nen, deltae, ecuts, niter, S.poly)
+                 for m in qp], axis=1)
+sx, vx = np.full(len(qp), -0.4), np.full(len(qp), -0.6)
+er = OS.qp_energies(refs.T, S.e1, S.e1, qp, deltae, sx, vx, xacc_ev=1e-7)
+eg = OS.qp_energies(got.T, S.e1, S.e1, qp, deltae, sx, vx, xacc_ev=1e-7)
+np.save({out!r}, np.array([abs(a[0] - b[0]) * 1e3 for a, b in zip(eg, er)] + [sh[10], sh[11]]))
+"""
+
+
+def test_cluster_split_k_gemm2_within_1mev(tmp_path):
+    """GEMM2 with its K split across a 2-CTA cluster (Clenshaw epilogue on
+    the cluster-summed tile): QP energies within 1 meV of the FP64 oracle."""
+    out = str(tmp_path / "qp.npy")
+    env = dict(os.environ, NGW_TILES="64,3,2,64,6,2")
+    subprocess.run([sys.executable, "-c", QP_SCRIPT.format(root=ROOT, out=out)], env=env, check=True,
+                   timeout=600)
+    r = np.load(out)
+    assert r[-2] == 6 and r[-1] == 2          # the pinned GEMM2 variant and split ran
+    assert np.all(r[:-2] < 1.0), r
