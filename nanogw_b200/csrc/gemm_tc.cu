@@ -85,8 +85,22 @@ __device__ __forceinline__ void split_bf16(float v, bf16 &hi, bf16 &lo) {
 
 constexpr int NTHREADS = 256;
 
-// Epilogue loads for one 16-column chunk, issued before any arithmetic so the
-// global-memory latencies overlap.
+// Clenshaw operands b_{k+1}, b_{k+2} and v of row m for the 8 columns from
+// nbase (zero past the valid rows / columns and for absent vectors).
+__device__ __forceinline__ void clenshaw_operands(const EpiParams &ep, bool mv, int m, int nbase, float *x,
+                                                  float *b2, float *v) {
+  const int nj = mv ? min(8, ep.Nv - nbase) : 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const size_t o = (size_t)(nbase + j) * ep.ldx + m;
+    x[j] = (j < nj) ? __ldg(ep.x + o) : 0.f;
+    b2[j] = (j < nj && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
+    v[j] = (j < nj && ep.v) ? __ldg(ep.v + o) : 0.f;
+  }
+}
+
+// One 128 x BN output tile per CTA (split-K slice blockIdx.z): warp 0 issues
+// the TMA loads, warp 1 the MMAs into TMEM, then all 8 warps run the epilogue.
 template <int BN, int STAGES, int MINB, bool FUSED, bool CRED = false>
 __global__ void __launch_bounds__(NTHREADS, MINB)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
@@ -198,14 +212,25 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
 
   // ---- epilogue: 8 warps; warp w reads TMEM lanes 32*(w%4).., warpgroup w/4
   // takes one half of the 16-column chunks ----
-  const bool have = tc::mbar_wait(tc::smem_u32(&done_bar), 0, status) && nkb > 0;
-  tc::tc_fence_after();
   const int wl = warp & 3, wg = warp >> 2;
   const int mloc = wl * 32 + lane;
   const int m = m0 + mloc;
   const uint32_t trow = tmem_d + ((uint32_t)(wl * 32) << 16);
   const int ch_begin = wg == 0 ? 0 : NCH0;
   const int ch_end = wg == 0 ? NCH0 : NCH;
+  // The Clenshaw operands (b_{k+1}, b_{k+2}, v) do not depend on the product:
+  // the first 8-column chunk of them is loaded while the MMAs still run, and
+  // every later chunk one iteration ahead of its use.
+  const bool clenshaw = !CRED && ep.kind == EPI_CLENSHAW;
+  const bool mv = m < ep.Mv;
+  float px[8], pb[8], pv[8];
+  double si = 0.0;
+  if (clenshaw) {
+    if (mv) si = ep.s[m];
+    clenshaw_operands(ep, mv, m, n0 + 16 * ch_begin, px, pb, pv);
+  }
+  const bool have = tc::mbar_wait(tc::smem_u32(&done_bar), 0, status) && nkb > 0;
+  tc::tc_fence_after();
 
   if (CRED) {
     // Split-K inside a thread-block cluster (the nsplit CTAs of this tile):
@@ -305,8 +330,6 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     // EPI_CLENSHAW: y = R^2 x + 4 R^1/2 z (TDA: R x + 2 z);
     // out = gamma v + alpha (y - c0 x) - beta b2; split((R^1/2 or 1) out).
     // 8-column chunks keep the register count low enough for 2 CTAs per SM.
-    const bool mv = m < ep.Mv;
-    const double si = mv ? ep.s[m] : 0.0;
     const double s2 = si * si;
     const double sc = ep.tda ? 1.0 : si;
     for (int ch = 2 * ch_begin; ch < 2 * ch_end; ++ch) {
@@ -318,26 +341,24 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
 #pragma unroll
         for (int j = 0; j < 8; ++j) z[j] = 0.f;
       }
+      float xv[8], b2v[8], vf[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        xv[j] = px[j];
+        b2v[j] = pb[j];
+        vf[j] = pv[j];
+      }
+      if (ch + 1 < 2 * ch_end) clenshaw_operands(ep, mv, m, n0 + c + 8, px, pb, pv);
       if (!mv) continue;
       const int nbase = n0 + c;
       const int nj = min(8, ep.Nv - nbase);
-      if (nj <= 0) continue;
-      float xv[8], b2v[8];
-      double vv[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const size_t o = (size_t)(nbase + j) * ep.ldx + m;
-        xv[j] = (j < nj) ? __ldg(ep.x + o) : 0.f;
-        b2v[j] = (j < nj && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
-        vv[j] = (j < nj && ep.v) ? (double)__ldg(ep.v + o) : 0.0;
-      }
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         if (j >= nj) break;
         const int n = nbase + j;
         const double x = (double)xv[j];
         const double y = ep.tda ? (s2 * x + 2.0 * (double)z[j]) : (s2 * s2 * x + 4.0 * si * (double)z[j]);
-        const double o = ep.gamma * vv[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
+        const double o = ep.gamma * (double)vf[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
         if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = (float)o;
         if (ep.out64) {
           double od = o;
