@@ -99,6 +99,20 @@ __device__ __forceinline__ void clenshaw_operands(const EpiParams &ep, bool mv, 
   }
 }
 
+// The same for the 4 columns n, n + step, ... below n_end.
+__device__ __forceinline__ void clenshaw_operands4(const EpiParams &ep, bool mv, int m, int n, int step, int n_end,
+                                                   float *x, float *b2, float *v) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int nn = n + j * step;
+    const bool ok = mv && nn < n_end && nn < ep.Nv;
+    const size_t o = (size_t)nn * ep.ldx + m;
+    x[j] = ok ? __ldg(ep.x + o) : 0.f;
+    b2[j] = (ok && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
+    v[j] = (ok && ep.v) ? __ldg(ep.v + o) : 0.f;
+  }
+}
+
 // One 128 x BN output tile per CTA (split-K slice blockIdx.z): warp 0 issues
 // the TMA loads, warp 1 the MMAs into TMEM, then all 8 warps run the epilogue.
 template <int BN, int STAGES, int MINB, bool FUSED, bool CRED = false>
@@ -229,6 +243,26 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     if (mv) si = ep.s[m];
     clenshaw_operands(ep, mv, m, n0 + 16 * ch_begin, px, pb, pv);
   }
+  // Cluster split-K: this CTA finishes the tile columns [c_lo, c_hi); thread
+  // row crow takes c_first, c_first + cstep, ... in groups of 4, the Clenshaw
+  // operands of each group loaded one group ahead (the first before the wait).
+  int c_lo = 0, c_hi = 0;
+  if constexpr (CRED) {
+    const int cpr = (BN + ga.nsplit - 1) / ga.nsplit;
+    c_lo = (int)cg::this_cluster().block_rank() * cpr;
+    c_hi = min(BN, c_lo + cpr);
+  }
+  constexpr int cstep = NTHREADS / BM;
+  const int crow = threadIdx.x % BM;
+  const int c_first = c_lo + (int)threadIdx.x / BM;
+  const int mm = m0 + crow;
+  const bool cred_clenshaw = CRED && ep.kind == EPI_CLENSHAW;
+  float qx[4], qb[4], qv[4];
+  double csi = 0.0;
+  if (cred_clenshaw) {
+    if (mm < ep.Mv) csi = ep.s[mm];
+    clenshaw_operands4(ep, mm < ep.Mv, mm, n0 + c_first, cstep, n0 + c_hi, qx, qb, qv);
+  }
   const bool have = tc::mbar_wait(tc::smem_u32(&done_bar), 0, status) && nkb > 0;
   tc::tc_fence_after();
 
@@ -256,43 +290,48 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     cg::cluster_group cl = cg::this_cluster();
     cl.sync();
     const int ns = ga.nsplit;
-    const int rank = (int)cl.block_rank();
-    const int cpr = (BN + ns - 1) / ns;
-    const int c_lo = rank * cpr, c_hi = min(BN, c_lo + cpr);
-    const int row = threadIdx.x % BM;
-    const int mm = m0 + row;
-    for (int c = c_lo + (int)threadIdx.x / BM; c < c_hi; c += NTHREADS / BM) {
-      float acc = 0.f;
-      for (int q = 0; q < ns; ++q) acc += cl.map_shared_rank(part, q)[c * BM + row];
-      const int n = n0 + c;
-      if (mm >= ep.Mv || n >= ep.Nv) continue;
-      if (ep.kind == EPI_SPLIT) {
-        bf16 hi, lo;
-        split_bf16(acc, hi, lo);
-        ep.out_hi[(size_t)n * ep.ldo + mm] = hi;
-        ep.out_lo[(size_t)n * ep.ldo + mm] = lo;
-      } else {
-        // the Clenshaw step of the EPI_CLENSHAW branch below, for one element
-        const double si = ep.s[mm];
-        const double s2 = si * si;
-        const double sc = ep.tda ? 1.0 : si;
-        const size_t o_ = (size_t)n * ep.ldx + mm;
-        const double x = (double)__ldg(ep.x + o_);
-        const double b2v = ep.b2 ? (double)__ldg(ep.b2 + o_) : 0.0;
-        const double vv = ep.v ? (double)__ldg(ep.v + o_) : 0.0;
-        const double y = ep.tda ? (s2 * x + 2.0 * (double)acc) : (s2 * s2 * x + 4.0 * si * (double)acc);
-        const double o = ep.gamma * vv + ep.alpha * (y - ep.c0 * x) - ep.beta * b2v;
-        if (ep.out32) ep.out32[(size_t)n * ep.ldx + mm] = (float)o;
-        if (ep.out64) {
-          double od = o;
-          for (int q = 0; q < ep.kdef; ++q) od += ep.Up[(size_t)q * ep.Mv + mm] * ep.xo[(size_t)n * ep.kdef + q];
-          ep.out64[(size_t)n * ep.ldv + mm] = od;
-        }
-        if (ep.s_hi) {
+    const double s2 = csi * csi;
+    const double sc = ep.tda ? 1.0 : csi;
+    for (int c = c_first; c < c_hi; c += 4 * cstep) {
+      float cx[4], cb[4], cv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        cx[j] = qx[j];
+        cb[j] = qb[j];
+        cv[j] = qv[j];
+      }
+      if (cred_clenshaw && c + 4 * cstep < c_hi)
+        clenshaw_operands4(ep, mm < ep.Mv, mm, n0 + c + 4 * cstep, cstep, n0 + c_hi, qx, qb, qv);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int cc = c + j * cstep;
+        if (cc >= c_hi) break;
+        float acc = 0.f;
+        for (int q = 0; q < ns; ++q) acc += cl.map_shared_rank(part, q)[cc * BM + crow];
+        const int n = n0 + cc;
+        if (mm >= ep.Mv || n >= ep.Nv) continue;
+        if (ep.kind == EPI_SPLIT) {
           bf16 hi, lo;
-          split_bf16((float)(sc * o), hi, lo);
-          ep.s_hi[(size_t)n * ep.lds + mm] = hi;
-          ep.s_lo[(size_t)n * ep.lds + mm] = lo;
+          split_bf16(acc, hi, lo);
+          ep.out_hi[(size_t)n * ep.ldo + mm] = hi;
+          ep.out_lo[(size_t)n * ep.ldo + mm] = lo;
+        } else {
+          // the Clenshaw step of the EPI_CLENSHAW branch below, for one element
+          const double x = (double)cx[j];
+          const double y = ep.tda ? (s2 * x + 2.0 * (double)acc) : (s2 * s2 * x + 4.0 * csi * (double)acc);
+          const double o = ep.gamma * (double)cv[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)cb[j];
+          if (ep.out32) ep.out32[(size_t)n * ep.ldx + mm] = (float)o;
+          if (ep.out64) {
+            double od = o;
+            for (int q = 0; q < ep.kdef; ++q) od += ep.Up[(size_t)q * ep.Mv + mm] * ep.xo[(size_t)n * ep.kdef + q];
+            ep.out64[(size_t)n * ep.ldv + mm] = od;
+          }
+          if (ep.s_hi) {
+            bf16 hi, lo;
+            split_bf16((float)(sc * o), hi, lo);
+            ep.s_hi[(size_t)n * ep.lds + mm] = hi;
+            ep.s_lo[(size_t)n * ep.lds + mm] = lo;
+          }
         }
       }
     }
@@ -515,11 +554,19 @@ __global__ void __launch_bounds__(PTHREADS, 1)
       const int tm = w % tiles_m, tn = (w / tiles_m) % tiles_n, sp = w / (tiles_m * tiles_n);
       const int kb0 = sp * kb_per, kb1 = min(total_kb, kb0 + kb_per);
       const int buf = t & 1;
+      const int m0 = tm * BM, n0 = tn * BN;
+      const int m = m0 + mloc;
+      // Clenshaw operands of the first chunk, loaded before the accumulator is ready
+      const bool mv = m < ep.Mv;
+      float px[8], pb[8], pv[8];
+      double si = 0.0;
+      if (ep.kind == EPI_CLENSHAW) {
+        if (mv) si = ep.s[m];
+        clenshaw_operands(ep, mv, m, n0 + 8 * ch_begin, px, pb, pv);
+      }
       const bool have = tc::mbar_wait(tc::smem_u32(&accf_bar[buf]), (t >> 1) & 1, status) && kb1 > kb0;
       tc::tc_fence_after();
       const uint32_t trow = tmem_base + buf * ACC_STRIDE + ((uint32_t)(wl * 32) << 16);
-      const int m0 = tm * BM, n0 = tn * BN;
-      const int m = m0 + mloc;
       if (ep.kind == EPI_SPLIT) {
         const bool partial = ga.nsplit > 1;
         const int tile = tn * tiles_m + tm;
@@ -550,8 +597,6 @@ __global__ void __launch_bounds__(PTHREADS, 1)
           }
         }
       } else {
-        const bool mv = m < ep.Mv;
-        const double si = mv ? ep.s[m] : 0.0;
         const double s2 = si * si;
         const double sc = ep.tda ? 1.0 : si;
         for (int ch = ch_begin; ch < ch_end; ++ch) {
@@ -563,26 +608,24 @@ __global__ void __launch_bounds__(PTHREADS, 1)
 #pragma unroll
             for (int j = 0; j < 8; ++j) z[j] = 0.f;
           }
+          float xv[8], b2v[8], vf[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            xv[j] = px[j];
+            b2v[j] = pb[j];
+            vf[j] = pv[j];
+          }
+          if (ch + 1 < ch_end) clenshaw_operands(ep, mv, m, n0 + c + 8, px, pb, pv);
           if (!mv) continue;
           const int nbase = n0 + c;
           const int nj = min(8, ep.Nv - nbase);
-          if (nj <= 0) continue;
-          float xv[8], b2v[8];
-          double vv[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const size_t o = (size_t)(nbase + j) * ep.ldx + m;
-            xv[j] = (j < nj) ? __ldg(ep.x + o) : 0.f;
-            b2v[j] = (j < nj && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
-            vv[j] = (j < nj && ep.v) ? (double)__ldg(ep.v + o) : 0.0;
-          }
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             if (j >= nj) break;
             const int n = nbase + j;
             const double x = (double)xv[j];
             const double y = ep.tda ? (s2 * x + 2.0 * (double)z[j]) : (s2 * s2 * x + 4.0 * si * (double)z[j]);
-            const double o = ep.gamma * vv[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
+            const double o = ep.gamma * (double)vf[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
             if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = (float)o;
             if (ep.out64) {
               double od = o;

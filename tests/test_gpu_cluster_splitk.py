@@ -1,7 +1,9 @@
-"""Split-K of GEMM1 summed inside a thread-block cluster (variants 5 and 6)
+"""GEMM tile forms pinned per process with NGW_TILES.
+
+Split-K of GEMM1 summed inside a thread-block cluster (variants 5 and 6)
 gives bit-identical Sigma_c to the same tiles with the separate reduction
 kernel (variants 3 and 4): the same partial tiles summed in the same order.
-Tiles are pinned per process with NGW_TILES."""
+Every GEMM2 form with the Clenshaw epilogue stays within 1 meV of the oracle."""
 import os
 import subprocess
 import sys
@@ -66,13 +68,36 @@ np.save({out!r}, np.array([abs(a[0] - b[0]) * 1e3 for a, b in zip(eg, er)] + [sh
 """
 
 
+def _qp(tmp_path, tiles):
+    out = str(tmp_path / ("qp_" + tiles.replace(",", "_") + ".npy"))
+    env = dict(os.environ, NGW_TILES=tiles)
+    subprocess.run([sys.executable, "-c", QP_SCRIPT.format(root=ROOT, out=out)], env=env, check=True,
+                   timeout=600)
+    return np.load(out)
+
+
 def test_cluster_split_k_gemm2_within_1mev(tmp_path):
     """GEMM2 with its K split across a 2-CTA cluster (Clenshaw epilogue on
     the cluster-summed tile): QP energies within 1 meV of the FP64 oracle."""
-    out = str(tmp_path / "qp.npy")
-    env = dict(os.environ, NGW_TILES="64,3,2,64,6,2")
-    subprocess.run([sys.executable, "-c", QP_SCRIPT.format(root=ROOT, out=out)], env=env, check=True,
-                   timeout=600)
-    r = np.load(out)
+    r = _qp(tmp_path, "64,3,2,64,6,2")
     assert r[-2] == 6 and r[-1] == 2          # the pinned GEMM2 variant and split ran
     assert np.all(r[:-2] < 1.0), r
+
+
+@pytest.mark.parametrize("gemm2", ["64,2", "64,3", "64,4", "32,4", "128,3", "32,6,4"])
+def test_gemm2_variants_within_1mev(tmp_path, gemm2):
+    """Every GEMM2 kernel form with the Clenshaw epilogue (persistent, fused
+    one or two CTAs per SM, cluster split-K) keeps the QP energies within
+    1 meV of the FP64 oracle."""
+    r = _qp(tmp_path, "64,3,2," + gemm2)
+    parts = [int(x) for x in gemm2.split(",")]
+    assert r[-2] == parts[1] and r[-1] == (parts[2] if len(parts) > 2 else 1)
+    assert np.all(r[:-2] < 1.0), r
+
+
+def test_gemm2_occupancy_forms_bit_identical(tmp_path):
+    """The fused GEMM2 at one and at two CTAs per SM runs the same MMAs and
+    the same epilogue arithmetic: identical Sigma_c."""
+    a = _run(tmp_path, "64,3,2,64,3")
+    b = _run(tmp_path, "64,3,2,64,4")
+    assert np.array_equal(a, b)
