@@ -195,6 +195,16 @@ int ngw_profile_mixed_gemms(ngw_session *s, int nb, int reps, double *us_gemm1, 
  * variant; split-K > 1 of GEMM2 only with the cluster variants 5 / 6). */
 int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape);
 
+/* Top Ritz pairs of the Casida operator (tamm_d 0: C = R^2 + 4 R^1/2 K R^1/2,
+ * 1: the TDA matrix A) from an FP64 Lanczos run of msteps steps with full
+ * reorthogonalisation started from a fixed pseudo-random vector: the kmax
+ * largest Ritz values (descending, Ry^2 or Ry) to vals and their residual
+ * bounds |beta_m y_m| to res; *count = number written (<= min(kmax, msteps)).
+ * These are the eigenpairs the mixed-precision path deflates.  No reference
+ * counterpart (the reference's Lanczos has no deflation). */
+int ngw_operator_eigenpairs(ngw_session *s, int tamm_d, int msteps, int kmax, double *vals,
+                            double *res, int *count);
+
 /* ---- setup path ---- */
 /* Shell sort (ascending) returning a 1-based permutation. Host code. */
 int ngw_shell_sort(int n, const double *arr, int *idx);

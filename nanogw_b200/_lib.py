@@ -48,6 +48,7 @@ SIGNATURES = {
     "ngw_qp_newton_noalloc": (_I, [_I, _I, _P, _P, _P, _D, _P, _P, _D, _P, _P, _P, _P]),
     "ngw_profile_mixed_gemms": (_I, [_P, _I, _I, _P, _P]),
     "ngw_mixed_gemm_shapes": (_I, [_P, _I, _P]),
+    "ngw_operator_eigenpairs": (_I, [_P, _I, _I, _I, _P, _P, _P]),
     "ngw_shell_sort": (_I, [_I, _P, _P]),
     "ngw_cvt": (_I, [_I, _P, _P, _I, _P, _I, _P, _P]),
     "ngw_cvt_device": (_I, [_P, _I, _P, _P, _I, _P, _I, _P, _P]),

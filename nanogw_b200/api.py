@@ -219,6 +219,17 @@ class Session:
         check(lib().ngw_mixed_gemm_shapes(self._h, int(nb), _p(sh)))
         return [int(x) for x in sh]
 
+    def operator_eigenpairs(self, kmax=16, msteps=240, tamm_d=False):
+        """Largest Ritz values of the Casida operator (C, or A with TDA) and
+        their residual bounds from an FP64 Lanczos run of msteps steps with
+        full reorthogonalisation (the pairs the mixed path deflates)."""
+        vals = np.zeros(kmax)
+        res = np.zeros(kmax)
+        cnt = ctypes.c_int(0)
+        check(lib().ngw_operator_eigenpairs(self._h, int(bool(tamm_d)), int(msteps), int(kmax), _p(vals),
+                                            _p(res), ctypes.byref(cnt)))
+        return vals[: cnt.value].copy(), res[: cnt.value].copy()
+
     def build_fxc_kernel(self, zeta, rho, h, return_fxc=False):
         """M_xc = zeta^T (f_xc * zeta) / hcub with the LDA f_xc of rho (Ry)."""
         zt = _f64(zeta)

@@ -1106,3 +1106,24 @@ int ngw_qp_newton(ngw_session *s, int nqp, int nen, const double *sigma_c_ev, co
 }
 
 }  // extern "C"
+
+extern "C" int ngw_operator_eigenpairs(ngw_session *s, int tamm_d, int msteps, int kmax, double *vals,
+                                       double *res, int *count) {
+  using namespace ngw;
+  if (!vals || !res || !count || msteps < 1 || kmax < 1 || (tamm_d != 0 && tamm_d != 1)) {
+    set_error("ngw_operator_eigenpairs: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  NGW_TRY(need_op(s));   // the FP64 pair products are gathered on first use
+  NGW_TRY(compute_top_eigs(s, tamm_d, kmax, msteps));
+  const int k = std::min(kmax, (int)s->eig_vals.size());
+  for (int i = 0; i < k; ++i) {
+    vals[i] = s->eig_vals[i];
+    res[i] = s->eig_res[i];
+  }
+  *count = k;
+  // the mixed-precision plan recomputes its own eigenpairs (and operator)
+  s->eig_tda = -1;
+  s->mixed_dirty = true;
+  return NGW_OK;
+}

@@ -15,6 +15,7 @@
 // plain Horner form.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <numeric>
 #include <vector>
 
@@ -34,6 +35,243 @@ __global__ void k_lanczos_next(const double *__restrict__ w, const double *__res
   const double inv = b > 0.0 ? 1.0 / b : 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x)
     vnext[i] = w[i] * inv;
+}
+
+// ---------------------------------------------------------------------------
+// The whole FP64 Lanczos run with full reorthogonalisation as ONE persistent
+// kernel (one CTA per SM, launched cooperatively so all CTAs are resident).
+// Per step j, between bounded grid barriers:
+//   A  v_j = w / beta_j (v_0 given); t1 partials = C (R^1/2 or 1) v_j, the
+//      columns of C split into CA ranges
+//   B  t2 partials = M t1 (t1 summed from its partials, M's columns in KB ranges)
+//   C  w = R^2 v_j + 4 R^1/2 C^T t2   (TDA: R v_j + 2 C^T t2), a warp per column
+//   D  twice: h = V_{0..j}^T w (a CTA per column of V), then w -= V_{0..j} h
+//      (groups of 32 rows, the k-sum split over the CTA's 8 warps); the
+//      second update also forms the CTA partials of ||w||^2
+// Every partition and summation order is fixed by the grid size, so the run
+// is deterministic.  Values written inside the kernel are read through L2
+// (ld.global.cg): L1 is not coherent between SMs.
+constexpr int EIG_NT = 256;
+
+struct EigLanczosArgs {
+  const double *C, *M, *sR;
+  int n, ncv, m, tda;
+  int RG, CA, KB;          // row groups of NT rows, column ranges of C, column ranges of M
+  double *V;               // (ncv, m + 1): column 0 given
+  double *pA, *pB;         // (CA, n) and (KB, n) partial products
+  double *w, *h, *pE;      // (ncv), (m + 1), (grid)
+  double *alpha, *beta;    // (m), (m + 1)
+  unsigned *bar;           // barrier arrival counter, zero at launch
+  int *status;
+};
+
+// Grid barrier with a bounded wait: returns false (and sets *status = 2) when
+// the other CTAs have not all arrived within ~1 s of clock cycles.  The
+// counter only grows (zero at launch): thread 0 of each CTA adds 1 after a
+// gpu-scope fence (the CTA's writes, ordered by the CTA barrier, are released
+// with it) and polls with acquire loads until the count reaches its epoch
+// times the grid size.  No atomic result and no second release are waited for.
+__device__ __forceinline__ bool eig_grid_sync(unsigned *cnt, unsigned &target, int *status, int *sh_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    target += gridDim.x;
+    asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
+    const long long t0 = clock64();
+    while (true) {
+      unsigned c;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(cnt) : "memory");
+      if ((int)(c - target) >= 0) break;
+      if (clock64() - t0 > (1LL << 31)) {
+        atomicExch(status, 2);
+        ok = 0;
+        break;
+      }
+    }
+    *sh_ok = ok;
+  }
+  __syncthreads();
+  return *sh_ok != 0;
+}
+
+// Sum over the CTA in a fixed order (value valid in every thread).
+__device__ __forceinline__ double eig_block_sum(double v, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int q = 0; q < EIG_NT / 32; ++q) t += red[q];
+  return t;
+}
+
+// Sum of p[0..G) by one warp in a fixed order (value valid in lane 0).
+__device__ __forceinline__ double eig_warp_sum_grid(const double *p, int G) {
+  double q = 0.0;
+  for (int g = (int)threadIdx.x; g < G; g += 32) q += __ldcg(p + g);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) q += __shfl_down_sync(0xffffffffu, q, o);
+  return q;
+}
+
+__global__ void __launch_bounds__(EIG_NT, 1) k_eig_lanczos(EigLanczosArgs a) {
+  extern __shared__ double sh[];   // max(n, m + 1) doubles
+  __shared__ double red[EIG_NT / 32];
+  __shared__ double xs[EIG_NT];                  // a chunk of (R^1/2 or 1) v_j
+  __shared__ double part[EIG_NT / 32][32];       // per-warp partial row sums
+  __shared__ double bcast;
+  __shared__ int sh_ok;
+  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+  const int n = a.n, ncv = a.ncv;
+  const int gwarp = b * (EIG_NT / 32) + (tid >> 5), nwarps = G * (EIG_NT / 32);
+  const int cpc = (ncv + a.CA - 1) / a.CA;   // columns of C per A item
+  const int kpc = (n + a.KB - 1) / a.KB;     // columns of M per B item
+  unsigned target = 0;                       // barrier epoch x grid size (thread 0)
+  for (int j = 0; j < a.m; ++j) {
+    double *vj = a.V + (size_t)j * ncv;
+    // ---- A: v_j, t1 partials ----
+    double inv = 1.0;
+    if (j > 0) {
+      if (tid < 32) {
+        const double q = eig_warp_sum_grid(a.pE, G);
+        if (tid == 0) bcast = sqrt(q);
+      }
+      __syncthreads();
+      const double bj = bcast;
+      inv = bj > 0.0 ? 1.0 / bj : 0.0;
+      if (b == 0 && tid == 0) a.beta[j] = bj;
+    }
+    for (int it = b; it < a.RG * a.CA; it += G) {
+      const int rg = it % a.RG, ca = it / a.RG;
+      const int i = rg * EIG_NT + tid;
+      const int c0 = ca * cpc, c1 = min(ncv, c0 + cpc);
+      double acc = 0.0;
+      for (int cb = c0; cb < c1; cb += EIG_NT) {
+        const int nc = min(EIG_NT, c1 - cb);
+        __syncthreads();   // xs of the previous chunk consumed
+        if (tid < nc) {
+          const int c = cb + tid;
+          double x;
+          if (j > 0) {
+            x = __ldcg(a.w + c) * inv;
+            if (rg == 0) vj[c] = x;
+          } else {
+            x = __ldcg(vj + c);
+          }
+          xs[tid] = a.tda ? x : __ldg(a.sR + c) * x;
+        }
+        __syncthreads();
+        if (i < n) {
+          const double *cp = a.C + (size_t)cb * n + i;
+#pragma unroll 8
+          for (int c = 0; c < nc; ++c) acc += __ldg(cp + (size_t)c * n) * xs[c];
+        }
+      }
+      if (i < n) a.pA[(size_t)ca * n + i] = acc;
+    }
+    if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+    // ---- B: t2 partials ----
+    for (int it = b; it < a.RG * a.KB; it += G) {
+      const int rg = it % a.RG, kb = it / a.RG;
+      const int k0 = kb * kpc, k1 = min(n, k0 + kpc);
+      __syncthreads();
+      for (int k = k0 + tid; k < k1; k += EIG_NT) {
+        double t = 0.0;
+#pragma unroll 16
+        for (int q = 0; q < a.CA; ++q) t += __ldcg(a.pA + (size_t)q * n + k);
+        sh[k - k0] = t;
+      }
+      __syncthreads();
+      const int i = rg * EIG_NT + tid;
+      if (i < n) {
+        double acc = 0.0;
+#pragma unroll 16
+        for (int k = k0; k < k1; ++k) acc += __ldg(a.M + (size_t)k * n + i) * sh[k - k0];
+        a.pB[(size_t)kb * n + i] = acc;
+      }
+    }
+    if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+    // ---- C: w = H v_j ----
+    for (int i = tid; i < n; i += EIG_NT) {
+      double t = 0.0;
+#pragma unroll 8
+      for (int q = 0; q < a.KB; ++q) t += __ldcg(a.pB + (size_t)q * n + i);
+      sh[i] = t;
+    }
+    __syncthreads();
+    for (int c = gwarp; c < ncv; c += nwarps) {
+      const double *cc = a.C + (size_t)c * n;
+      double z = 0.0;
+#pragma unroll 16
+      for (int i = lane; i < n; i += 32) z += __ldg(cc + i) * sh[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+      if (lane == 0) {
+        const double si = __ldg(a.sR + c);
+        const double x = __ldcg(vj + c);
+        double r;
+        if (a.tda) {
+          r = (si * si) * x;
+          r = r + 2.0 * z;
+        } else {
+          r = (si * si * si) * (si * x);
+          r = r + 4.0 * si * z;
+        }
+        a.w[c] = r;
+      }
+    }
+    if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+    // ---- D: two passes of classical Gram-Schmidt ----
+    for (int p = 0; p < 2; ++p) {
+      for (int k = b; k <= j; k += G) {
+        const double *vk = a.V + (size_t)k * ncv;
+        double d = 0.0;
+        for (int r = tid; r < ncv; r += EIG_NT) d += __ldcg(vk + r) * __ldcg(a.w + r);
+        d = eig_block_sum(d, red);
+        if (tid == 0) {
+          a.h[k] = d;
+          if (p == 0 && k == j) a.alpha[j] = d;
+        }
+      }
+      if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+      for (int k = tid; k <= j; k += EIG_NT) sh[k] = __ldcg(a.h + k);
+      __syncthreads();
+      // w -= V h over groups of 32 rows: warp wq sums k = wq, wq + 8, ...;
+      // warp 0 adds the 8 warp sums in order and updates the rows
+      double q = 0.0;
+      const int wq = tid >> 5;
+      for (int g = b; g * 32 < ncv; g += G) {
+        const int r = g * 32 + lane;
+        double sacc = 0.0;
+        if (r < ncv) {
+#pragma unroll 16
+          for (int k = wq; k <= j; k += EIG_NT / 32) sacc += __ldcg(a.V + (size_t)k * ncv + r) * sh[k];
+        }
+        part[wq][lane] = sacc;
+        __syncthreads();
+        if (wq == 0 && r < ncv) {
+          double t = 0.0;
+#pragma unroll
+          for (int u = 0; u < EIG_NT / 32; ++u) t += part[u][lane];
+          const double wn = __ldcg(a.w + r) - t;
+          a.w[r] = wn;
+          q += wn * wn;
+        }
+        __syncthreads();
+      }
+      if (p == 1) {
+        q = eig_block_sum(q, red);
+        if (tid == 0) a.pE[b] = q;
+      }
+      if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+    }
+  }
+  if (b == 0 && tid < 32) {
+    const double q = eig_warp_sum_grid(a.pE, G);
+    if (tid == 0) a.beta[a.m] = sqrt(q);
+  }
 }
 
 // Eigen-decomposition of the small symmetric Lanczos matrix T (column-major
@@ -94,6 +332,102 @@ static int sym_eig(ngw_session *s, const std::vector<double> &T, int n, std::vec
   return rc;
 }
 
+// The Lanczos loop of compute_top_eigs as one persistent kernel.  *done is
+// false (and nothing is launched) when the operator does not fit its shared
+// memory plan or the device cannot hold one CTA per SM.
+static int eig_lanczos_persistent(ngw_session *s, int tamm_d, int m, double *V, double *dalpha,
+                                  double *dbeta, bool *done) {
+  *done = false;
+  const int n = s->n_isdf, ncv = s->ncv;
+  const size_t smem = (size_t)std::max(n, m + 1) * 8;
+  if (smem > 200 * 1024) return NGW_OK;
+  int dev = 0, nsm = 0, coop = 0, per_sm = 0;
+  NGW_CUDA(cudaGetDevice(&dev));
+  NGW_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  NGW_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  if (!coop) return NGW_OK;
+  NGW_CUDA(cudaFuncSetAttribute(k_eig_lanczos, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  NGW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_eig_lanczos, EIG_NT, smem));
+  if (per_sm < 1) return NGW_OK;
+  EigLanczosArgs a{};
+  a.C = s->d_C;
+  a.M = s->d_M;
+  a.sR = s->d_sqrtR;
+  a.n = n;
+  a.ncv = ncv;
+  a.m = m;
+  a.tda = tamm_d;
+  const int G = nsm;
+  a.RG = (n + EIG_NT - 1) / EIG_NT;
+  a.CA = std::max(1, G / a.RG);
+  a.KB = std::max(1, std::min(8, G / a.RG));
+  a.V = V;
+  a.alpha = dalpha;
+  a.beta = dbeta;
+  const size_t bytes = ((size_t)a.CA * n + (size_t)a.KB * n + ncv + (m + 1) + G) * 8 + 64;
+  char *ws = nullptr;
+  NGW_TRY(dalloc(s, (void **)&ws, bytes));
+  a.pA = reinterpret_cast<double *>(ws);
+  a.pB = a.pA + (size_t)a.CA * n;
+  a.w = a.pB + (size_t)a.KB * n;
+  a.h = a.w + ncv;
+  a.pE = a.h + (m + 1);
+  a.bar = reinterpret_cast<unsigned *>(a.pE + G);
+  a.status = reinterpret_cast<int *>(a.bar + 2);
+  int rc = NGW_OK;
+  int hstatus = 0;
+  void *args[] = {&a};
+  if (cudaMemsetAsync(a.bar, 0, 16, s->stream) != cudaSuccess ||
+      cudaLaunchCooperativeKernel((const void *)k_eig_lanczos, dim3(G), dim3(EIG_NT), args, smem, s->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(&hstatus, a.status, 4, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess) {
+    set_error("eigenpair Lanczos: persistent kernel failed (%s)", cudaGetErrorString(cudaGetLastError()));
+    rc = NGW_ERR_CUDA;
+  } else if (hstatus != 0) {
+    set_error("eigenpair Lanczos: a grid barrier timed out");
+    rc = NGW_ERR_TIMEOUT;
+  }
+  dfree(s, ws, bytes);
+  *done = rc == NGW_OK;
+  return rc;
+}
+
+// The same loop from cuBLAS level-2 calls (operators whose ISDF dimension
+// exceeds the persistent kernel's shared memory, or NGW_EIG_BLAS set).
+static int eig_lanczos_blas(ngw_session *s, int tamm_d, int m, double *V, double *w, double *hs, double *h,
+                            double *dalpha, double *dbeta) {
+  const int ncv = s->ncv;
+  const double one = 1.0, mone = -1.0, zero = 0.0;
+  const int nblk = std::min(148 * 4, (ncv + 255) / 256);
+  int rc = NGW_OK;
+  for (int j = 0; j < m && rc == NGW_OK; ++j) {
+    double *vj = V + (size_t)j * ncv;
+    launch_scale_rows(s->d_sqrtR, vj, ncv, hs, ncv, ncv, 1, tamm_d, s->stream);
+    if ((rc = matvec_f64_dev_pub(s, 1, hs, w, tamm_d)) != NGW_OK) break;
+    // two passes of classical Gram-Schmidt against all previous vectors
+    for (int pass = 0; pass < 2 && rc == NGW_OK; ++pass) {
+      if (cublasDgemv(s->cublas, CUBLAS_OP_T, ncv, j + 1, &one, V, ncv, w, 1, &zero, h, 1) ||
+          (pass == 0 && cudaMemcpyAsync(dalpha + j, h + j, 8, cudaMemcpyDeviceToDevice, s->stream)) ||
+          cublasDgemv(s->cublas, CUBLAS_OP_N, ncv, j + 1, &mone, V, ncv, h, 1, &one, w, 1)) {
+        set_error("eigenpair Lanczos: Gram-Schmidt step failed");
+        rc = NGW_ERR_CUDA;
+      }
+    }
+    if (rc != NGW_OK) break;
+    cublasSetPointerMode(s->cublas, CUBLAS_POINTER_MODE_DEVICE);
+    const cublasStatus_t st2 = cublasDnrm2(s->cublas, ncv, w, 1, dbeta + j + 1);
+    cublasSetPointerMode(s->cublas, CUBLAS_POINTER_MODE_HOST);
+    if (st2 != CUBLAS_STATUS_SUCCESS) {
+      set_error("eigenpair Lanczos: norm failed");
+      rc = NGW_ERR_CUDA;
+      break;
+    }
+    k_lanczos_next<<<nblk, 256, 0, s->stream>>>(w, dbeta + j + 1, ncv, V + (size_t)(j + 1) * ncv);
+  }
+  return rc;
+}
+
 // FP64 Lanczos with full (twice-applied) reorthogonalisation on one vector.
 // Fills s->eig_* with Ritz values (descending), residual bounds and the Ritz
 // vectors of the top kmax pairs (device, ncv x kmax).
@@ -123,33 +457,14 @@ int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
   NGW_TRY(dalloc(s, (void **)&dab, (size_t)(2 * m + 1) * 8));
   NGW_CUDA(cudaMemsetAsync(dab, 0, (size_t)(2 * m + 1) * 8, s->stream));
   double *dalpha = dab, *dbeta = dab + m;
-  const double one = 1.0, mone = -1.0, zero = 0.0;
-  const int nblk = std::min(148 * 4, (ncv + 255) / 256);
   int rc = NGW_OK;
-  for (int j = 0; j < m && rc == NGW_OK; ++j) {
-    double *vj = V + (size_t)j * ncv;
-    launch_scale_rows(s->d_sqrtR, vj, ncv, hs, ncv, ncv, 1, tamm_d, s->stream);
-    if ((rc = matvec_f64_dev_pub(s, 1, hs, w, tamm_d)) != NGW_OK) break;
-    // two passes of classical Gram-Schmidt against all previous vectors
-    for (int pass = 0; pass < 2 && rc == NGW_OK; ++pass) {
-      if (cublasDgemv(s->cublas, CUBLAS_OP_T, ncv, j + 1, &one, V, ncv, w, 1, &zero, h, 1) ||
-          (pass == 0 && cudaMemcpyAsync(dalpha + j, h + j, 8, cudaMemcpyDeviceToDevice, s->stream)) ||
-          cublasDgemv(s->cublas, CUBLAS_OP_N, ncv, j + 1, &mone, V, ncv, h, 1, &one, w, 1)) {
-        set_error("eigenpair Lanczos: Gram-Schmidt step failed");
-        rc = NGW_ERR_CUDA;
-      }
-    }
-    if (rc != NGW_OK) break;
-    cublasSetPointerMode(s->cublas, CUBLAS_POINTER_MODE_DEVICE);
-    const cublasStatus_t st2 = cublasDnrm2(s->cublas, ncv, w, 1, dbeta + j + 1);
-    cublasSetPointerMode(s->cublas, CUBLAS_POINTER_MODE_HOST);
-    if (st2 != CUBLAS_STATUS_SUCCESS) {
-      set_error("eigenpair Lanczos: norm failed");
-      rc = NGW_ERR_CUDA;
-      break;
-    }
-    k_lanczos_next<<<nblk, 256, 0, s->stream>>>(w, dbeta + j + 1, ncv, V + (size_t)(j + 1) * ncv);
+  bool done = false;
+  if (!getenv("NGW_EIG_BLAS")) {
+    const int rcp = eig_lanczos_persistent(s, tamm_d, m, V, dalpha, dbeta, &done);
+    if (rcp != NGW_OK) rc = rcp;
   }
+  if (!done && rc == NGW_OK) rc = eig_lanczos_blas(s, tamm_d, m, V, w, hs, h, dalpha, dbeta);
+  const double one = 1.0, zero = 0.0;
   std::vector<double> alpha(m), beta(m + 1, 0.0);
   if (rc == NGW_OK &&
       (cudaGetLastError() != cudaSuccess ||
