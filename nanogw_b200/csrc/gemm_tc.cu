@@ -113,6 +113,52 @@ __device__ __forceinline__ void clenshaw_operands4(const EpiParams &ep, bool mv,
   }
 }
 
+// Clenshaw step in FP32.  The row coefficient (R^2 or R) - c0 is formed in
+// FP64 once per row and rounded once, so the combine
+//   out = gamma v + alpha ((R^2 - c0) x + 4 R^1/2 z) - beta b2   (TDA: R, 2)
+// has no cancellation of R^2 x against c0 x and runs as three FP32 FMAs; its
+// inputs and outputs are FP32 (or split BF16) anyway, so FP64 here only cost
+// issue slots (FP64 and conversion pipes are narrow on this part).
+struct ClenCoef {
+  float d;             // (R^2 or R) - c0
+  float kz;            // 4 R^1/2 or 2
+  float sc;            // R^1/2 or 1: scale of the split output
+  float ga, al, mbe;   // gamma, alpha, -beta
+};
+
+__device__ __forceinline__ ClenCoef clen_coef(const EpiParams &ep, double si) {
+  const double s2 = si * si;
+  ClenCoef k;
+  k.d = (float)((ep.tda ? s2 : s2 * s2) - ep.c0);
+  k.kz = (float)(ep.tda ? 2.0 : 4.0 * si);
+  k.sc = (float)(ep.tda ? 1.0 : si);
+  k.ga = (float)ep.gamma;
+  k.al = (float)ep.alpha;
+  k.mbe = (float)(-ep.beta);
+  return k;
+}
+
+__device__ __forceinline__ float clen_out(const ClenCoef &k, float x, float z, float v, float b2) {
+  const float t = fmaf(k.d, x, k.kz * z);
+  return fmaf(k.al, t, fmaf(k.ga, v, k.mbe * b2));
+}
+
+// Stores of one Clenshaw output element (row m, chain n).
+__device__ __forceinline__ void clen_store(const EpiParams &ep, const ClenCoef &k, int m, int n, float o) {
+  if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = o;
+  if (ep.out64) {
+    double od = (double)o;
+    for (int q = 0; q < ep.kdef; ++q) od += ep.Up[(size_t)q * ep.Mv + m] * ep.xo[(size_t)n * ep.kdef + q];
+    ep.out64[(size_t)n * ep.ldv + m] = od;
+  }
+  if (ep.s_hi) {
+    bf16 hi, lo;
+    split_bf16(k.sc * o, hi, lo);
+    ep.s_hi[(size_t)n * ep.lds + m] = hi;
+    ep.s_lo[(size_t)n * ep.lds + m] = lo;
+  }
+}
+
 // One 128 x BN output tile per CTA (split-K slice blockIdx.z): warp 0 issues
 // the TMA loads, warp 1 the MMAs into TMEM, then all 8 warps run the epilogue.
 template <int BN, int STAGES, int MINB, bool FUSED, bool CRED = false>
@@ -290,8 +336,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     cg::cluster_group cl = cg::this_cluster();
     cl.sync();
     const int ns = ga.nsplit;
-    const double s2 = csi * csi;
-    const double sc = ep.tda ? 1.0 : csi;
+    const ClenCoef kc = clen_coef(ep, csi);
     for (int c = c_first; c < c_hi; c += 4 * cstep) {
       float cx[4], cb[4], cv[4];
 #pragma unroll
@@ -317,21 +362,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
           ep.out_lo[(size_t)n * ep.ldo + mm] = lo;
         } else {
           // the Clenshaw step of the EPI_CLENSHAW branch below, for one element
-          const double x = (double)cx[j];
-          const double y = ep.tda ? (s2 * x + 2.0 * (double)acc) : (s2 * s2 * x + 4.0 * csi * (double)acc);
-          const double o = ep.gamma * (double)cv[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)cb[j];
-          if (ep.out32) ep.out32[(size_t)n * ep.ldx + mm] = (float)o;
-          if (ep.out64) {
-            double od = o;
-            for (int q = 0; q < ep.kdef; ++q) od += ep.Up[(size_t)q * ep.Mv + mm] * ep.xo[(size_t)n * ep.kdef + q];
-            ep.out64[(size_t)n * ep.ldv + mm] = od;
-          }
-          if (ep.s_hi) {
-            bf16 hi, lo;
-            split_bf16((float)(sc * o), hi, lo);
-            ep.s_hi[(size_t)n * ep.lds + mm] = hi;
-            ep.s_lo[(size_t)n * ep.lds + mm] = lo;
-          }
+          clen_store(ep, kc, mm, n, clen_out(kc, cx[j], acc, cv[j], cb[j]));
         }
       }
     }
@@ -366,11 +397,10 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
       }
     }
   } else {
-    // EPI_CLENSHAW: y = R^2 x + 4 R^1/2 z (TDA: R x + 2 z);
-    // out = gamma v + alpha (y - c0 x) - beta b2; split((R^1/2 or 1) out).
+    // EPI_CLENSHAW: out = gamma v + alpha ((R^2 - c0) x + 4 R^1/2 z) - beta b2
+    // (TDA: R - c0, 2 z) in FP32 (clen_out); split((R^1/2 or 1) out).
     // 8-column chunks keep the register count low enough for 2 CTAs per SM.
-    const double s2 = si * si;
-    const double sc = ep.tda ? 1.0 : si;
+    const ClenCoef kc = clen_coef(ep, si);
     for (int ch = 2 * ch_begin; ch < 2 * ch_end; ++ch) {
       const int c = ch * 8;
       float z[8];
@@ -394,23 +424,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         if (j >= nj) break;
-        const int n = nbase + j;
-        const double x = (double)xv[j];
-        const double y = ep.tda ? (s2 * x + 2.0 * (double)z[j]) : (s2 * s2 * x + 4.0 * si * (double)z[j]);
-        const double o = ep.gamma * (double)vf[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
-        if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = (float)o;
-        if (ep.out64) {
-          double od = o;
-          for (int q = 0; q < ep.kdef; ++q)
-            od += ep.Up[(size_t)q * ep.Mv + m] * ep.xo[(size_t)n * ep.kdef + q];
-          ep.out64[(size_t)n * ep.ldv + m] = od;
-        }
-        if (ep.s_hi) {
-          bf16 hi, lo;
-          split_bf16((float)(sc * o), hi, lo);
-          ep.s_hi[(size_t)n * ep.lds + m] = hi;
-          ep.s_lo[(size_t)n * ep.lds + m] = lo;
-        }
+        clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]));
       }
     }
   }
@@ -597,8 +611,7 @@ __global__ void __launch_bounds__(PTHREADS, 1)
           }
         }
       } else {
-        const double s2 = si * si;
-        const double sc = ep.tda ? 1.0 : si;
+        const ClenCoef kc = clen_coef(ep, si);
         for (int ch = ch_begin; ch < ch_end; ++ch) {
           const int c = ch * 8;
           float z[8];
@@ -622,23 +635,7 @@ __global__ void __launch_bounds__(PTHREADS, 1)
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             if (j >= nj) break;
-            const int n = nbase + j;
-            const double x = (double)xv[j];
-            const double y = ep.tda ? (s2 * x + 2.0 * (double)z[j]) : (s2 * s2 * x + 4.0 * si * (double)z[j]);
-            const double o = ep.gamma * (double)vf[j] + ep.alpha * (y - ep.c0 * x) - ep.beta * (double)b2v[j];
-            if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = (float)o;
-            if (ep.out64) {
-              double od = o;
-              for (int q = 0; q < ep.kdef; ++q)
-                od += ep.Up[(size_t)q * ep.Mv + m] * ep.xo[(size_t)n * ep.kdef + q];
-              ep.out64[(size_t)n * ep.ldv + m] = od;
-            }
-            if (ep.s_hi) {
-              bf16 hi, lo;
-              split_bf16((float)(sc * o), hi, lo);
-              ep.s_hi[(size_t)n * ep.lds + m] = hi;
-              ep.s_lo[(size_t)n * ep.lds + m] = lo;
-            }
+            clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]));
           }
         }
       }
