@@ -36,12 +36,29 @@ void set_error(const char *fmt, ...) {
   va_end(ap);
 }
 
-int dalloc(ngw_session *s, void **p, size_t bytes) {
+// Device memory comes from the device's stream-ordered pool on the session
+// stream (its release threshold is raised at session creation, so freed
+// blocks stay cached for the next request).  A free is ordered after the
+// work already queued on the session stream and, unlike cudaFree, does not
+// wait for the whole device: sessions serving requests side by side do not
+// stall each other.  An allocation waits for the session stream, so the
+// block is ready for use on any stream when pool_alloc returns.
+cudaError_t pool_alloc(ngw_session *s, void **p, size_t bytes) {
   *p = nullptr;
+  cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  return e;
+}
+
+void pool_free(ngw_session *s, void *p) {
+  if (p) cudaFreeAsync(p, s->stream);
+}
+
+int dalloc(ngw_session *s, void **p, size_t bytes) {
   if (bytes == 0) bytes = 16;
-  cudaError_t e = cudaMalloc(p, bytes);
+  cudaError_t e = pool_alloc(s, p, bytes);
   if (e != cudaSuccess) {
-    set_error("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     *p = nullptr;
     return NGW_ERR_OOM;
   }
@@ -51,7 +68,7 @@ int dalloc(ngw_session *s, void **p, size_t bytes) {
 
 void dfree(ngw_session *s, void *p, size_t bytes) {
   if (!p) return;
-  cudaFree(p);
+  pool_free(s, p);
   s->bytes -= bytes;
 }
 
@@ -660,6 +677,13 @@ int ngw_session_create(int device, ngw_session **out) {
     return NGW_ERR_ARG;
   }
   NGW_CUDA(cudaSetDevice(device));
+  {
+    // keep freed pool memory cached in this process (not returned at each sync)
+    cudaMemPool_t pool;
+    uint64_t keep = UINT64_MAX;
+    NGW_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    NGW_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   ngw_session *s = new ngw_session();
   s->device = device;
   cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
@@ -695,15 +719,16 @@ void ngw_session_destroy(ngw_session *s) {
   if (!s) return;
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
-  mixed_free(s);
   for (auto &g : s->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
-  for (auto &b : s->scratch)
-    if (b.p) cudaFree(b.p);
-  if (s->cublas_ws) cudaFree(s->cublas_ws);
-  void *ptrs[] = {s->d_psi, s->d_M, s->d_Mxc, s->d_cvpair, s->d_sqrtR, s->d_C, s->d_status, s->eig_U};
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
+  if (s->stream) {   // frees are queued on the session stream, before it goes
+    mixed_free(s);
+    for (auto &b : s->scratch) pool_free(s, b.p);
+    pool_free(s, s->cublas_ws);
+    void *ptrs[] = {s->d_psi, s->d_M, s->d_Mxc, s->d_cvpair, s->d_sqrtR, s->d_C, s->d_status, s->eig_U};
+    for (void *p : ptrs) pool_free(s, p);
+    cudaStreamSynchronize(s->stream);
+  }
   if (s->cublas) cublasDestroy(s->cublas);
   if (s->cusolver) cusolverDnDestroy((cusolverDnHandle_t)s->cusolver);
   if (s->stream) cudaStreamDestroy(s->stream);

@@ -201,25 +201,40 @@ __global__ void __launch_bounds__(EIG_NT, 1) k_eig_lanczos(EigLanczosArgs a) {
       sh[i] = t;
     }
     __syncthreads();
-    for (int c = gwarp; c < ncv; c += nwarps) {
+    // two columns per warp pass (c and c + nwarps): two independent load chains
+    for (int c = gwarp; c < ncv; c += 2 * nwarps) {
+      const int c2 = c + nwarps;
+      const bool two = c2 < ncv;
       const double *cc = a.C + (size_t)c * n;
-      double z = 0.0;
-#pragma unroll 16
-      for (int i = lane; i < n; i += 32) z += __ldg(cc + i) * sh[i];
+      const double *cc2 = a.C + (size_t)(two ? c2 : c) * n;
+      double z = 0.0, z2 = 0.0;
+#pragma unroll 8
+      for (int i = lane; i < n; i += 32) {
+        const double t = sh[i];
+        z += __ldg(cc + i) * t;
+        z2 += __ldg(cc2 + i) * t;
+      }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+      for (int o = 16; o > 0; o >>= 1) {
+        z += __shfl_xor_sync(0xffffffffu, z, o);
+        z2 += __shfl_xor_sync(0xffffffffu, z2, o);
+      }
       if (lane == 0) {
-        const double si = __ldg(a.sR + c);
-        const double x = __ldcg(vj + c);
-        double r;
-        if (a.tda) {
-          r = (si * si) * x;
-          r = r + 2.0 * z;
-        } else {
-          r = (si * si * si) * (si * x);
-          r = r + 4.0 * si * z;
+        for (int u = 0; u < (two ? 2 : 1); ++u) {
+          const int cu = u ? c2 : c;
+          const double zu = u ? z2 : z;
+          const double si = __ldg(a.sR + cu);
+          const double x = __ldcg(vj + cu);
+          double r;
+          if (a.tda) {
+            r = (si * si) * x;
+            r = r + 2.0 * zu;
+          } else {
+            r = (si * si * si) * (si * x);
+            r = r + 4.0 * si * zu;
+          }
+          a.w[cu] = r;
         }
-        a.w[c] = r;
       }
     }
     if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
@@ -359,7 +374,8 @@ static int eig_lanczos_persistent(ngw_session *s, int tamm_d, int m, double *V, 
   a.tda = tamm_d;
   const int G = nsm;
   a.RG = (n + EIG_NT - 1) / EIG_NT;
-  a.CA = std::max(1, G / a.RG);
+  // about 64 columns of C per A item: more ranges only lengthen B's sums
+  a.CA = std::max(1, std::min(G / a.RG, (ncv + 63) / 64));
   a.KB = std::max(1, std::min(8, G / a.RG));
   a.V = V;
   a.alpha = dalpha;

@@ -1030,7 +1030,7 @@ static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
   void *ptrs[] = {op->S_hi, op->S_lo, op->T_hi, op->T_lo, op->bb[0], op->bb[1], op->bb[2],
                   op->ws,   op->vperp, op->xo};
   for (void *p : ptrs)
-    if (p) cudaFree(p);
+    pool_free(s, p);
   op->S_hi = op->S_lo = op->T_hi = op->T_lo = nullptr;
   op->bb[0] = op->bb[1] = op->bb[2] = nullptr;
   op->ws = nullptr;
@@ -1049,7 +1049,7 @@ void mixed_free(ngw_session *s) {
   free_chain_buffers(s, op);
   void *ptrs[] = {op->A1_hi, op->A1_lo, op->A3_hi, op->A3_lo, op->Up};
   for (void *p : ptrs)
-    if (p) cudaFree(p);
+    pool_free(s, p);
   s->bytes -= op->op_bytes;
   delete op;
   s->mixed = nullptr;
@@ -1092,13 +1092,13 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
     op->mu_pad = round_up(s->n_isdf + kdef, BM);
     op->mu_k = round_up(s->n_isdf + kdef, BK);
     op->cv_pad = round_up(s->ncv, BM);
-    NGW_CUDA(cudaMalloc(&op->A1_hi, a1));
-    NGW_CUDA(cudaMalloc(&op->A1_lo, a1));
-    NGW_CUDA(cudaMalloc(&op->A3_hi, a3));
-    NGW_CUDA(cudaMalloc(&op->A3_lo, a3));
+    NGW_CUDA(pool_alloc(s, (void **)&op->A1_hi, a1));
+    NGW_CUDA(pool_alloc(s, (void **)&op->A1_lo, a1));
+    NGW_CUDA(pool_alloc(s, (void **)&op->A3_hi, a3));
+    NGW_CUDA(pool_alloc(s, (void **)&op->A3_lo, a3));
     op->op_bytes = 2 * (a1 + a3);
     if (kdef > 0) {
-      NGW_CUDA(cudaMalloc(&op->Up, (size_t)s->ncv * kdef * 8));
+      NGW_CUDA(pool_alloc(s, (void **)&op->Up, (size_t)s->ncv * kdef * 8));
       op->op_bytes += (size_t)s->ncv * kdef * 8;
     }
     s->bytes += op->op_bytes;
@@ -1118,8 +1118,8 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
   if (kdef > 0) {
     // G = (C U) / s  in FP64: C applied to the Ritz vectors with the FP64 matvec
     double *hs = nullptr, *CU = nullptr;
-    NGW_CUDA(cudaMalloc(&hs, (size_t)s->ncv * kdef * 8));
-    NGW_CUDA(cudaMalloc(&CU, (size_t)s->ncv * kdef * 8));
+    NGW_CUDA(pool_alloc(s, (void **)&hs, (size_t)s->ncv * kdef * 8));
+    NGW_CUDA(pool_alloc(s, (void **)&CU, (size_t)s->ncv * kdef * 8));
     launch_scale_rows(s->d_sqrtR, s->eig_U, s->ncv, hs, s->ncv, s->ncv, kdef, tda, st);
     int rc = matvec_f64_dev_pub(s, kdef, hs, CU, tda);
     if (rc == NGW_OK) {
@@ -1130,19 +1130,19 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
                                                           s->n_isdf);
     }
     NGW_CUDA(cudaStreamSynchronize(st));
-    cudaFree(hs);
-    cudaFree(CU);
+    pool_free(s, hs);
+    pool_free(s, CU);
     NGW_TRY(rc);
     NGW_CUDA(cudaGetLastError());
   }
   // D = M * C (FP64, cuBLAS), then split into A3[cv][mu] with the -U/(4s) columns
   double *D = nullptr;
-  NGW_CUDA(cudaMalloc(&D, (size_t)s->n_isdf * s->ncv * sizeof(double)));
+  NGW_CUDA(pool_alloc(s, (void **)&D, (size_t)s->n_isdf * s->ncv * sizeof(double)));
   cublasStatus_t cst = cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, s->n_isdf, s->ncv,
                                    s->n_isdf, &one, s->d_M, s->n_isdf, s->d_C, s->n_isdf, &zero,
                                    D, s->n_isdf);
   if (cst != CUBLAS_STATUS_SUCCESS) {
-    cudaFree(D);
+    pool_free(s, D);
     set_error("cublasDgemm (M*C) failed %d", (int)cst);
     return NGW_ERR_CUDA;
   }
@@ -1153,7 +1153,7 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
     NGW_CUDA(cudaGetLastError());
   }
   NGW_CUDA(cudaStreamSynchronize(st));
-  cudaFree(D);
+  pool_free(s, D);
   NGW_TRY(make_tmap(&op->tA1hi, op->A1_hi, op->mu_pad, op->cv_pad, BM));
   NGW_TRY(make_tmap(&op->tA1lo, op->A1_lo, op->mu_pad, op->cv_pad, BM));
   NGW_TRY(make_tmap(&op->tA3hi, op->A3_hi, op->cv_pad, op->mu_k, BM));
@@ -1365,14 +1365,14 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
     const size_t xbytes = (size_t)nbp * std::max(op->kdef, 1) * sizeof(double);
     // split-K partials: enough for 16 splits of the smallest tile grid
     const size_t wsbytes = (size_t)(op->mu_pad / BM) * ((nbp + 63) / 64) * 16 * 64 * BM * sizeof(float);
-    NGW_CUDA(cudaMalloc(&op->S_hi, sbytes));
-    NGW_CUDA(cudaMalloc(&op->S_lo, sbytes));
-    NGW_CUDA(cudaMalloc(&op->T_hi, tbytes));
-    NGW_CUDA(cudaMalloc(&op->T_lo, tbytes));
-    for (int i = 0; i < 3; ++i) NGW_CUDA(cudaMalloc(&op->bb[i], bbytes));
-    NGW_CUDA(cudaMalloc(&op->vperp, vbytes));
-    NGW_CUDA(cudaMalloc(&op->xo, xbytes));
-    NGW_CUDA(cudaMalloc(&op->ws, wsbytes));
+    NGW_CUDA(pool_alloc(s, (void **)&op->S_hi, sbytes));
+    NGW_CUDA(pool_alloc(s, (void **)&op->S_lo, sbytes));
+    NGW_CUDA(pool_alloc(s, (void **)&op->T_hi, tbytes));
+    NGW_CUDA(pool_alloc(s, (void **)&op->T_lo, tbytes));
+    for (int i = 0; i < 3; ++i) NGW_CUDA(pool_alloc(s, (void **)&op->bb[i], bbytes));
+    NGW_CUDA(pool_alloc(s, (void **)&op->vperp, vbytes));
+    NGW_CUDA(pool_alloc(s, (void **)&op->xo, xbytes));
+    NGW_CUDA(pool_alloc(s, (void **)&op->ws, wsbytes));
     op->ws_bytes = wsbytes;
     op->buf_bytes = 2 * sbytes + 2 * tbytes + 3 * bbytes + vbytes + xbytes + wsbytes;
     s->bytes += op->buf_bytes;

@@ -104,6 +104,8 @@ struct ngw_session {
 namespace ngw {
 
 // allocation helpers (track session bytes)
+cudaError_t pool_alloc(ngw_session *s, void **p, size_t bytes);
+void pool_free(ngw_session *s, void *p);
 int dalloc(ngw_session *s, void **p, size_t bytes);
 void dfree(ngw_session *s, void *p, size_t bytes);
 int scratch(ngw_session *s, int slot, size_t bytes, void **p);
