@@ -329,7 +329,7 @@ def main():
                     help="batched: uneven molecules in one graph launch; serving: request stream")
     ap.add_argument("--batched-qp", type=int, default=2)
     ap.add_argument("--serving-requests", type=int, default=24)
-    ap.add_argument("--serving-workers", type=int, default=2)
+    ap.add_argument("--serving-workers", type=int, default=4)
     args = ap.parse_args()
     W = max(3, args.warmup)
     K = args.steps

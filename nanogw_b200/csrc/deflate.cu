@@ -361,7 +361,8 @@ static int eig_lanczos_persistent(ngw_session *s, int tamm_d, int m, double *V, 
   NGW_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   NGW_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
   if (!coop) return NGW_OK;
-  NGW_CUDA(cudaFuncSetAttribute(k_eig_lanczos, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  static std::atomic<unsigned long long> attr{0};
+  NGW_CUDA(smem_limit_once(k_eig_lanczos, 200 * 1024, attr));
   NGW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_eig_lanczos, EIG_NT, smem));
   if (per_sm < 1) return NGW_OK;
   EigLanczosArgs a{};

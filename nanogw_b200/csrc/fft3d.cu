@@ -215,16 +215,13 @@ int fft_coulomb_boxes(ngw_session *s, int n, int ncol, double *box, double2 *spe
     const int row_blocks = (int)std::min<size_t>((nrows + tl - 1) / tl, 148 * 16);
     const int tk = 8;
     const size_t smem_str = (size_t)2 * tk * n * sizeof(double2);
-    static bool attr = false;
-    if (!attr) {
-      const int mx = 200 * 1024;
-      cudaFuncSetAttribute(k_fft_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      cudaFuncSetAttribute(k_fft_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      cudaFuncSetAttribute(k_fft_strided<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      cudaFuncSetAttribute(k_fft_strided<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      cudaFuncSetAttribute(k_fft_strided<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      attr = true;
-    }
+    static std::atomic<unsigned long long> attr[5] = {};
+    const int mx = 200 * 1024;
+    NGW_CUDA(smem_limit_once(k_fft_rows_r2c, mx, attr[0]));
+    NGW_CUDA(smem_limit_once(k_fft_rows_c2r, mx, attr[1]));
+    NGW_CUDA(smem_limit_once(k_fft_strided<0>, mx, attr[2]));
+    NGW_CUDA(smem_limit_once(k_fft_strided<1>, mx, attr[3]));
+    NGW_CUDA(smem_limit_once(k_fft_strided<2>, mx, attr[4]));
     const dim3 rblk(64, tl), sblk(8, tk);
     const dim3 sgrid((h + tk - 1) / tk, ygrid((long long)ncol * n));
     const size_t colsz = (size_t)n * n * h;

@@ -748,12 +748,8 @@ static int launch_tc(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUt
                      const CUtensorMap &b_lo, int tiles_m, int tiles_n, const GemmArgs &ga,
                      const EpiParams &ep, int *status, cudaStream_t st) {
   constexpr size_t smem = (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) * (FUSED ? 2 : 1) + 1024;
-  static bool attr = false;
-  if (!attr) {
-    NGW_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, MINB, FUSED>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  NGW_CUDA(smem_limit_once(k_tc_gemm<BN, STAGES, MINB, FUSED>, (int)smem, attr));
   dim3 grid(tiles_m, tiles_n, ga.nsplit);
   NGW_CUDA(launch_pdl(k_tc_gemm<BN, STAGES, MINB, FUSED>, grid, dim3(NTHREADS), smem, st, a_hi, a_lo,
                       b_hi, b_lo, ga, ep, status));
@@ -767,12 +763,8 @@ static int launch_tc_cluster(const CUtensorMap &a_hi, const CUtensorMap &a_lo, c
                              const EpiParams &ep, int *status, cudaStream_t st) {
   constexpr size_t smem = (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) * 2 + 1024;
   static_assert((size_t)BN * BM * 4 <= smem - 1024, "partial tile must fit the stage buffers");
-  static bool attr = false;
-  if (!attr) {
-    NGW_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, MINB, true, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  NGW_CUDA(smem_limit_once(k_tc_gemm<BN, STAGES, MINB, true, true>, (int)smem, attr));
   if (ga.nsplit < 2 || ga.nsplit > 8) {
     set_error("cluster split-K needs 2..8 splits (got %d)", ga.nsplit);
     return NGW_ERR_ARG;
@@ -801,12 +793,8 @@ static int launch_tc_p(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const C
                        const CUtensorMap &b_lo, int tiles_m, int tiles_n, const GemmArgs &ga,
                        const EpiParams &ep, int *status, cudaStream_t st) {
   constexpr size_t smem = (size_t)STAGES * (2 * BM * BK * 2 + 2 * BN * BK * 2) + 1024;
-  static bool attr = false;
-  if (!attr) {
-    NGW_CUDA(cudaFuncSetAttribute(k_tc_gemm_p<BN, STAGES>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  NGW_CUDA(smem_limit_once(k_tc_gemm_p<BN, STAGES>, (int)smem, attr));
   GemmArgs g2 = ga;
   g2.num_kb = ga.num_kb;   // fused segments: one k-block carries all three products
   const int nwork = tiles_m * tiles_n * ga.nsplit;

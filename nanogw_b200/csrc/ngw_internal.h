@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cublas_v2.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -106,6 +107,21 @@ namespace ngw {
 // allocation helpers (track session bytes)
 cudaError_t pool_alloc(ngw_session *s, void **p, size_t bytes);
 void pool_free(ngw_session *s, void *p);
+
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current
+// device, once per device (the attribute is per device; `done` holds one bit
+// per device already set).  Safe to call from several threads.
+template <class Kernel>
+inline cudaError_t smem_limit_once(Kernel kernel, int bytes, std::atomic<unsigned long long> &done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
 int dalloc(ngw_session *s, void **p, size_t bytes);
 void dfree(ngw_session *s, void *p, size_t bytes);
 int scratch(ngw_session *s, int slot, size_t bytes, void **p);

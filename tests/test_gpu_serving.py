@@ -47,7 +47,7 @@ def test_alone_equals_in_mix(requests, precision):
     mix = [_clone(r) for r in requests] + [_clone(r) for r in requests]
     for i, r in enumerate(mix):
         r.rid = i
-    srv = SigmaServer(workers=3, precision=precision)
+    srv = SigmaServer(workers=6, precision=precision)   # all six at once
     st = srv.run(mix, realtime=False)
     srv.close()
     assert st["requests"] == 6
