@@ -652,6 +652,150 @@ __global__ void __launch_bounds__(PTHREADS, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// GEMM2 with the Clenshaw operands staged by TMA (variant 7).  Fused hi/lo
+// stages as variants 3 / 4, one CTA per SM; the CTA's 128 x BN tiles of
+// b_{k+1}, b_{k+2} and v (FP32) are loaded into their own shared-memory
+// region by three bulk tensor copies issued as soon as the previous kernel's
+// results are visible, so they arrive while the MMAs run and the epilogue
+// reads them from shared memory: no per-element global loads, no registers
+// held for prefetch.  Epilogue arithmetic and stores as k_tc_gemm.
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_tc_gemm_te(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
+                 const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
+                 const __grid_constant__ CUtensorMap tX, const __grid_constant__ CUtensorMap tB2,
+                 const __grid_constant__ CUtensorMap tV, GemmArgs ga, EpiParams ep, int *status) {
+  constexpr uint32_t A_BYTES = BM * BK * 2;
+  constexpr uint32_t B_BYTES = BN * BK * 2;
+  constexpr uint32_t STAGE_BYTES = 2 * (A_BYTES + B_BYTES);
+  constexpr uint32_t OPER_BYTES = BM * BN * 4;          // one FP32 operand tile
+  constexpr uint32_t TMEM_COLS = (BN <= 32) ? 32 : (BN <= 64) ? 64 : 128;
+  constexpr uint32_t IDESC = tc::idesc_bf16_f32(BM, BN);
+  constexpr int NCH = BN / 16;
+  constexpr int NCH0 = (NCH + 1) / 2;
+
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  float *eop = reinterpret_cast<float *>(smem + STAGES * STAGE_BYTES);   // x | b2 | v tiles
+  __shared__ __align__(8) uint64_t full_bar[STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[STAGES];
+  __shared__ __align__(8) uint64_t done_bar;
+  __shared__ __align__(8) uint64_t epi_bar;
+  __shared__ uint32_t tmem_base_sh;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int nkb = ga.num_kb;
+  const bool has_b2 = ep.b2 != nullptr, has_v = ep.v != nullptr;
+
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < STAGES; ++st) {
+      tc::mbar_init(tc::smem_u32(&full_bar[st]), 1);
+      tc::mbar_init(tc::smem_u32(&empty_bar[st]), 1);
+    }
+    tc::mbar_init(tc::smem_u32(&done_bar), 1);
+    tc::mbar_init(tc::smem_u32(&epi_bar), 1);
+    tc::fence_barrier_init();
+    tc::prefetch_tmap(&tA_hi);
+    tc::prefetch_tmap(&tB_hi);
+    tc::prefetch_tmap(&tX);
+  }
+  if (warp == 2) {
+    tc::tmem_alloc(tc::smem_u32(&tmem_base_sh), TMEM_COLS);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem_d = tmem_base_sh;
+  tc::pdl_wait();                 // operands / epilogue inputs come from the previous kernel
+  tc::pdl_launch_dependents();
+
+  if (warp == 0 && lane == 0) {
+    // the Clenshaw operand tiles first (they are read last but have no
+    // dependence on the MMAs), then the k-blocks of the product
+    const uint32_t eb = tc::smem_u32(&epi_bar);
+    tc::mbar_arrive_expect_tx(eb, OPER_BYTES * (1u + (has_b2 ? 1u : 0u) + (has_v ? 1u : 0u)));
+    tc::tma_load_2d(tc::smem_u32(eop), &tX, eb, m0, n0);
+    if (has_b2) tc::tma_load_2d(tc::smem_u32(eop) + OPER_BYTES, &tB2, eb, m0, n0);
+    if (has_v) tc::tma_load_2d(tc::smem_u32(eop) + 2 * OPER_BYTES, &tV, eb, m0, n0);
+    for (int i = 0; i < nkb; ++i) {
+      const int st = i % STAGES;
+      if (i >= STAGES) {
+        if (!tc::mbar_wait(tc::smem_u32(&empty_bar[st]), ((i / STAGES) - 1) & 1, status)) break;
+      }
+      const uint32_t bar = tc::smem_u32(&full_bar[st]);
+      const uint32_t sa = tc::smem_u32(smem + st * STAGE_BYTES);
+      tc::mbar_arrive_expect_tx(bar, STAGE_BYTES);
+      tc::tma_load_2d(sa, &tA_hi, bar, i * BK, m0);
+      tc::tma_load_2d(sa + A_BYTES, &tA_lo, bar, i * BK, m0);
+      tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, i * BK, n0);
+      tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, i * BK, n0);
+    }
+  } else if (warp == 1 && lane == 0) {
+    for (int i = 0; i < nkb; ++i) {
+      const int st = i % STAGES;
+      if (!tc::mbar_wait(tc::smem_u32(&full_bar[st]), (i / STAGES) & 1, status)) break;
+      tc::tc_fence_after();
+      const uint32_t sa = tc::smem_u32(smem + st * STAGE_BYTES);
+      const uint32_t sal = sa + A_BYTES, sbh = sa + 2 * A_BYTES, sbl = sbh + B_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        const uint32_t acc0 = (i > 0 || kk > 0) ? 1u : 0u;
+        tc::mma_bf16(tmem_d, tc::smem_desc_sw128(sa + kk * 32), tc::smem_desc_sw128(sbh + kk * 32), IDESC, acc0);
+        tc::mma_bf16(tmem_d, tc::smem_desc_sw128(sa + kk * 32), tc::smem_desc_sw128(sbl + kk * 32), IDESC, 1u);
+        tc::mma_bf16(tmem_d, tc::smem_desc_sw128(sal + kk * 32), tc::smem_desc_sw128(sbh + kk * 32), IDESC, 1u);
+      }
+      tc::mma_commit(tc::smem_u32(&empty_bar[st]));
+    }
+    tc::mma_commit(tc::smem_u32(&done_bar));
+  }
+  __syncwarp();
+
+  const int wl = warp & 3, wg = warp >> 2;
+  const int mloc = wl * 32 + lane;
+  const int m = m0 + mloc;
+  const uint32_t trow = tmem_d + ((uint32_t)(wl * 32) << 16);
+  const int ch_begin = wg == 0 ? 0 : NCH0;
+  const int ch_end = wg == 0 ? NCH0 : NCH;
+  const bool mv = m < ep.Mv;
+  const ClenCoef kc = clen_coef(ep, mv ? ep.s[m] : 0.0);
+  bool have = tc::mbar_wait(tc::smem_u32(&done_bar), 0, status) && nkb > 0;
+  const bool have_ops = tc::mbar_wait(tc::smem_u32(&epi_bar), 0, status);
+  tc::tc_fence_after();
+  for (int ch = 2 * ch_begin; ch < 2 * ch_end; ++ch) {
+    const int c = ch * 8;
+    float z[8];
+    if (have) {
+      tc::tmem_ld8(trow + c, z);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) z[j] = 0.f;
+    }
+    if (!mv || !have_ops) continue;
+    const int nbase = n0 + c;
+    const int nj = min(8, ep.Nv - nbase);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (j >= nj) break;
+      const int e = (c + j) * BM + mloc;
+      const float x = eop[e];
+      const float b2 = has_b2 ? eop[BM * BN + e] : 0.f;
+      const float v = has_v ? eop[2 * BM * BN + e] : 0.f;
+      clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2));
+    }
+  }
+
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem_d, TMEM_COLS);
+  }
+}
+
 // Deterministic split-K reduction: D(m, n) = sum_s partial_s(m, n) in split
 // order, written as the split-BF16 pair.  One thread per output element,
 // consecutive threads on consecutive rows (coalesced partial reads).
@@ -711,6 +855,26 @@ static int make_tmap(CUtensorMap *map, const void *ptr, int rows, int cols, int 
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed (%d) rows=%d cols=%d box_rows=%d", (int)r, rows, cols,
               box_rows);
+    return NGW_ERR_CUDA;
+  }
+  return NGW_OK;
+}
+
+// FP32 column-major matrix (rows contiguous, leading dimension rows) as 2-D
+// tiles of 128 rows x box_cols columns, no swizzle: the tile lands in shared
+// memory column after column, row r of column c at word c * 128 + r.
+static int make_tmap_f32(CUtensorMap *map, const void *ptr, int rows, int cols, int box_cols) {
+  NGW_TRY(get_encode());
+  cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+  cuuint64_t strides[1] = {(cuuint64_t)rows * 4};
+  cuuint32_t box[2] = {(cuuint32_t)BM, (cuuint32_t)box_cols};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(ptr), dims, strides,
+                        box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (FP32) failed (%d) rows=%d cols=%d box_cols=%d", (int)r, rows, cols,
+              box_cols);
     return NGW_ERR_CUDA;
   }
   return NGW_OK;
@@ -802,6 +966,37 @@ static int launch_tc_p(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const C
   NGW_CUDA(launch_pdl(k_tc_gemm_p<BN, STAGES>, dim3(grid), dim3(PTHREADS), smem, st, a_hi, a_lo, b_hi,
                       b_lo, g2, ep, tiles_m, tiles_n, status));
   return NGW_OK;
+}
+
+template <int BN, int STAGES>
+static int launch_tc_te(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
+                        const CUtensorMap &b_lo, const CUtensorMap &tx, const CUtensorMap &tb2,
+                        const CUtensorMap &tv, int tiles_m, int tiles_n, const GemmArgs &ga,
+                        const EpiParams &ep, int *status, cudaStream_t st) {
+  constexpr size_t smem = (size_t)STAGES * 2 * (BM * BK * 2 + BN * BK * 2) + (size_t)3 * BM * BN * 4 + 1024;
+  static_assert(smem <= 232448 - 256, "variant 7 tile does not fit shared memory");
+  static std::atomic<unsigned long long> attr{0};
+  NGW_CUDA(smem_limit_once(k_tc_gemm_te<BN, STAGES>, (int)smem, attr));
+  NGW_CUDA(launch_pdl(k_tc_gemm_te<BN, STAGES>, dim3(tiles_m, tiles_n, 1), dim3(NTHREADS), smem, st, a_hi,
+                      a_lo, b_hi, b_lo, tx, tb2, tv, ga, ep, status));
+  return NGW_OK;
+}
+
+// variant 7 (GEMM2 only): fused stages + Clenshaw operands staged by TMA
+static bool has_te(int BN) { return BN == 32 || BN == 48 || BN == 64 || BN == 80; }
+
+static int dispatch_te(int BN, const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
+                       const CUtensorMap &b_lo, const CUtensorMap &tx, const CUtensorMap &tb2,
+                       const CUtensorMap &tv, int tiles_m, int tiles_n, const GemmArgs &ga,
+                       const EpiParams &ep, int *status, cudaStream_t st) {
+  switch (BN) {
+    case 32: return launch_tc_te<32, 4>(a_hi, a_lo, b_hi, b_lo, tx, tb2, tv, tiles_m, tiles_n, ga, ep, status, st);
+    case 48: return launch_tc_te<48, 3>(a_hi, a_lo, b_hi, b_lo, tx, tb2, tv, tiles_m, tiles_n, ga, ep, status, st);
+    case 64: return launch_tc_te<64, 2>(a_hi, a_lo, b_hi, b_lo, tx, tb2, tv, tiles_m, tiles_n, ga, ep, status, st);
+    case 80: return launch_tc_te<80, 2>(a_hi, a_lo, b_hi, b_lo, tx, tb2, tv, tiles_m, tiles_n, ga, ep, status, st);
+  }
+  set_error("variant 7 has no N tile %d", BN);
+  return NGW_ERR_ARG;
 }
 
 static bool has_persistent(int BN) { return BN <= 160; }
@@ -1007,6 +1202,8 @@ struct MixedOperator {
   CUtensorMap tShi, tSlo, tThi, tTlo;
   float *bb[3] = {nullptr, nullptr, nullptr};
   float *vperp = nullptr;
+  CUtensorMap tBB[3], tVp;   // FP32 tiles of bb[i] / vperp for variant 7 (N tile maps_te_bn)
+  int maps_te_bn = -1;
   double *xo = nullptr;
   float *ws = nullptr;
   size_t buf_bytes = 0;
@@ -1028,6 +1225,7 @@ static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
   op->buf_bytes = 0;
   op->nb_cap = 0;
   op->maps_bn1 = op->maps_bn2 = -1;
+  op->maps_te_bn = -1;
   op->tuned_nb = -1;
 }
 
@@ -1260,6 +1458,13 @@ static int autotune(ngw_session *s, int nb) {
       }
     }
   }
+  // variant 7 (GEMM2 only): Clenshaw operands staged by TMA
+  for (int bn : kBNs) {
+    if (!has_te(bn)) continue;
+    if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
+    if ((round_up(nb, bn) - nb) * 8 > nb && bn != kBNs[0]) continue;
+    c2.push_back({bn, 7, 1});
+  }
   // GEMM2 fixed while GEMM1 is tuned: the 64-wide (or smallest) non-fused tile
   C2 fix2 = c2.front();
   for (const C2 &c : c2)
@@ -1482,6 +1687,27 @@ static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, co
   }
   const int tiles_m = op->cv_pad / BM;
   const int tiles_n = (nb + op->BN2 - 1) / op->BN2;
+  if (op->var2 == 7) {
+    // operands are chain buffers: FP32 tensor maps of each, built per N tile
+    if (op->maps_te_bn != op->BN2) {
+      for (int i = 0; i < 3; ++i) NGW_TRY(make_tmap_f32(&op->tBB[i], op->bb[i], op->cv_pad, op->nb_pad, op->BN2));
+      NGW_TRY(make_tmap_f32(&op->tVp, op->vperp, op->cv_pad, op->nb_pad, op->BN2));
+      op->maps_te_bn = op->BN2;
+    }
+    auto pick = [&](const float *p) -> const CUtensorMap * {
+      for (int i = 0; i < 3; ++i)
+        if (p == op->bb[i]) return &op->tBB[i];
+      return p == op->vperp ? &op->tVp : nullptr;
+    };
+    const CUtensorMap *mx = pick(x), *mb2 = b2 ? pick(b2) : &op->tBB[0], *mvv = v ? pick(v) : &op->tBB[0];
+    if (!mx || !mb2 || !mvv) {
+      set_error("GEMM2 variant 7: Clenshaw operand outside the chain buffers");
+      return NGW_ERR_ARG;
+    }
+    ga.nsplit = 1;
+    return dispatch_te(op->BN2, op->tA3hi, op->tA3lo, op->tThi, op->tTlo, *mx, *mb2, *mvv, tiles_m, tiles_n,
+                       ga, ep, s->d_status, s->stream);
+  }
   return dispatch_tc(op->BN2, op->var2, op->tA3hi, op->tA3lo, op->tThi, op->tTlo, tiles_m, tiles_n,
                      ga, ep, s->d_status, s->stream);
 }

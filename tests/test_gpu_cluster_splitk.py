@@ -84,7 +84,7 @@ def test_cluster_split_k_gemm2_within_1mev(tmp_path):
     assert np.all(r[:-2] < 1.0), r
 
 
-@pytest.mark.parametrize("gemm2", ["64,2", "64,3", "64,4", "32,4", "128,3", "32,6,4"])
+@pytest.mark.parametrize("gemm2", ["64,2", "64,3", "64,4", "32,4", "128,3", "32,6,4", "32,7", "64,7", "80,7"])
 def test_gemm2_variants_within_1mev(tmp_path, gemm2):
     """Every GEMM2 kernel form with the Clenshaw epilogue (persistent, fused
     one or two CTAs per SM, cluster split-K) keeps the QP energies within
@@ -96,8 +96,11 @@ def test_gemm2_variants_within_1mev(tmp_path, gemm2):
 
 
 def test_gemm2_occupancy_forms_bit_identical(tmp_path):
-    """The fused GEMM2 at one and at two CTAs per SM runs the same MMAs and
-    the same epilogue arithmetic: identical Sigma_c."""
+    """The fused GEMM2 at one and at two CTAs per SM, and with its Clenshaw
+    operands staged by TMA (variant 7), runs the same MMAs and the same
+    epilogue arithmetic: identical Sigma_c."""
     a = _run(tmp_path, "64,3,2,64,3")
     b = _run(tmp_path, "64,3,2,64,4")
+    c = _run(tmp_path, "64,3,2,64,7")
     assert np.array_equal(a, b)
+    assert np.array_equal(a, c)
