@@ -70,6 +70,7 @@ struct EpiParams {
   double *out64;         // final p(C) v (nullable)
   bf16 *s_hi, *s_lo;     // split of (R^1/2 or 1) * out  [n * lds + m] (nullable)
   int lds;
+  int ring;              // EPI_CLENSHAW in k_tc_gemm: operands through the TMA chunk ring
 };
 
 struct GemmArgs {
@@ -165,7 +166,8 @@ template <int BN, int STAGES, int MINB, bool FUSED, bool CRED = false>
 __global__ void __launch_bounds__(NTHREADS, MINB)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
               const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
-              GemmArgs ga, EpiParams ep, int *status) {
+              const __grid_constant__ CUtensorMap tRx, const __grid_constant__ CUtensorMap tRb2,
+              const __grid_constant__ CUtensorMap tRv, GemmArgs ga, EpiParams ep, int *status) {
   // FUSED: one stage holds A_hi, A_lo, B_hi, B_lo of a k-block and carries all
   // three split products; otherwise one stage is one (A, B) pair of a segment.
   constexpr uint32_t A_BYTES = BM * BK * 2;
@@ -182,6 +184,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
   __shared__ __align__(8) uint64_t full_bar[STAGES];
   __shared__ __align__(8) uint64_t empty_bar[STAGES];
   __shared__ __align__(8) uint64_t done_bar;
+  __shared__ __align__(8) uint64_t ring_bar[2][4];   // Clenshaw operand ring, per warpgroup
   __shared__ uint32_t tmem_base_sh;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -199,6 +202,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
       tc::mbar_init(tc::smem_u32(&empty_bar[s]), 1);
     }
     tc::mbar_init(tc::smem_u32(&done_bar), 1);
+    for (int g = 0; g < 2; ++g)
+      for (int r = 0; r < 4; ++r) tc::mbar_init(tc::smem_u32(&ring_bar[g][r]), 1);
     tc::fence_barrier_init();
     tc::prefetch_tmap(&tA_hi);
     tc::prefetch_tmap(&tB_hi);
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
   double si = 0.0;
   if (clenshaw) {
     if (mv) si = ep.s[m];
-    clenshaw_operands(ep, mv, m, n0 + 16 * ch_begin, px, pb, pv);
+    if (!ep.ring) clenshaw_operands(ep, mv, m, n0 + 16 * ch_begin, px, pb, pv);
   }
   // Cluster split-K: this CTA finishes the tile columns [c_lo, c_hi); thread
   // row crow takes c_first, c_first + cstep, ... in groups of 4, the Clenshaw
@@ -401,6 +406,62 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     // (TDA: R - c0, 2 z) in FP32 (clen_out); split((R^1/2 or 1) out).
     // 8-column chunks keep the register count low enough for 2 CTAs per SM.
     const ClenCoef kc = clen_coef(ep, si);
+    if (ep.ring) {
+      // Operand ring in the stage memory the MMAs no longer need: per
+      // warpgroup RS slots of one 8-column chunk (b_{k+1} | b_{k+2} | v,
+      // 128 rows each).  The warpgroup's first thread fills a slot with
+      // three bulk tensor copies and refills it once all four warps have
+      // read it (named barrier), RS chunks ahead of its use.
+      constexpr uint32_t OP8 = BM * 8 * 4;
+      constexpr uint32_t CHUNK = 3 * OP8;
+      constexpr int RS = (int)((STAGES * STAGE_BYTES) / (2 * CHUNK)) < 4 ? (int)((STAGES * STAGE_BYTES) / (2 * CHUNK)) : 4;
+      static_assert(RS >= 1, "stage memory too small for the operand ring");
+      const uint32_t ring = tc::smem_u32(smem) + (uint32_t)(wg * RS) * CHUNK;
+      const float *ringf = reinterpret_cast<const float *>(smem + (size_t)wg * RS * CHUNK);
+      const bool leader = (threadIdx.x & 127) == 0;
+      const int nq = 2 * (ch_end - ch_begin);
+      const int c_first = 16 * ch_begin;
+      const uint32_t bytes = OP8 * (1u + (ep.b2 ? 1u : 0u) + (ep.v ? 1u : 0u));
+      auto issue = [&](int q) {
+        const int r = q % RS;
+        const uint32_t bar = tc::smem_u32(&ring_bar[wg][r]);
+        const uint32_t dst = ring + (uint32_t)r * CHUNK;
+        const int nc = n0 + c_first + 8 * q;
+        tc::mbar_arrive_expect_tx(bar, bytes);
+        tc::tma_load_2d(dst, &tRx, bar, m0, nc);
+        if (ep.b2) tc::tma_load_2d(dst + OP8, &tRb2, bar, m0, nc);
+        if (ep.v) tc::tma_load_2d(dst + 2 * OP8, &tRv, bar, m0, nc);
+      };
+      if (leader)
+        for (int q = 0; q < nq && q < RS; ++q) issue(q);
+      for (int q = 0; q < nq; ++q) {
+        const int r = q % RS;
+        const int c = c_first + 8 * q;
+        float z[8];
+        if (have) {
+          tc::tmem_ld8(trow + c, z);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) z[j] = 0.f;
+        }
+        const bool ok = tc::mbar_wait(tc::smem_u32(&ring_bar[wg][r]), (uint32_t)((q / RS) & 1), status);
+        if (mv && ok) {
+          const float *sl = ringf + (size_t)r * (CHUNK / 4) + mloc;
+          const int nbase = n0 + c;
+          const int nj = min(8, ep.Nv - nbase);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            if (j >= nj) break;
+            const float x = sl[j * BM];
+            const float b2 = ep.b2 ? sl[OP8 / 4 + j * BM] : 0.f;
+            const float v = ep.v ? sl[2 * (OP8 / 4) + j * BM] : 0.f;
+            clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2));
+          }
+        }
+        asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");   // slot r read by the warpgroup
+        if (leader && q + RS < nq) issue(q + RS);
+      }
+    } else
     for (int ch = 2 * ch_begin; ch < 2 * ch_end; ++ch) {
       const int c = ch * 8;
       float z[8];
@@ -910,13 +971,15 @@ static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, siz
 template <int BN, int STAGES, int MINB, bool FUSED = false>
 static int launch_tc(const CUtensorMap &a_hi, const CUtensorMap &a_lo, const CUtensorMap &b_hi,
                      const CUtensorMap &b_lo, int tiles_m, int tiles_n, const GemmArgs &ga,
-                     const EpiParams &ep, int *status, cudaStream_t st) {
+                     const EpiParams &ep, int *status, cudaStream_t st, const CUtensorMap *rm) {
   constexpr size_t smem = (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) * (FUSED ? 2 : 1) + 1024;
   static std::atomic<unsigned long long> attr{0};
   NGW_CUDA(smem_limit_once(k_tc_gemm<BN, STAGES, MINB, FUSED>, (int)smem, attr));
   dim3 grid(tiles_m, tiles_n, ga.nsplit);
+  // operand-ring maps (x, b2, v) of the Clenshaw epilogue; unused (ring = 0) otherwise
+  const CUtensorMap &rx = rm ? rm[0] : a_hi, &rb2 = rm ? rm[1] : a_hi, &rv = rm ? rm[2] : a_hi;
   NGW_CUDA(launch_pdl(k_tc_gemm<BN, STAGES, MINB, FUSED>, grid, dim3(NTHREADS), smem, st, a_hi, a_lo,
-                      b_hi, b_lo, ga, ep, status));
+                      b_hi, b_lo, rx, rb2, rv, ga, ep, status));
   return NGW_OK;
 }
 
@@ -947,8 +1010,8 @@ static int launch_tc_cluster(const CUtensorMap &a_hi, const CUtensorMap &a_lo, c
   attrs[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attrs;
   cfg.numAttrs = pdl_enabled() ? 2 : 1;
-  NGW_CUDA(cudaLaunchKernelEx(&cfg, k_tc_gemm<BN, STAGES, MINB, true, true>, a_hi, a_lo, b_hi, b_lo, ga, ep,
-                              status));
+  NGW_CUDA(cudaLaunchKernelEx(&cfg, k_tc_gemm<BN, STAGES, MINB, true, true>, a_hi, a_lo, b_hi, b_lo, a_hi,
+                              a_hi, a_hi, ga, ep, status));
   return NGW_OK;
 }
 
@@ -1015,9 +1078,10 @@ static bool has_shallow(int BN) { return BN <= 160; }
 
 static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
                        const CUtensorMap &b_hi, const CUtensorMap &b_lo, int tiles_m, int tiles_n,
-                       const GemmArgs &ga, const EpiParams &ep, int *status, cudaStream_t st) {
+                       const GemmArgs &ga, const EpiParams &ep, int *status, cudaStream_t st,
+                       const CUtensorMap *rm = nullptr) {
 #define NGW_TC(BNV, ST, MB) \
-  return launch_tc<BNV, ST, MB>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st)
+  return launch_tc<BNV, ST, MB>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st, rm)
 #define NGW_TCP(BNV, ST) \
   return launch_tc_p<BNV, ST>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st)
   if (var == 2) {
@@ -1034,7 +1098,7 @@ static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorM
   }
 #undef NGW_TCP
 #define NGW_TCF(BNV, ST, MB) \
-  return launch_tc<BNV, ST, MB, true>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st)
+  return launch_tc<BNV, ST, MB, true>(a_hi, a_lo, b_hi, b_lo, tiles_m, tiles_n, ga, ep, status, st, rm)
   if (var == 3) {
     switch (BN) {
       case 32: NGW_TCF(32, 5, 1);
@@ -1204,6 +1268,8 @@ struct MixedOperator {
   float *vperp = nullptr;
   CUtensorMap tBB[3], tVp;   // FP32 tiles of bb[i] / vperp for variant 7 (N tile maps_te_bn)
   int maps_te_bn = -1;
+  CUtensorMap tR[4];         // 128 x 8 FP32 chunks of bb[0..2], vperp (the epilogue operand ring)
+  bool maps_ring = false;
   double *xo = nullptr;
   float *ws = nullptr;
   size_t buf_bytes = 0;
@@ -1226,6 +1292,7 @@ static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
   op->nb_cap = 0;
   op->maps_bn1 = op->maps_bn2 = -1;
   op->maps_te_bn = -1;
+  op->maps_ring = false;
   op->tuned_nb = -1;
 }
 
@@ -1707,6 +1774,32 @@ static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, co
     ga.nsplit = 1;
     return dispatch_te(op->BN2, op->tA3hi, op->tA3lo, op->tThi, op->tTlo, *mx, *mb2, *mvv, tiles_m, tiles_n,
                        ga, ep, s->d_status, s->stream);
+  }
+  // variants 0, 1, 3, 4: Clenshaw operands through the TMA chunk ring
+  static const bool ring_on = [] {
+    const char *e = getenv("NGW_RING");
+    return !(e && e[0] == '0');
+  }();
+  if (ring_on && (op->var2 == 0 || op->var2 == 1 || op->var2 == 3 || op->var2 == 4)) {
+    if (!op->maps_ring) {
+      for (int i = 0; i < 3; ++i) NGW_TRY(make_tmap_f32(&op->tR[i], op->bb[i], op->cv_pad, op->nb_pad, 8));
+      NGW_TRY(make_tmap_f32(&op->tR[3], op->vperp, op->cv_pad, op->nb_pad, 8));
+      op->maps_ring = true;
+    }
+    auto slot = [&](const float *p) -> int {
+      for (int i = 0; i < 3; ++i)
+        if (p == op->bb[i]) return i;
+      return p == op->vperp ? 3 : -1;
+    };
+    const int ix = slot(x), ib2 = b2 ? slot(b2) : 0, iv = v ? slot(v) : 0;
+    if (ix < 0 || ib2 < 0 || iv < 0) {
+      set_error("GEMM2: Clenshaw operand outside the chain buffers");
+      return NGW_ERR_ARG;
+    }
+    const CUtensorMap rm[3] = {op->tR[ix], op->tR[ib2], op->tR[iv]};
+    ep.ring = 1;
+    return dispatch_tc(op->BN2, op->var2, op->tA3hi, op->tA3lo, op->tThi, op->tTlo, tiles_m, tiles_n,
+                       ga, ep, s->d_status, s->stream, rm);
   }
   return dispatch_tc(op->BN2, op->var2, op->tA3hi, op->tA3lo, op->tThi, op->tTlo, tiles_m, tiles_n,
                      ga, ep, s->d_status, s->stream);

@@ -30,9 +30,9 @@ np.save({out!r}, sig)
 """
 
 
-def _run(tmp_path, tiles):
-    out = str(tmp_path / ("sig_" + tiles.replace(",", "_") + ".npy"))
-    env = dict(os.environ, NGW_TILES=tiles)
+def _run(tmp_path, tiles, **extra_env):
+    out = str(tmp_path / ("sig_" + tiles.replace(",", "_") + "_".join(extra_env) + ".npy"))
+    env = dict(os.environ, NGW_TILES=tiles, **extra_env)
     subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT, out=out)], env=env, check=True,
                    timeout=600)
     return np.load(out)
@@ -104,3 +104,12 @@ def test_gemm2_occupancy_forms_bit_identical(tmp_path):
     c = _run(tmp_path, "64,3,2,64,7")
     assert np.array_equal(a, b)
     assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("tiles", ["64,3,2,64,4", "64,3,2,96,1"])
+def test_operand_ring_bit_identical(tmp_path, tiles):
+    """GEMM2's Clenshaw operands through the TMA chunk ring or loaded by each
+    thread (NGW_RING=0): the same values in the same arithmetic."""
+    a = _run(tmp_path, tiles)
+    b = _run(tmp_path, tiles, NGW_RING="0")
+    assert np.array_equal(a, b)
