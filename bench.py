@@ -136,7 +136,10 @@ def solve_once(sess, op, qp, poly, wl, sigx, vxc):
 # Operator dimensions of the large single-molecule workload (60 atoms, 240
 # occupied + 960 empty orbitals, 4800 ISDF points: N_cv = 230,400) and of the
 # largest molecule of the batched workload (140 + 560 orbitals, 1120 points).
-LARGE_OPERATORS = {"large-molecule": (4800, 240, 960), "batched-max": (1120, 140, 560)}
+# (n_isdf, n_occ, n_empty) of operators the GEMM scan times: the large single
+# molecule, the batched configuration's largest, and a mid-size serving request
+LARGE_OPERATORS = {"large-molecule": (4800, 240, 960), "batched-max": (1120, 140, 560),
+                   "serving-mid": (304, 38, 152)}
 
 
 def random_operator(n_isdf, nocc, nemp, seed):
