@@ -411,43 +411,60 @@ void launch_sigma_spectra(const double *a, const double *b, int niter, int nchai
 //   TDA:     -S_n(ezz) * eta_n * sqrt(2) * pnorm2_n   (sqrt(2) in single precision, as 2.0**0.5)
 // (calculate_sigma_lanczos_lowcomsym.F90:736-745).  The chain of (QP iq,
 // band nn) is slot[iq*nbsum + nn] of this block (iq*nbsum + nn without slot).
-__global__ void k_sigma_reduce(const double *__restrict__ S, const double *__restrict__ pnorm2,
-                               const double *__restrict__ e1, const int *__restrict__ chain_band,
-                               const double *__restrict__ zz0, double de, int nen, double ecuts,
-                               int nval, int nbsum, int nqp, int tamm_d,
-                               double *__restrict__ sigma, int accumulate,
-                               const int *__restrict__ slot) {
+// Block (32 energies) x (8 band groups): lane x of warp y sums bands
+// y, y + 8, ... for energy x (consecutive lanes read consecutive energies of
+// a chain's spectrum); the 8 partial sums are added in a fixed order.
+constexpr int SR_E = 32, SR_G = 8;
+__global__ void __launch_bounds__(SR_E *SR_G)
+    k_sigma_reduce(const double *__restrict__ S, const double *__restrict__ pnorm2,
+                   const double *__restrict__ e1, const int *__restrict__ chain_band,
+                   const double *__restrict__ zz0, double de, int nen, double ecuts, int nval, int nbsum,
+                   int nqp, int tamm_d, double *__restrict__ sigma, int accumulate,
+                   const int *__restrict__ slot) {
+  __shared__ double part[SR_G][SR_E][2];
   const int iq = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (iq >= nqp || i >= nen) return;
-  const double zz = de * (double)i + zz0[iq];
-  const double sqrt2f = (double)sqrtf(2.0f);
+  const int i = blockIdx.x * SR_E + threadIdx.x;
+  const bool on = iq < nqp && i < nen;
   cplx acc = {0.0, 0.0};
-  if (accumulate) {
-    acc.re = sigma[2 * ((size_t)iq * nen + i)];
-    acc.im = sigma[2 * ((size_t)iq * nen + i) + 1];
-  }
-  for (int nn = 0; nn < nbsum; ++nn) {
-    const int j = slot ? slot[iq * nbsum + nn] : iq * nbsum + nn;
-    const int n = chain_band[j];
-    const double eta = (n <= nval) ? 1.0 : -1.0;
-    const size_t o = (size_t)j * (nen + 1);
-    cplx s = {S[2 * (o + i)], S[2 * (o + i) + 1]};
-    cplx t;
-    if (tamm_d) {
-      t.re = -s.re * eta * sqrt2f * pnorm2[j];
-      t.im = -s.im * eta * sqrt2f * pnorm2[j];
-    } else {
-      cplx s0 = {S[2 * (o + nen)], S[2 * (o + nen) + 1]};
-      cplx d = {(s0.re - s.re) * eta * 2.0 * pnorm2[j], (s0.im - s.im) * eta * 2.0 * pnorm2[j]};
-      cplx ez = {(-zz + e1[n - 1]) * eta, ecuts};
-      t = cdivd(d, ez);
+  if (on) {
+    const double zz = de * (double)i + zz0[iq];
+    const double sqrt2f = (double)sqrtf(2.0f);
+    for (int nn = threadIdx.y; nn < nbsum; nn += SR_G) {
+      const int j = slot ? slot[iq * nbsum + nn] : iq * nbsum + nn;
+      const int n = chain_band[j];
+      const double eta = (n <= nval) ? 1.0 : -1.0;
+      const size_t o = (size_t)j * (nen + 1);
+      cplx s = {S[2 * (o + i)], S[2 * (o + i) + 1]};
+      cplx t;
+      if (tamm_d) {
+        t.re = -s.re * eta * sqrt2f * pnorm2[j];
+        t.im = -s.im * eta * sqrt2f * pnorm2[j];
+      } else {
+        cplx s0 = {S[2 * (o + nen)], S[2 * (o + nen) + 1]};
+        cplx d = {(s0.re - s.re) * eta * 2.0 * pnorm2[j], (s0.im - s.im) * eta * 2.0 * pnorm2[j]};
+        cplx ez = {(-zz + e1[n - 1]) * eta, ecuts};
+        t = cdivd(d, ez);
+      }
+      acc.re += t.re;
+      acc.im += t.im;
     }
-    acc.re += t.re;
-    acc.im += t.im;
   }
-  sigma[2 * ((size_t)iq * nen + i)] = acc.re;
-  sigma[2 * ((size_t)iq * nen + i) + 1] = acc.im;
+  part[threadIdx.y][threadIdx.x][0] = acc.re;
+  part[threadIdx.y][threadIdx.x][1] = acc.im;
+  __syncthreads();
+  if (threadIdx.y == 0 && on) {
+    cplx tot = {0.0, 0.0};
+    if (accumulate) {
+      tot.re = sigma[2 * ((size_t)iq * nen + i)];
+      tot.im = sigma[2 * ((size_t)iq * nen + i) + 1];
+    }
+    for (int g = 0; g < SR_G; ++g) {
+      tot.re += part[g][threadIdx.x][0];
+      tot.im += part[g][threadIdx.x][1];
+    }
+    sigma[2 * ((size_t)iq * nen + i)] = tot.re;
+    sigma[2 * ((size_t)iq * nen + i) + 1] = tot.im;
+  }
 }
 
 void launch_sigma_reduce(const double *S, const double *pnorm2, const double *e1,
@@ -455,9 +472,8 @@ void launch_sigma_reduce(const double *S, const double *pnorm2, const double *e1
                          double ecuts, int nval, int nbsum, int nqp, int tamm_d, double *sigma,
                          int accumulate, const int *slot, cudaStream_t st) {
   if (nqp <= 0) return;
-  k_sigma_reduce<<<dim3(cdiv(nen, 128), nqp), 128, 0, st>>>(S, pnorm2, e1, chain_band, zz0, de,
-                                                            nen, ecuts, nval, nbsum, nqp, tamm_d,
-                                                            sigma, accumulate, slot);
+  k_sigma_reduce<<<dim3(cdiv(nen, SR_E), nqp), dim3(SR_E, SR_G), 0, st>>>(
+      S, pnorm2, e1, chain_band, zz0, de, nen, ecuts, nval, nbsum, nqp, tamm_d, sigma, accumulate, slot);
 }
 
 // P = P * sqrtR (non-TDA) ; pnorm2 = <P, P>   (calculate_sigma_lanczos_lowcomsym.F90:696-705)
