@@ -308,12 +308,99 @@ __global__ void k_lanczos_step(double *__restrict__ w, double *__restrict__ v,
   }
 }
 
+// The same step with the chain's elements held in registers (EPT per thread,
+// element i = threadIdx.x + e * LNT, the order of the three-pass form, so
+// both block sums and every result are bit-identical to it): t, w, v are read
+// once and w, v (and hs) written once, instead of three passes over the
+// vectors.  For ncv <= EPT * LNT.
+template <int EPT>
+__global__ void __launch_bounds__(LNT)
+    k_lanczos_step_reg(double *__restrict__ w, double *__restrict__ v, const double *__restrict__ t, int ncv,
+                       int k, double *__restrict__ a, double *__restrict__ b, int niter,
+                       const double *__restrict__ s, double *__restrict__ hs, int tamm_d, int prescale_next,
+                       int *__restrict__ clen, double eps) {
+  __shared__ double sh[33];
+  const int j = blockIdx.x;
+  const int L = clen ? clen[j] : niter;
+  if (k >= L) return;
+  double *wj = w + (size_t)j * ncv;
+  double *vj = v + (size_t)j * ncv;
+  const double *tj = t + (size_t)j * ncv;
+  double wr[EPT], vr[EPT];
+  double acc = 0.0;
+#pragma unroll
+  for (int e = 0; e < EPT; ++e) {
+    const int i = threadIdx.x + e * LNT;
+    wr[e] = 0.0;
+    vr[e] = 0.0;
+    if (i < ncv) {
+      wr[e] = wj[i] + tj[i];
+      vr[e] = vj[i];
+      acc += wr[e] * vr[e];
+    }
+  }
+  const double ak = block_sum<LNT>(acc, sh);
+  if (threadIdx.x == 0) a[(size_t)j * niter + k] = ak;
+  if (k + 1 >= L) {
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      const int i = threadIdx.x + e * LNT;
+      if (i < ncv) wj[i] = wr[e];
+    }
+    return;
+  }
+  acc = 0.0;
+#pragma unroll
+  for (int e = 0; e < EPT; ++e) {
+    const int i = threadIdx.x + e * LNT;
+    if (i < ncv) {
+      wr[e] = wr[e] - ak * vr[e];
+      acc += wr[e] * wr[e];
+    }
+  }
+  const double bk1 = sqrt(block_sum<LNT>(acc, sh));
+  const bool stop = clen && eps > 0.0 && bk1 < eps;
+  if (threadIdx.x == 0) {
+    b[(size_t)j * niter + k + 1] = bk1;
+    if (stop) clen[j] = k + 1;
+  }
+  const bool pre = prescale_next && !stop;
+  double *hj = hs ? hs + (size_t)j * ncv : nullptr;
+#pragma unroll
+  for (int e = 0; e < EPT; ++e) {
+    const int i = threadIdx.x + e * LNT;
+    if (i >= ncv) continue;
+    if (pre) {
+      const double wi = wr[e] / bk1;
+      wj[i] = wi;
+      vj[i] = -vr[e] * bk1;
+      if (hj) hj[i] = tamm_d ? wi : s[i] * wi;
+    } else {
+      wj[i] = wr[e];
+    }
+  }
+}
+
 void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb, int k, double *a,
                          double *b, int niter, const double *s, double *hs, int tamm_d,
                          int prescale_next, int *clen, double eps, cudaStream_t st) {
   if (nb <= 0) return;
-  k_lanczos_step<<<nb, LNT, 0, st>>>(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next, clen,
-                                     eps);
+#define NGW_LSR(E)                                                                                       \
+  k_lanczos_step_reg<E><<<nb, LNT, 0, st>>>(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next, \
+                                            clen, eps)
+  if (ncv <= 8 * LNT) {
+    NGW_LSR(8);
+  } else if (ncv <= 16 * LNT) {
+    NGW_LSR(16);
+  } else if (ncv <= 24 * LNT) {
+    NGW_LSR(24);
+  } else if (ncv <= 32 * LNT) {
+    NGW_LSR(32);
+  } else {
+    k_lanczos_step<<<nb, LNT, 0, st>>>(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next, clen,
+                                       eps);
+  }
+#undef NGW_LSR
 }
 
 // ---------------------------------------------------------------------------
