@@ -38,8 +38,10 @@ WORKLOAD = dict(name="12-atom molecule, 30 occ + 90 empty, 600 ISDF points, 150 
 METRIC = "Sigma_c solves/s"
 # DRAM bytes (read + write) of one in-situ GEMM1 + GEMM2 pair of the 12-atom
 # workload from an ncu capture, by tile choice "bn1,var1,split1,bn2,var2"
-MEASURED_TRAFFIC = {"80,3,3,64,4": 15.37e6 + 28.84e6, "128,5,4,64,4": 15.92e6 + 28.84e6,
-                    "64,6,4,64,4": 15.89e6 + 28.84e6}
+# (GEMM1 [+ split-K reduce] + GEMM2, current kernels; ncu --metrics
+# dram__bytes_read.sum,dram__bytes_write.sum -k "regex:k_tc_gemm|k_splitk_reduce")
+MEASURED_TRAFFIC = {"128,3,4,64,4": 15.93e6 + 7.01e6 + 35.22e6, "128,5,4,64,4": 15.93e6 + 35.22e6,
+                    "64,6,4,64,4": 15.93e6 + 35.22e6, "64,4,1,80,7": 15.93e6 + 33.46e6}
 RYD = 13.60569193
 
 
