@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <numeric>
+#include <utility>
 #include <vector>
 
 #include <cusolverDn.h>
@@ -448,15 +449,32 @@ static int eig_lanczos_blas(ngw_session *s, int tamm_d, int m, double *V, double
 // FP64 Lanczos with full (twice-applied) reorthogonalisation on one vector.
 // Fills s->eig_* with Ritz values (descending), residual bounds and the Ritz
 // vectors of the top kmax pairs (device, ncv x kmax).
+// Temporary device buffers of one call, freed (stream-ordered) when the
+// scope ends, on the error paths too.
+struct ScopedBufs {
+  ngw_session *s;
+  std::vector<std::pair<void *, size_t>> held;
+  explicit ScopedBufs(ngw_session *s_) : s(s_) {}
+  ~ScopedBufs() {
+    for (auto &b : held) dfree(s, b.first, b.second);
+  }
+  int alloc(void **p, size_t bytes) {
+    NGW_TRY(dalloc(s, p, bytes));
+    held.push_back({*p, bytes});
+    return NGW_OK;
+  }
+};
+
 int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
   const int ncv = s->ncv;
   int m = std::min(msteps, ncv);
   kmax = std::min(kmax, m);
+  ScopedBufs tmp(s);
   double *V = nullptr, *w = nullptr, *hs = nullptr, *h = nullptr;
-  NGW_TRY(dalloc(s, (void **)&V, (size_t)ncv * (m + 1) * 8));
-  NGW_TRY(dalloc(s, (void **)&w, (size_t)ncv * 8));
-  NGW_TRY(dalloc(s, (void **)&hs, (size_t)ncv * 8));
-  NGW_TRY(dalloc(s, (void **)&h, (size_t)(m + 1) * 8));
+  NGW_TRY(tmp.alloc((void **)&V, (size_t)ncv * (m + 1) * 8));
+  NGW_TRY(tmp.alloc((void **)&w, (size_t)ncv * 8));
+  NGW_TRY(tmp.alloc((void **)&hs, (size_t)ncv * 8));
+  NGW_TRY(tmp.alloc((void **)&h, (size_t)(m + 1) * 8));
   std::vector<double> v0(ncv);
   uint64_t st = 0xD1B54A32D192ED03ull;
   double nrm = 0.0;
@@ -471,7 +489,7 @@ int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
   // The loop is asynchronous: alpha_j = <v_j, w> (first Gram-Schmidt pass)
   // and beta_{j+1} = ||w|| stay on the device and are read back once.
   double *dab = nullptr;   // alpha (m) then beta (m + 1)
-  NGW_TRY(dalloc(s, (void **)&dab, (size_t)(2 * m + 1) * 8));
+  NGW_TRY(tmp.alloc((void **)&dab, (size_t)(2 * m + 1) * 8));
   NGW_CUDA(cudaMemsetAsync(dab, 0, (size_t)(2 * m + 1) * 8, s->stream));
   double *dalpha = dab, *dbeta = dab + m;
   int rc = NGW_OK;
@@ -491,7 +509,6 @@ int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
     rc = NGW_ERR_CUDA;
   }
   cudaStreamSynchronize(s->stream);
-  dfree(s, dab, (size_t)(2 * m + 1) * 8);
   NGW_TRY(rc);
   // cut the run at the first negligible beta (invariant subspace found)
   int mm = m;
@@ -525,24 +542,22 @@ int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
   for (int c = 0; c < k; ++c)
     for (int r = 0; r < mm; ++r) Yk[(size_t)c * mm + r] = Y[(size_t)ord[c] * mm + r];
   double *dY = nullptr;
-  NGW_TRY(dalloc(s, (void **)&dY, (size_t)mm * k * 8));
+  NGW_TRY(tmp.alloc((void **)&dY, (size_t)mm * k * 8));
   const size_t ubytes = (size_t)ncv * std::max(k, 1) * 8;
   if (!s->eig_U || s->eig_U_bytes != ubytes) {   // captured graphs hold eig_U's address
     bump_generation(s);
     if (s->eig_U) dfree(s, s->eig_U, s->eig_U_bytes);
+    s->eig_U = nullptr;
+    s->eig_U_bytes = 0;
+    s->eig_tda = -1;
+    NGW_TRY(dalloc(s, (void **)&s->eig_U, ubytes));
     s->eig_U_bytes = ubytes;
-    NGW_TRY(dalloc(s, (void **)&s->eig_U, s->eig_U_bytes));
   }
   NGW_CUDA(cudaMemcpyAsync(dY, Yk.data(), (size_t)mm * k * 8, cudaMemcpyHostToDevice, s->stream));
   if (k > 0)
     NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, ncv, k, mm, &one, V, ncv, dY, mm, &zero,
                            s->eig_U, ncv));
   NGW_CUDA(cudaStreamSynchronize(s->stream));
-  dfree(s, dY, (size_t)mm * k * 8);
-  dfree(s, V, (size_t)ncv * (m + 1) * 8);
-  dfree(s, w, (size_t)ncv * 8);
-  dfree(s, hs, (size_t)ncv * 8);
-  dfree(s, h, (size_t)(m + 1) * 8);
   s->eig_k = k;
   s->eig_tda = tamm_d;
   return NGW_OK;

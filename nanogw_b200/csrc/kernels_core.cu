@@ -385,10 +385,18 @@ void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb,
                          double *b, int niter, const double *s, double *hs, int tamm_d,
                          int prescale_next, int *clen, double eps, cudaStream_t st) {
   if (nb <= 0) return;
+  // NGW_LSTEP=3 keeps the three-pass form at every size (comparison runs)
+  static const bool three_pass = [] {
+    const char *e = getenv("NGW_LSTEP");
+    return e && e[0] == '3';
+  }();
 #define NGW_LSR(E)                                                                                       \
   k_lanczos_step_reg<E><<<nb, LNT, 0, st>>>(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next, \
                                             clen, eps)
-  if (ncv <= 8 * LNT) {
+  if (three_pass) {
+    k_lanczos_step<<<nb, LNT, 0, st>>>(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next, clen,
+                                       eps);
+  } else if (ncv <= 8 * LNT) {
     NGW_LSR(8);
   } else if (ncv <= 16 * LNT) {
     NGW_LSR(16);
