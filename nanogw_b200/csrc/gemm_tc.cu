@@ -20,6 +20,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <cstdio>
@@ -1446,6 +1447,53 @@ static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, co
                      int ldv, double gamma, double alpha, double c0, double beta, int tda,
                      float *out32, double *out64, bool write_split, bool add_defl = false);
 
+// Admissible tile choices (N tile, kernel variant, split-K) of GEMM1 (c1) and
+// GEMM2 (c2) for the operator's shapes and nb chains: the tuner's candidates.
+struct TileC {
+  int bn, var, sp;
+};
+static void tune_candidates(const MixedOperator *op, int nb, std::vector<TileC> &c1, std::vector<TileC> &c2) {
+  c1.clear();
+  c2.clear();
+  const int total_kb1 = 3 * (op->cv_pad / BK);
+  const int tiles_m1 = op->mu_pad / BM;
+  for (int bn : kBNs) {
+    if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
+    const int waste = round_up(nb, bn) - nb;
+    if (waste * 8 > nb && bn != kBNs[0]) continue;     // at most 12.5% padding
+    for (int var = 0; var < 7; ++var) {
+      if (var == 1 && !has_shallow(bn)) continue;
+      if (var == 2 && !has_persistent(bn)) continue;
+      if ((var == 3 || var == 5) && !has_fused(bn)) continue;
+      if ((var == 4 || var == 6) && !has_fused2(bn)) continue;
+      if (!is_cluster_var(var)) {
+        c2.push_back({bn, var, 1});
+      } else {
+        const int kb2 = op->mu_k / BK;   // GEMM2 k-blocks (fused stages)
+        for (int sp : {2, 3, 4})
+          if (kb2 / sp >= 2) c2.push_back({bn, var, sp});
+      }
+      const int tiles = tiles_m1 * ((nb + bn - 1) / bn);
+      const int tkb = (var >= 2) ? total_kb1 / 3 : total_kb1;
+      for (int sp : {1, 2, 3, 4, 6, 8, 12, 16}) {
+        if (sp > 1 && tkb / sp < 3) break;
+        if (is_cluster_var(var) && (sp < 2 || sp > 8)) continue;
+        if (!is_cluster_var(var) && (size_t)tiles * sp * bn * BM * sizeof(float) > op->ws_bytes && sp > 1)
+          break;
+        if (tiles * sp > 4 * 148) break;
+        c1.push_back({bn, var, sp});
+      }
+    }
+  }
+  // variant 7 (GEMM2 only): Clenshaw operands staged by TMA
+  for (int bn : kBNs) {
+    if (!has_te(bn)) continue;
+    if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
+    if ((round_up(nb, bn) - nb) * 8 > nb && bn != kBNs[0]) continue;
+    c2.push_back({bn, 7, 1});
+  }
+}
+
 // Autotuner.  Candidates: every admissible (N tile, variant, split-K) for
 // GEMM1 and (N tile, variant) for GEMM2.  Each candidate is timed inside the
 // alternating GEMM1 -> GEMM2 sequence a Clenshaw step runs (so L2 holds what
@@ -1491,47 +1539,11 @@ static int autotune(ngw_session *s, int nb) {
     *ms = best;
     return NGW_OK;
   };
-  struct C1 { int bn, var, sp; };
-  struct C2 { int bn, var, sp; };
+  using C1 = TileC;
+  using C2 = TileC;
   std::vector<C1> c1;
   std::vector<C2> c2;
-  const int total_kb1 = 3 * (op->cv_pad / BK);
-  const int tiles_m1 = op->mu_pad / BM;
-  for (int bn : kBNs) {
-    if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
-    const int waste = round_up(nb, bn) - nb;
-    if (waste * 8 > nb && bn != kBNs[0]) continue;     // at most 12.5% padding
-    for (int var = 0; var < 7; ++var) {
-      if (var == 1 && !has_shallow(bn)) continue;
-      if (var == 2 && !has_persistent(bn)) continue;
-      if ((var == 3 || var == 5) && !has_fused(bn)) continue;
-      if ((var == 4 || var == 6) && !has_fused2(bn)) continue;
-      if (!is_cluster_var(var)) {
-        c2.push_back({bn, var, 1});
-      } else {
-        const int kb2 = op->mu_k / BK;   // GEMM2 k-blocks (fused stages)
-        for (int sp : {2, 3, 4})
-          if (kb2 / sp >= 2) c2.push_back({bn, var, sp});
-      }
-      const int tiles = tiles_m1 * ((nb + bn - 1) / bn);
-      const int tkb = (var >= 2) ? total_kb1 / 3 : total_kb1;
-      for (int sp : {1, 2, 3, 4, 6, 8, 12, 16}) {
-        if (sp > 1 && tkb / sp < 3) break;
-        if (is_cluster_var(var) && (sp < 2 || sp > 8)) continue;
-        if (!is_cluster_var(var) && (size_t)tiles * sp * bn * BM * sizeof(float) > op->ws_bytes && sp > 1)
-          break;
-        if (tiles * sp > 4 * 148) break;
-        c1.push_back({bn, var, sp});
-      }
-    }
-  }
-  // variant 7 (GEMM2 only): Clenshaw operands staged by TMA
-  for (int bn : kBNs) {
-    if (!has_te(bn)) continue;
-    if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
-    if ((round_up(nb, bn) - nb) * 8 > nb && bn != kBNs[0]) continue;
-    c2.push_back({bn, 7, 1});
-  }
+  tune_candidates(op, nb, c1, c2);
   // GEMM2 fixed while GEMM1 is tuned: the 64-wide (or smallest) non-fused tile
   C2 fix2 = c2.front();
   for (const C2 &c : c2)
@@ -1671,16 +1683,57 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
   if (op->tuned_nb != nb) {
     const TuneKey key{op->mu_pad, op->cv_pad, op->mu_k, op->kdef, op->n_isdf, op->ncv, nb, op->tda};
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune.find(key);
-    if (it != g_tune.end()) {
-      op->BN1 = it->second.bn1;
-      op->var1 = it->second.var1;
-      op->split1 = it->second.split1;
-      op->BN2 = it->second.bn2;
-      op->var2 = it->second.var2;
-      op->split2 = it->second.split2;
+    auto use = [&](const TuneVal &v) {
+      op->BN1 = v.bn1;
+      op->var1 = v.var1;
+      op->split1 = v.split1;
+      op->BN2 = v.bn2;
+      op->var2 = v.var2;
+      op->split2 = v.split2;
       op->tuned_nb = nb;
       return encode_chain_maps(op, op->BN1, op->BN2);
+    };
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return use(it->second);
+    // A request stream brings new shapes with almost every molecule: reuse
+    // the choice of the nearest tuned shape (same padded N_mu and K of GEMM2,
+    // deflation and TDA classes, N_cv and chain count within 25 %) when it is
+    // admissible here, instead of tuning again.  NGW_TUNE_EXACT=1 tunes every
+    // new shape.
+    static const bool exact = [] {
+      const char *e = getenv("NGW_TUNE_EXACT");
+      return e && e[0] == '1';
+    }();
+    if (!exact) {
+      const TuneVal *best = nullptr;
+      double best_d = 1e30;
+      for (const auto &kv : g_tune) {
+        const TuneKey &k = kv.first;
+        if (k.mu_pad != key.mu_pad || k.mu_k != key.mu_k || (k.kdef > 0) != (key.kdef > 0) || k.tda != key.tda)
+          continue;
+        const double rc = std::log((double)k.cv_pad / key.cv_pad), rn = std::log((double)k.nb / key.nb);
+        if (std::fabs(rc) > std::log(1.25) || std::fabs(rn) > std::log(1.25)) continue;
+        const double d = std::fabs(rc) + std::fabs(rn);
+        if (d < best_d) {
+          best_d = d;
+          best = &kv.second;
+        }
+      }
+      if (best) {
+        std::vector<TileC> c1, c2;
+        tune_candidates(op, nb, c1, c2);
+        const TuneVal v = *best;
+        const bool ok1 = std::any_of(c1.begin(), c1.end(), [&](const TileC &c) {
+          return c.bn == v.bn1 && c.var == v.var1 && c.sp == v.split1;
+        });
+        const bool ok2 = std::any_of(c2.begin(), c2.end(), [&](const TileC &c) {
+          return c.bn == v.bn2 && c.var == v.var2 && c.sp == v.split2;
+        });
+        if (ok1 && ok2) {
+          g_tune[key] = v;
+          return use(v);
+        }
+      }
     }
     NGW_TRY(autotune(s, nb));
     g_tune[key] = TuneVal{op->BN1, op->var1, op->split1, op->BN2, op->var2, op->split2};
