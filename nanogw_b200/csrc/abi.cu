@@ -54,6 +54,11 @@ void pool_free(ngw_session *s, void *p) {
   if (p) cudaFreeAsync(p, s->stream);
 }
 
+std::shared_mutex &gpu_quiet_lock(int device) {
+  static std::shared_mutex locks[64];
+  return locks[device & 63];
+}
+
 int dalloc(ngw_session *s, void **p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   cudaError_t e = pool_alloc(s, p, bytes);
@@ -1024,6 +1029,7 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
   SigmaJob J;
   NGW_TRY(sigma_prepare(J, s, p, e1));
   tm.mark("plan");
+  std::shared_lock<std::shared_mutex> busy(gpu_quiet_lock(s->device));   // no tuning meanwhile
   for (int q0 = 0; q0 < p->nqp; q0 += J.nq_blk) {
     NGW_TRY(sigma_block_setup(J, q0));
     std::vector<unsigned long long> key;
@@ -1091,8 +1097,12 @@ int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_s
     }
     return NGW_OK;
   };
-  const int rc = run_graphed(s0, key, region);
-  if (rc == NGW_OK) NGW_CUDA(cudaStreamSynchronize(s0->stream));
+  std::shared_lock<std::shared_mutex> busy(gpu_quiet_lock(s0->device));   // no tuning meanwhile
+  int rc = run_graphed(s0, key, region);
+  if (rc == NGW_OK && cudaStreamSynchronize(s0->stream) != cudaSuccess) {
+    set_error("ngw_sigma_lanczos_batch: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = NGW_ERR_CUDA;
+  }
   for (auto &e : ev) cudaEventDestroy(e);
   NGW_TRY(rc);
   for (int i = 0; i < count; ++i) NGW_TRY(sigma_finish(jobs[i], sigma_c[i]));

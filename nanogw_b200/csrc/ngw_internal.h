@@ -4,6 +4,7 @@
 #include <cuda_bf16.h>
 #include <cublas_v2.h>
 #include <atomic>
+#include <shared_mutex>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -107,6 +108,12 @@ namespace ngw {
 // allocation helpers (track session bytes)
 cudaError_t pool_alloc(ngw_session *s, void **p, size_t bytes);
 void pool_free(ngw_session *s, void *p);
+
+// Per-device lock that keeps the autotuner's timings clean: a Sigma_c solve
+// holds it shared from the launch of its device region until its results
+// are on the host; the autotuner holds it exclusively, so it times its
+// candidates without other sessions' solves running beside them.
+std::shared_mutex &gpu_quiet_lock(int device);
 
 // Raises a kernel's dynamic shared-memory limit to `bytes` on the current
 // device, once per device (the attribute is per device; `done` holds one bit
