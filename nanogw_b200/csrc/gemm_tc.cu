@@ -146,7 +146,10 @@ __device__ __forceinline__ float clen_out(const ClenCoef &k, float x, float z, f
 }
 
 // Stores of one Clenshaw output element (row m, chain n).
-__device__ __forceinline__ void clen_store(const EpiParams &ep, const ClenCoef &k, int m, int n, float o) {
+// The split S is read by the next GEMM1: stored with an evict_last policy
+// (keep) so it is still in L2 when that GEMM runs.
+__device__ __forceinline__ void clen_store(const EpiParams &ep, const ClenCoef &k, int m, int n, float o,
+                                           uint64_t keep) {
   if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = o;
   if (ep.out64) {
     double od = (double)o;
@@ -156,8 +159,8 @@ __device__ __forceinline__ void clen_store(const EpiParams &ep, const ClenCoef &
   if (ep.s_hi) {
     bf16 hi, lo;
     split_bf16(k.sc * o, hi, lo);
-    ep.s_hi[(size_t)n * ep.lds + m] = hi;
-    ep.s_lo[(size_t)n * ep.lds + m] = lo;
+    tc::st_b16_hint(ep.s_hi + (size_t)n * ep.lds + m, __bfloat16_as_ushort(hi), keep);
+    tc::st_b16_hint(ep.s_lo + (size_t)n * ep.lds + m, __bfloat16_as_ushort(lo), keep);
   }
 }
 
@@ -222,6 +225,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer: k-blocks of the concatenated segments ----
+    const bool b_once = ep.kind == EPI_SPLIT;
+    const uint64_t pol_b = tc::l2_evict_first();
     for (int i = 0; i < nkb; ++i) {
       const int s = i % STAGES;
       if (i >= STAGES) {
@@ -234,15 +239,23 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
       if (FUSED) {
         tc::tma_load_2d(sa, &tA_hi, bar, kbg * BK, m0);
         tc::tma_load_2d(sa + A_BYTES, &tA_lo, bar, kbg * BK, m0);
-        tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kbg * BK, n0);
-        tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kbg * BK, n0);
+        if (b_once) {   // GEMM1: S is not read again after this GEMM
+          tc::tma_load_2d_hint(sa + 2 * A_BYTES, &tB_hi, bar, kbg * BK, n0, pol_b);
+          tc::tma_load_2d_hint(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kbg * BK, n0, pol_b);
+        } else {
+          tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kbg * BK, n0);
+          tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kbg * BK, n0);
+        }
       } else {
         const int seg = kbg / ga.num_kb;
         const int kb = kbg - seg * ga.num_kb;
         const CUtensorMap *ta = (seg == 2) ? &tA_lo : &tA_hi;   // (hi,hi) (hi,lo) (lo,hi)
         const CUtensorMap *tb = (seg == 1) ? &tB_lo : &tB_hi;
         tc::tma_load_2d(sa, ta, bar, kb * BK, m0);
-        tc::tma_load_2d(sa + A_BYTES, tb, bar, kb * BK, n0);
+        if (b_once && seg > 0)   // last reads of S_lo (segment 1) and S_hi (segment 2)
+          tc::tma_load_2d_hint(sa + A_BYTES, tb, bar, kb * BK, n0, pol_b);
+        else
+          tc::tma_load_2d(sa + A_BYTES, tb, bar, kb * BK, n0);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -343,6 +356,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     cl.sync();
     const int ns = ga.nsplit;
     const ClenCoef kc = clen_coef(ep, csi);
+    const uint64_t l2keep = tc::l2_evict_last();
     for (int c = c_first; c < c_hi; c += 4 * cstep) {
       float cx[4], cb[4], cv[4];
 #pragma unroll
@@ -368,7 +382,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
           ep.out_lo[(size_t)n * ep.ldo + mm] = lo;
         } else {
           // the Clenshaw step of the EPI_CLENSHAW branch below, for one element
-          clen_store(ep, kc, mm, n, clen_out(kc, cx[j], acc, cv[j], cb[j]));
+          clen_store(ep, kc, mm, n, clen_out(kc, cx[j], acc, cv[j], cb[j]), l2keep);
         }
       }
     }
@@ -407,6 +421,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     // (TDA: R - c0, 2 z) in FP32 (clen_out); split((R^1/2 or 1) out).
     // 8-column chunks keep the register count low enough for 2 CTAs per SM.
     const ClenCoef kc = clen_coef(ep, si);
+    const uint64_t l2keep = tc::l2_evict_last();
     if (ep.ring) {
       // Operand ring in the stage memory the MMAs no longer need: per
       // warpgroup RS slots of one 8-column chunk (b_{k+1} | b_{k+2} | v,
@@ -423,15 +438,17 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
       const int nq = 2 * (ch_end - ch_begin);
       const int c_first = 16 * ch_begin;
       const uint32_t bytes = OP8 * (1u + (ep.b2 ? 1u : 0u) + (ep.v ? 1u : 0u));
+      const uint64_t pol_once = tc::l2_evict_first(), pol_keep = tc::l2_evict_last();
       auto issue = [&](int q) {
         const int r = q % RS;
         const uint32_t bar = tc::smem_u32(&ring_bar[wg][r]);
         const uint32_t dst = ring + (uint32_t)r * CHUNK;
         const int nc = n0 + c_first + 8 * q;
         tc::mbar_arrive_expect_tx(bar, bytes);
-        tc::tma_load_2d(dst, &tRx, bar, m0, nc);
-        if (ep.b2) tc::tma_load_2d(dst + OP8, &tRb2, bar, m0, nc);
-        if (ep.v) tc::tma_load_2d(dst + 2 * OP8, &tRv, bar, m0, nc);
+        // b_{k+1}, b_{k+2}: one more read each at most; v: read by every GEMM2 of the step
+        tc::tma_load_2d_hint(dst, &tRx, bar, m0, nc, pol_once);
+        if (ep.b2) tc::tma_load_2d_hint(dst + OP8, &tRb2, bar, m0, nc, pol_once);
+        if (ep.v) tc::tma_load_2d_hint(dst + 2 * OP8, &tRv, bar, m0, nc, pol_keep);
       };
       if (leader)
         for (int q = 0; q < nq && q < RS; ++q) issue(q);
@@ -456,7 +473,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             const float x = sl[j * BM];
             const float b2 = ep.b2 ? sl[OP8 / 4 + j * BM] : 0.f;
             const float v = ep.v ? sl[2 * (OP8 / 4) + j * BM] : 0.f;
-            clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2));
+            clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2), l2keep);
           }
         }
         asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");   // slot r read by the warpgroup
@@ -486,7 +503,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         if (j >= nj) break;
-        clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]));
+        clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]), l2keep);
       }
     }
   }
@@ -565,6 +582,7 @@ __global__ void __launch_bounds__(PTHREADS, 1)
   if (warp == 0) {
     if (lane == 0) {
       // ---- TMA producer ----
+      const uint64_t pol_b = tc::l2_evict_first();
       int it = 0;
       bool ok = true;
       for (int w = blockIdx.x; w < nwork && ok; w += gridDim.x) {
@@ -581,8 +599,13 @@ __global__ void __launch_bounds__(PTHREADS, 1)
           tc::mbar_arrive_expect_tx(bar, STAGE_BYTES);
           tc::tma_load_2d(sa, &tA_hi, bar, kb * BK, tm * BM);
           tc::tma_load_2d(sa + A_BYTES, &tA_lo, bar, kb * BK, tm * BM);
-          tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kb * BK, tn * BN);
-          tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kb * BK, tn * BN);
+          if (ep.kind == EPI_SPLIT) {   // GEMM1: S is not read again after this GEMM
+            tc::tma_load_2d_hint(sa + 2 * A_BYTES, &tB_hi, bar, kb * BK, tn * BN, pol_b);
+            tc::tma_load_2d_hint(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kb * BK, tn * BN, pol_b);
+          } else {
+            tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kb * BK, tn * BN);
+            tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kb * BK, tn * BN);
+          }
         }
       }
     }
@@ -674,6 +697,7 @@ __global__ void __launch_bounds__(PTHREADS, 1)
         }
       } else {
         const ClenCoef kc = clen_coef(ep, si);
+        const uint64_t l2keep = tc::l2_evict_last();
         for (int ch = ch_begin; ch < ch_end; ++ch) {
           const int c = ch * 8;
           float z[8];
@@ -697,7 +721,7 @@ __global__ void __launch_bounds__(PTHREADS, 1)
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             if (j >= nj) break;
-            clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]));
+            clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]), l2keep);
           }
         }
       }
@@ -780,9 +804,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // dependence on the MMAs), then the k-blocks of the product
     const uint32_t eb = tc::smem_u32(&epi_bar);
     tc::mbar_arrive_expect_tx(eb, OPER_BYTES * (1u + (has_b2 ? 1u : 0u) + (has_v ? 1u : 0u)));
-    tc::tma_load_2d(tc::smem_u32(eop), &tX, eb, m0, n0);
-    if (has_b2) tc::tma_load_2d(tc::smem_u32(eop) + OPER_BYTES, &tB2, eb, m0, n0);
-    if (has_v) tc::tma_load_2d(tc::smem_u32(eop) + 2 * OPER_BYTES, &tV, eb, m0, n0);
+    const uint64_t pol_once = tc::l2_evict_first(), pol_keep = tc::l2_evict_last();
+    tc::tma_load_2d_hint(tc::smem_u32(eop), &tX, eb, m0, n0, pol_once);
+    if (has_b2) tc::tma_load_2d_hint(tc::smem_u32(eop) + OPER_BYTES, &tB2, eb, m0, n0, pol_once);
+    if (has_v) tc::tma_load_2d_hint(tc::smem_u32(eop) + 2 * OPER_BYTES, &tV, eb, m0, n0, pol_keep);
     for (int i = 0; i < nkb; ++i) {
       const int st = i % STAGES;
       if (i >= STAGES) {
@@ -824,6 +849,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   const int ch_end = wg == 0 ? NCH0 : NCH;
   const bool mv = m < ep.Mv;
   const ClenCoef kc = clen_coef(ep, mv ? ep.s[m] : 0.0);
+  const uint64_t l2keep = tc::l2_evict_last();
   bool have = tc::mbar_wait(tc::smem_u32(&done_bar), 0, status) && nkb > 0;
   const bool have_ops = tc::mbar_wait(tc::smem_u32(&epi_bar), 0, status);
   tc::tc_fence_after();
@@ -846,7 +872,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const float x = eop[e];
       const float b2 = has_b2 ? eop[BM * BN + e] : 0.f;
       const float v = has_v ? eop[2 * BM * BN + e] : 0.f;
-      clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2));
+      clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2), l2keep);
     }
   }
 
