@@ -476,7 +476,10 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2), l2keep);
           }
         }
-        asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");   // slot r read by the warpgroup
+        if (wg == 0)   // slot r read by the warpgroup (literal barrier ids 1 / 2)
+          asm volatile("bar.sync 1, 128;" ::: "memory");
+        else
+          asm volatile("bar.sync 2, 128;" ::: "memory");
         if (leader && q + RS < nq) issue(q + RS);
       }
     } else
@@ -1096,12 +1099,13 @@ static bool has_fused(int BN) { return BN <= 128; }
 static bool has_fused2(int BN) { return BN <= 64; }
 
 // Supported N tiles (multiples of 16, <= 256).  Variant 0 ("deep"): one CTA
-// per SM with a long TMA ring; variant 1 ("shallow", N <= 160): 3-4 stages
+// per SM with a long TMA ring; variant 1 ("shallow", N <= 256; two stages
+// above N = 160): 3-4 stages
 // and <= 128 registers so two CTAs share an SM and one CTA's epilogue
 // overlaps the other's main loop.
 static const int kBNs[] = {32, 48, 64, 80, 96, 128, 144, 160, 192, 240, 256};
 
-static bool has_shallow(int BN) { return BN <= 160; }
+static bool has_shallow(int BN) { return BN <= 256; }
 
 static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorMap &a_lo,
                        const CUtensorMap &b_hi, const CUtensorMap &b_lo, int tiles_m, int tiles_n,
@@ -1188,6 +1192,10 @@ static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorM
       case 128: NGW_TC(128, 3, 2);
       case 144: NGW_TC(144, 3, 2);
       case 160: NGW_TC(160, 3, 2);
+      // wide tiles (fewer re-reads of A) at two stages: 2 x 48 KB + TMEM 256 columns per CTA
+      case 192: NGW_TC(192, 2, 2);
+      case 240: NGW_TC(240, 2, 2);
+      case 256: NGW_TC(256, 2, 2);
     }
   }
 #undef NGW_TC

@@ -84,7 +84,7 @@ def test_cluster_split_k_gemm2_within_1mev(tmp_path):
     assert np.all(r[:-2] < 1.0), r
 
 
-@pytest.mark.parametrize("gemm2", ["64,2", "64,3", "64,4", "32,4", "128,3", "32,6,4", "32,7", "64,7", "80,7"])
+@pytest.mark.parametrize("gemm2", ["64,2", "64,3", "64,4", "32,4", "128,3", "32,6,4", "32,7", "64,7", "80,7", "256,1"])
 def test_gemm2_variants_within_1mev(tmp_path, gemm2):
     """Every GEMM2 kernel form with the Clenshaw epilogue (persistent, fused
     one or two CTAs per SM, cluster split-K) keeps the QP energies within
