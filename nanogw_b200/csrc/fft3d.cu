@@ -199,6 +199,13 @@ int fft_coulomb_boxes(ngw_session *s, int n, int ncol, double *box, double2 *spe
     const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)e / (long double)n;
     hroot[e] = make_double2((double)cosl(ang), (double)sinl(ang));
   }
+  static std::atomic<unsigned long long> attr[5] = {};
+  const int mx = 200 * 1024;
+  NGW_CUDA(smem_limit_once(k_fft_rows_r2c, mx, attr[0]));
+  NGW_CUDA(smem_limit_once(k_fft_rows_c2r, mx, attr[1]));
+  NGW_CUDA(smem_limit_once(k_fft_strided<0>, mx, attr[2]));
+  NGW_CUDA(smem_limit_once(k_fft_strided<1>, mx, attr[3]));
+  NGW_CUDA(smem_limit_once(k_fft_strided<2>, mx, attr[4]));
   double2 *root = nullptr;
   NGW_TRY(dalloc(s, (void **)&root, (size_t)n * sizeof(double2)));
   int rc = NGW_OK;
@@ -215,13 +222,6 @@ int fft_coulomb_boxes(ngw_session *s, int n, int ncol, double *box, double2 *spe
     const int row_blocks = (int)std::min<size_t>((nrows + tl - 1) / tl, 148 * 16);
     const int tk = 8;
     const size_t smem_str = (size_t)2 * tk * n * sizeof(double2);
-    static std::atomic<unsigned long long> attr[5] = {};
-    const int mx = 200 * 1024;
-    NGW_CUDA(smem_limit_once(k_fft_rows_r2c, mx, attr[0]));
-    NGW_CUDA(smem_limit_once(k_fft_rows_c2r, mx, attr[1]));
-    NGW_CUDA(smem_limit_once(k_fft_strided<0>, mx, attr[2]));
-    NGW_CUDA(smem_limit_once(k_fft_strided<1>, mx, attr[3]));
-    NGW_CUDA(smem_limit_once(k_fft_strided<2>, mx, attr[4]));
     const dim3 rblk(64, tl), sblk(8, tk);
     const dim3 sgrid((h + tk - 1) / tk, ygrid((long long)ncol * n));
     const size_t colsz = (size_t)n * n * h;

@@ -1312,6 +1312,15 @@ struct MixedOperator {
 
 static int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
+// A temporary device buffer of one call, returned to the pool (stream-ordered)
+// when the scope ends, on error paths too.
+struct PoolTmp {
+  ngw_session *s;
+  void *p = nullptr;
+  explicit PoolTmp(ngw_session *s_) : s(s_) {}
+  ~PoolTmp() { pool_free(s, p); }
+};
+
 static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
   void *ptrs[] = {op->S_hi, op->S_lo, op->T_hi, op->T_lo, op->bb[0], op->bb[1], op->bb[2],
                   op->ws,   op->vperp, op->xo};
@@ -1405,9 +1414,10 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
   const double one = 1.0, zero = 0.0;
   if (kdef > 0) {
     // G = (C U) / s  in FP64: C applied to the Ritz vectors with the FP64 matvec
-    double *hs = nullptr, *CU = nullptr;
-    NGW_CUDA(pool_alloc(s, (void **)&hs, (size_t)s->ncv * kdef * 8));
-    NGW_CUDA(pool_alloc(s, (void **)&CU, (size_t)s->ncv * kdef * 8));
+    PoolTmp ths(s), tcu(s);
+    NGW_CUDA(pool_alloc(s, &ths.p, (size_t)s->ncv * kdef * 8));
+    NGW_CUDA(pool_alloc(s, &tcu.p, (size_t)s->ncv * kdef * 8));
+    double *hs = static_cast<double *>(ths.p), *CU = static_cast<double *>(tcu.p);
     launch_scale_rows(s->d_sqrtR, s->eig_U, s->ncv, hs, s->ncv, s->ncv, kdef, tda, st);
     int rc = matvec_f64_dev_pub(s, kdef, hs, CU, tda);
     if (rc == NGW_OK) {
@@ -1417,20 +1427,17 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
                                                           1.0, op->A1_hi, op->A1_lo, op->cv_pad,
                                                           s->n_isdf);
     }
-    NGW_CUDA(cudaStreamSynchronize(st));
-    pool_free(s, hs);
-    pool_free(s, CU);
     NGW_TRY(rc);
     NGW_CUDA(cudaGetLastError());
   }
   // D = M * C (FP64, cuBLAS), then split into A3[cv][mu] with the -U/(4s) columns
-  double *D = nullptr;
-  NGW_CUDA(pool_alloc(s, (void **)&D, (size_t)s->n_isdf * s->ncv * sizeof(double)));
+  PoolTmp td(s);
+  NGW_CUDA(pool_alloc(s, &td.p, (size_t)s->n_isdf * s->ncv * sizeof(double)));
+  double *D = static_cast<double *>(td.p);
   cublasStatus_t cst = cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, s->n_isdf, s->ncv,
                                    s->n_isdf, &one, s->d_M, s->n_isdf, s->d_C, s->n_isdf, &zero,
                                    D, s->n_isdf);
   if (cst != CUBLAS_STATUS_SUCCESS) {
-    pool_free(s, D);
     set_error("cublasDgemm (M*C) failed %d", (int)cst);
     return NGW_ERR_CUDA;
   }
@@ -1441,7 +1448,6 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
     NGW_CUDA(cudaGetLastError());
   }
   NGW_CUDA(cudaStreamSynchronize(st));
-  pool_free(s, D);
   NGW_TRY(make_tmap(&op->tA1hi, op->A1_hi, op->mu_pad, op->cv_pad, BM));
   NGW_TRY(make_tmap(&op->tA1lo, op->A1_lo, op->mu_pad, op->cv_pad, BM));
   NGW_TRY(make_tmap(&op->tA3hi, op->A3_hi, op->cv_pad, op->mu_k, BM));
