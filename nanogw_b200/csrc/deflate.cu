@@ -117,7 +117,7 @@ __device__ __forceinline__ double eig_warp_sum_grid(const double *p, int G) {
   return q;
 }
 
-__global__ void __launch_bounds__(EIG_NT, 1) k_eig_lanczos(EigLanczosArgs a) {
+__global__ void __launch_bounds__(EIG_NT, 2) k_eig_lanczos(EigLanczosArgs a) {
   extern __shared__ double sh[];   // max(n, m + 1) doubles
   __shared__ double red[EIG_NT / 32];
   __shared__ double xs[EIG_NT];                  // a chunk of (R^1/2 or 1) v_j
