@@ -146,10 +146,7 @@ __device__ __forceinline__ float clen_out(const ClenCoef &k, float x, float z, f
 }
 
 // Stores of one Clenshaw output element (row m, chain n).
-// The split S is read by the next GEMM1: stored with an evict_last policy
-// (keep) so it is still in L2 when that GEMM runs.
-__device__ __forceinline__ void clen_store(const EpiParams &ep, const ClenCoef &k, int m, int n, float o,
-                                           uint64_t keep) {
+__device__ __forceinline__ void clen_store(const EpiParams &ep, const ClenCoef &k, int m, int n, float o) {
   if (ep.out32) ep.out32[(size_t)n * ep.ldx + m] = o;
   if (ep.out64) {
     double od = (double)o;
@@ -159,8 +156,8 @@ __device__ __forceinline__ void clen_store(const EpiParams &ep, const ClenCoef &
   if (ep.s_hi) {
     bf16 hi, lo;
     split_bf16(k.sc * o, hi, lo);
-    tc::st_b16_hint(ep.s_hi + (size_t)n * ep.lds + m, __bfloat16_as_ushort(hi), keep);
-    tc::st_b16_hint(ep.s_lo + (size_t)n * ep.lds + m, __bfloat16_as_ushort(lo), keep);
+    ep.s_hi[(size_t)n * ep.lds + m] = hi;
+    ep.s_lo[(size_t)n * ep.lds + m] = lo;
   }
 }
 
@@ -225,8 +222,6 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer: k-blocks of the concatenated segments ----
-    const bool b_once = ep.kind == EPI_SPLIT;
-    const uint64_t pol_b = tc::l2_evict_first();
     for (int i = 0; i < nkb; ++i) {
       const int s = i % STAGES;
       if (i >= STAGES) {
@@ -239,23 +234,15 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
       if (FUSED) {
         tc::tma_load_2d(sa, &tA_hi, bar, kbg * BK, m0);
         tc::tma_load_2d(sa + A_BYTES, &tA_lo, bar, kbg * BK, m0);
-        if (b_once) {   // GEMM1: S is not read again after this GEMM
-          tc::tma_load_2d_hint(sa + 2 * A_BYTES, &tB_hi, bar, kbg * BK, n0, pol_b);
-          tc::tma_load_2d_hint(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kbg * BK, n0, pol_b);
-        } else {
-          tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kbg * BK, n0);
-          tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kbg * BK, n0);
-        }
+        tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kbg * BK, n0);
+        tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kbg * BK, n0);
       } else {
         const int seg = kbg / ga.num_kb;
         const int kb = kbg - seg * ga.num_kb;
         const CUtensorMap *ta = (seg == 2) ? &tA_lo : &tA_hi;   // (hi,hi) (hi,lo) (lo,hi)
         const CUtensorMap *tb = (seg == 1) ? &tB_lo : &tB_hi;
         tc::tma_load_2d(sa, ta, bar, kb * BK, m0);
-        if (b_once && seg > 0)   // last reads of S_lo (segment 1) and S_hi (segment 2)
-          tc::tma_load_2d_hint(sa + A_BYTES, tb, bar, kb * BK, n0, pol_b);
-        else
-          tc::tma_load_2d(sa + A_BYTES, tb, bar, kb * BK, n0);
+        tc::tma_load_2d(sa + A_BYTES, tb, bar, kb * BK, n0);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -356,7 +343,6 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     cl.sync();
     const int ns = ga.nsplit;
     const ClenCoef kc = clen_coef(ep, csi);
-    const uint64_t l2keep = tc::l2_evict_last();
     for (int c = c_first; c < c_hi; c += 4 * cstep) {
       float cx[4], cb[4], cv[4];
 #pragma unroll
@@ -382,7 +368,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
           ep.out_lo[(size_t)n * ep.ldo + mm] = lo;
         } else {
           // the Clenshaw step of the EPI_CLENSHAW branch below, for one element
-          clen_store(ep, kc, mm, n, clen_out(kc, cx[j], acc, cv[j], cb[j]), l2keep);
+          clen_store(ep, kc, mm, n, clen_out(kc, cx[j], acc, cv[j], cb[j]));
         }
       }
     }
@@ -421,7 +407,6 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     // (TDA: R - c0, 2 z) in FP32 (clen_out); split((R^1/2 or 1) out).
     // 8-column chunks keep the register count low enough for 2 CTAs per SM.
     const ClenCoef kc = clen_coef(ep, si);
-    const uint64_t l2keep = tc::l2_evict_last();
     if (ep.ring) {
       // Operand ring in the stage memory the MMAs no longer need: per
       // warpgroup RS slots of one 8-column chunk (b_{k+1} | b_{k+2} | v,
@@ -473,7 +458,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
             const float x = sl[j * BM];
             const float b2 = ep.b2 ? sl[OP8 / 4 + j * BM] : 0.f;
             const float v = ep.v ? sl[2 * (OP8 / 4) + j * BM] : 0.f;
-            clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2), l2keep);
+            clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2));
           }
         }
         if (wg == 0)   // slot r read by the warpgroup (literal barrier ids 1 / 2)
@@ -506,7 +491,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         if (j >= nj) break;
-        clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]), l2keep);
+        clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]));
       }
     }
   }
@@ -585,7 +570,6 @@ __global__ void __launch_bounds__(PTHREADS, 1)
   if (warp == 0) {
     if (lane == 0) {
       // ---- TMA producer ----
-      const uint64_t pol_b = tc::l2_evict_first();
       int it = 0;
       bool ok = true;
       for (int w = blockIdx.x; w < nwork && ok; w += gridDim.x) {
@@ -602,13 +586,8 @@ __global__ void __launch_bounds__(PTHREADS, 1)
           tc::mbar_arrive_expect_tx(bar, STAGE_BYTES);
           tc::tma_load_2d(sa, &tA_hi, bar, kb * BK, tm * BM);
           tc::tma_load_2d(sa + A_BYTES, &tA_lo, bar, kb * BK, tm * BM);
-          if (ep.kind == EPI_SPLIT) {   // GEMM1: S is not read again after this GEMM
-            tc::tma_load_2d_hint(sa + 2 * A_BYTES, &tB_hi, bar, kb * BK, tn * BN, pol_b);
-            tc::tma_load_2d_hint(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kb * BK, tn * BN, pol_b);
-          } else {
-            tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kb * BK, tn * BN);
-            tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kb * BK, tn * BN);
-          }
+          tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kb * BK, tn * BN);
+          tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kb * BK, tn * BN);
         }
       }
     }
@@ -700,7 +679,6 @@ __global__ void __launch_bounds__(PTHREADS, 1)
         }
       } else {
         const ClenCoef kc = clen_coef(ep, si);
-        const uint64_t l2keep = tc::l2_evict_last();
         for (int ch = ch_begin; ch < ch_end; ++ch) {
           const int c = ch * 8;
           float z[8];
@@ -724,7 +702,7 @@ __global__ void __launch_bounds__(PTHREADS, 1)
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             if (j >= nj) break;
-            clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]), l2keep);
+            clen_store(ep, kc, m, nbase + j, clen_out(kc, xv[j], z[j], vf[j], b2v[j]));
           }
         }
       }
@@ -852,7 +830,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   const int ch_end = wg == 0 ? NCH0 : NCH;
   const bool mv = m < ep.Mv;
   const ClenCoef kc = clen_coef(ep, mv ? ep.s[m] : 0.0);
-  const uint64_t l2keep = tc::l2_evict_last();
   bool have = tc::mbar_wait(tc::smem_u32(&done_bar), 0, status) && nkb > 0;
   const bool have_ops = tc::mbar_wait(tc::smem_u32(&epi_bar), 0, status);
   tc::tc_fence_after();
@@ -875,7 +852,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const float x = eop[e];
       const float b2 = has_b2 ? eop[BM * BN + e] : 0.f;
       const float v = has_v ? eop[2 * BM * BN + e] : 0.f;
-      clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2), l2keep);
+      clen_store(ep, kc, m, nbase + j, clen_out(kc, x, z[j], v, b2));
     }
   }
 
@@ -1593,8 +1570,8 @@ static int autotune(ngw_session *s, int nb) {
   op->BN2 = fix2.bn;
   op->var2 = fix2.var;
   op->split2 = fix2.sp;
-  // Two stages per GEMM: every candidate briefly (one warm pair, the mean of
-  // three timed pairs), then the best-of-two trials of time_pair for the
+  // Two stages per GEMM: every candidate briefly (one warm pair and one timed
+  // pair, the mean of three more below 0.5 ms), then time_pair for the
   // `refine` fastest (NGW_TUNE_REFINE, default 6; 0 = every candidate).
   static const int refine = [] {
     const char *e = getenv("NGW_TUNE_REFINE");
@@ -1603,7 +1580,9 @@ static int autotune(ngw_session *s, int nb) {
   auto time_quick = [&](float *ms) -> int {
     NGW_TRY(g1());
     NGW_TRY(g2());
-    return timed(3, ms);
+    NGW_TRY(timed(1, ms));
+    if (*ms < 0.5f) NGW_TRY(timed(3, ms));   // short pairs: the mean of three
+    return NGW_OK;
   };
   auto pick = [&](int nc, auto set, const char *name) -> int {
     std::vector<std::pair<float, int>> quick;
