@@ -1,7 +1,7 @@
-"""The Lanczos step with each chain's vectors held in registers and the
-three-pass form (NGW_LSTEP=3, the form used above N_cv = 8192) run the same
-arithmetic in the same order: identical alpha, beta and Sigma_c, in the
-FP64 and in the mixed-precision path."""
+"""The Lanczos step with each chain's vectors held in registers (forced with
+NGW_LSTEP=r; by default used for 4096 < N_cv <= 8192) and the three-pass form
+(NGW_LSTEP=3) run the same arithmetic in the same order: identical alpha,
+beta and Sigma_c, in the FP64 and in the mixed-precision path."""
 import os
 import subprocess
 import sys
@@ -40,6 +40,6 @@ def _run(tmp_path, name, **env_extra):
 
 
 def test_register_and_three_pass_step_identical(tmp_path):
-    a = _run(tmp_path, "reg")
+    a = _run(tmp_path, "reg", NGW_LSTEP="r")
     b = _run(tmp_path, "pass3", NGW_LSTEP="3")
     assert np.array_equal(a, b)
