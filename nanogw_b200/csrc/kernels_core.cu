@@ -506,7 +506,7 @@ void launch_sigma_spectra(const double *a, const double *b, int niter, int nchai
       a, b, niter, nchain, e1, chain_band, chain_qp, zz0, de, nen, ecuts, nval, S, clen);
 }
 
-// Sigma_c(i, iq) (+)= sum_n in band order of
+// Sigma_c(i, iq) (+)= sum over the bands n of
 //   non-TDA: (S_n(0) - S_n(ezz)) * eta_n * 2 * pnorm2_n / ezz
 //   TDA:     -S_n(ezz) * eta_n * sqrt(2) * pnorm2_n   (sqrt(2) in single precision, as 2.0**0.5)
 // (calculate_sigma_lanczos_lowcomsym.F90:736-745).  The chain of (QP iq,
