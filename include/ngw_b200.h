@@ -123,6 +123,13 @@ typedef struct {
                               (chain = iq*nbands_sum + n-1); NULL = niter for every chain */
   double early_exit_eps;   /* > 0: a chain stops when |b_k| < eps (convergence mask, as
                               shared/lanczos_spectra.f90:24,58); 0 = never (lowcomsym) */
+  int reorth;              /* 1: full reorthogonalisation of every chain (classical Gram-Schmidt
+                              against all its earlier Lanczos vectors, applied twice, FP64); the
+                              reference recurrence has none (shared/lanczos_spectra_lowcomsym.F90
+                              :117-166), so 0 reproduces it.  The Krylov bases take
+                              chains x (niter+1) x ncv x 8 bytes: the QP states are blocked so
+                              they fit NGW_REORTH_MAX_GB (default 40 % of free device memory);
+                              NGW_ERR_BUDGET when one QP state does not fit.  niter <= 6000. */
 } ngw_sigma_params;
 
 /* ngw_lanczos_spectra_isdf with per-chain lengths and a convergence mask:

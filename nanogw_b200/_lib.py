@@ -70,7 +70,7 @@ class SigmaParams(ctypes.Structure):
         ("nen", _I), ("deltae", _D), ("ecuts", _D), ("niter", _I), ("npoly", _I),
         ("polynomial", _P), ("tamm_d", _I), ("nval", _I), ("nqp", _I), ("qp_bands", _P),
         ("nbands_sum", _I), ("block_chains", _I), ("cheb_lo", _D), ("cheb_hi", _D),
-        ("chain_niter", _P), ("early_exit_eps", _D),
+        ("chain_niter", _P), ("early_exit_eps", _D), ("reorth", _I),
     ]
 
 

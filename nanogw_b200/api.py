@@ -155,7 +155,7 @@ class Session:
 
     def _sigma_params(self, e1, nval, qp_bands, nen, deltae, ecuts, niter, polynomial, tamm_d=False,
                       nbands_sum=0, block_chains=0, cheb=(0.0, 0.0), chain_niter=None,
-                      early_exit_eps=0.0):
+                      early_exit_eps=0.0, reorth=False):
         """ngw_sigma_params for one request, with the arrays it points to."""
         e = np.ascontiguousarray(e1, dtype=np.float64)
         qp = np.ascontiguousarray(qp_bands, dtype=np.int32)
@@ -167,7 +167,7 @@ class Session:
                           nval=int(nval), nqp=len(qp), qp_bands=_p(qp), nbands_sum=int(nbands_sum),
                           block_chains=int(block_chains), cheb_lo=float(cheb[0]),
                           cheb_hi=float(cheb[1]), chain_niter=None,
-                          early_exit_eps=float(early_exit_eps))
+                          early_exit_eps=float(early_exit_eps), reorth=int(bool(reorth)))
         ln = None
         if chain_niter is not None:
             ln = np.ascontiguousarray(chain_niter, dtype=np.int32).reshape(-1)
@@ -179,13 +179,14 @@ class Session:
 
     def calculate_sigma_lanczos(self, e1, nval, qp_bands, nen, deltae, ecuts, niter, polynomial,
                                 tamm_d=False, nbands_sum=0, block_chains=0, cheb=(0.0, 0.0),
-                                return_ab=False, chain_niter=None, early_exit_eps=0.0):
+                                return_ab=False, chain_niter=None, early_exit_eps=0.0, reorth=False):
         """Sigma_c(omega) (Ry) for each QP band: complex array (nen, nqp).
         chain_niter: optional (nqp, nbands_sum) per-chain Lanczos lengths
-        (1..niter); early_exit_eps > 0 stops a chain when |b_k| < eps."""
+        (1..niter); early_exit_eps > 0 stops a chain when |b_k| < eps;
+        reorth: full reorthogonalisation of every chain (not in the reference)."""
         prm, e, sig, keep, nbs = self._sigma_params(e1, nval, qp_bands, nen, deltae, ecuts, niter,
                                                     polynomial, tamm_d, nbands_sum, block_chains,
-                                                    cheb, chain_niter, early_exit_eps)
+                                                    cheb, chain_niter, early_exit_eps, reorth)
         a = b = None
         if return_ab:
             a = np.zeros((niter, nbs * sig.shape[1]), order="F")

@@ -103,8 +103,20 @@ int check_status(ngw_session *s) {
   if (h != DEV_OK) {
     int z = 0;
     cudaMemcpy(s->d_status, &z, sizeof(int), cudaMemcpyHostToDevice);
-    set_error("device status %d (%s)", h, h == DEV_TIMEOUT ? "bounded wait timed out" : "index check");
-    return h == DEV_TIMEOUT ? NGW_ERR_TIMEOUT : NGW_ERR_CUDA;
+    if (h == DEV_TIMEOUT) {
+      // a GEMM CTA gave up with its own copies possibly in flight: the
+      // kernel's state is not defined afterwards, so the session stops here
+      s->poisoned = true;
+      set_error("device status %d: a tensor-core GEMM's bounded wait timed out; the session refuses "
+                "further work (destroy and create it again)", h);
+      return NGW_ERR_TIMEOUT;
+    }
+    if (h == DEV_BARRIER_TIMEOUT) {
+      set_error("device status %d: a grid barrier's bounded wait timed out", h);
+      return NGW_ERR_TIMEOUT;
+    }
+    set_error("device status %d (index check)", h);
+    return NGW_ERR_CUDA;
   }
   return NGW_OK;
 }
@@ -144,7 +156,8 @@ static bool all_finite(const double *x, size_t n) {
 enum {
   SL_IN = 0, SL_OUT, SL_HS, SL_T1, SL_T2, SL_Z, SL_VEC, SL_WVEC, SL_TMP, SL_A, SL_B, SL_ZZ,
   SL_SPEC, SL_CMN, SL_CM, SL_P, SL_P2, SL_PN2, SL_PN, SL_CHB, SL_CHQ, SL_E1, SL_ZZ0, SL_SIG,
-  SL_KR, SL_KC, SL_KM, SL_B1, SL_B2, SL_QPW, SL_QPIO, SL_SPECS, SL_CLEN, SL_LEN, SL_SLOT, SL_NUM
+  SL_KR, SL_KC, SL_KM, SL_B1, SL_B2, SL_QPW, SL_QPIO, SL_SPECS, SL_CLEN, SL_LEN, SL_SLOT, SL_BASIS,
+  SL_NUM
 };
 
 // ---------------------------------------------------------------------------
@@ -219,23 +232,35 @@ static int apply_poly(ngw_session *s, const PolyPlan &pp, int nb, const double *
 // 0 .. nact[k]-1 only.
 static int lanczos_dev(ngw_session *s, const PolyPlan &pp, int nb, int niter, double *V,
                        double *W, double *hs, double *tmp, double *a, double *b, int *clen,
-                       double eps, const std::vector<int> *nact) {
-  // wvec = p(H) vec
-  NGW_TRY(apply_poly(s, pp, nb, V, hs, W));
-  launch_lanczos_first(W, V, s->ncv, nb, a, b, niter, clen, eps, s->stream);
+                       double eps, const std::vector<int> *nact, double *basis = nullptr,
+                       long long ldb = 0) {
   // the scaled copy hs feeds only the FP64 path's first DGEMM
   double *hsn = (s->precision == NGW_PREC_MIXED) ? nullptr : hs;
   auto active = [&](int k) { return nact ? (*nact)[k] : nb; };
-  if (niter >= 2)
-    launch_lanczos_prescale(W, V, s->ncv, active(1), 1, b, niter, s->d_sqrtR, hsn, pp.tamm_d, clen,
-                            s->stream);
+  if (basis) launch_basis_init(V, s->ncv, nb, basis, ldb, s->stream);
+  // wvec = p(H) vec
+  NGW_TRY(apply_poly(s, pp, nb, V, hs, W));
+  if (basis) {
+    // first step with Gram-Schmidt against v_0, rescale into v_1
+    launch_lanczos_reorth_step(W, V, nullptr, s->ncv, nb, 0, a, b, niter, s->d_sqrtR, hsn, pp.tamm_d,
+                               niter >= 2 ? 1 : 0, clen, eps, basis, ldb, s->stream);
+  } else {
+    launch_lanczos_first(W, V, s->ncv, nb, a, b, niter, clen, eps, s->stream);
+    if (niter >= 2)
+      launch_lanczos_prescale(W, V, s->ncv, active(1), 1, b, niter, s->d_sqrtR, hsn, pp.tamm_d, clen,
+                              s->stream);
+  }
   double *vec = W, *wvec = V;   // roles after the swap
   for (int k = 1; k < niter; ++k) {
     const int nk = active(k);
     if (nk <= 0) break;
     NGW_TRY(apply_poly(s, pp, nk, vec, hs, tmp));
-    launch_lanczos_step(wvec, vec, tmp, s->ncv, nk, k, a, b, niter, s->d_sqrtR, hsn, pp.tamm_d,
-                        (k + 1 < niter) ? 1 : 0, clen, eps, s->stream);
+    if (basis)
+      launch_lanczos_reorth_step(wvec, vec, tmp, s->ncv, nk, k, a, b, niter, s->d_sqrtR, hsn, pp.tamm_d,
+                                 (k + 1 < niter) ? 1 : 0, clen, eps, basis, ldb, s->stream);
+    else
+      launch_lanczos_step(wvec, vec, tmp, s->ncv, nk, k, a, b, niter, s->d_sqrtR, hsn, pp.tamm_d,
+                          (k + 1 < niter) ? 1 : 0, clen, eps, s->stream);
     if (k + 1 < niter) {
       double *t = vec;
       vec = wvec;
@@ -279,6 +304,10 @@ static int need_op(ngw_session *s) {
   if (!s) {
     set_error("null session");
     return NGW_ERR_ARG;
+  }
+  if (s->poisoned) {
+    set_error("a tensor-core GEMM of this session timed out earlier; destroy and create the session again");
+    return NGW_ERR_STATE;
   }
   if (!s->have_isdf || !s->have_pairs) {
     set_error("ISDF operator or pair list not set");
@@ -444,6 +473,8 @@ struct SigmaJob {
   PolyPlan pp;
   double de = 0.0;
   double *de1, *zz0, *sig, *cmn, *cm, *P, *P2, *pn2, *pn, *V, *W, *hs, *tmp, *a, *b, *S;
+  double *basis = nullptr;     // Krylov bases (reorth): chain j at basis + j * ldb
+  long long ldb = 0;
   int *chb, *chq, *clen, *dlen, *dslot;
   // current block
   int q0 = 0, nq = 0, nb = 0;
@@ -498,6 +529,26 @@ static int sigma_prepare(SigmaJob &J, ngw_session *s, const ngw_sigma_params *p,
   // chain blocking: whole QP states per block
   J.nq_blk = p->nqp;
   if (p->block_chains > 0) J.nq_blk = std::max(1, std::min(p->nqp, p->block_chains / nbsum));
+  if (p->reorth) {
+    // the Krylov bases of a block's chains must fit the cap: fewer QP states
+    // per block when they do not
+    if (p->niter > 6000) {
+      set_error("reorth: niter %d > 6000", p->niter);
+      return NGW_ERR_ARG;
+    }
+    size_t freeb = 0, totb = 0;
+    NGW_CUDA(cudaMemGetInfo(&freeb, &totb));
+    double cap = 0.4 * (double)freeb;
+    if (const char *e = getenv("NGW_REORTH_MAX_GB")) cap = atof(e) * 1073741824.0;
+    const double per_state = (double)nbsum * (p->niter + 1) * (double)s->ncv * 8.0;
+    const int fit = (int)std::min<double>(p->nqp, std::floor(cap / per_state));
+    if (fit < 1) {
+      set_error("reorth: the Krylov bases of one QP state (%.3g bytes) exceed the cap (%.3g bytes)",
+                per_state, cap);
+      return NGW_ERR_BUDGET;
+    }
+    J.nq_blk = std::min(J.nq_blk, fit);
+  }
   const int nb_max = J.nq_blk * nbsum, ncv = J.ncv, n = J.n, nen = J.nen, niter = J.niter;
   J.nb_max = nb_max;
   NGW_TRY(scratch(s, SL_E1, (size_t)s->nmem * 8, (void **)&J.de1));
@@ -521,6 +572,10 @@ static int sigma_prepare(SigmaJob &J, ngw_session *s, const ngw_sigma_params *p,
   NGW_TRY(scratch(s, SL_CLEN, (size_t)nb_max * 4, (void **)&J.clen));
   NGW_TRY(scratch(s, SL_LEN, (size_t)nb_max * 4, (void **)&J.dlen));
   NGW_TRY(scratch(s, SL_SLOT, (size_t)nb_max * 4, (void **)&J.dslot));
+  if (p->reorth) {
+    J.ldb = (long long)(niter + 1) * ncv;
+    NGW_TRY(scratch(s, SL_BASIS, (size_t)nb_max * (size_t)J.ldb * 8, (void **)&J.basis));
+  }
   if (s->precision == NGW_PREC_MIXED) NGW_TRY(mixed_prepare_chains(s, nb_max, 0, 0, 0));
   NGW_CUDA(cudaMemcpyAsync(J.de1, e1, (size_t)s->nmem * 8, cudaMemcpyHostToDevice, s->stream));
   // energy grid origin per QP state: en0 = e1(m) - deltae/2, step deltae/(nen-1)
@@ -595,7 +650,7 @@ static int sigma_region(SigmaJob &J) {
   launch_lanczos_init(J.P2, ncv, J.pn, J.V, J.hs, s->d_sqrtR, ncv, nb, tamm_d, J.b, niter, J.dlen, J.clen,
                       s->stream);
   NGW_TRY(lanczos_dev(s, J.pp, nb, niter, J.V, J.W, J.hs, J.tmp, J.a, J.b, J.clen, p->early_exit_eps,
-                      J.len ? &J.nact : nullptr));
+                      J.len ? &J.nact : nullptr, J.basis, J.ldb));
   launch_sigma_spectra(J.a, J.b, niter, nb, J.de1, J.chb + nb, J.chq, J.zz0, J.de, J.nen, p->ecuts, p->nval,
                        J.S, J.clen, s->stream);
   launch_sigma_reduce(J.S, J.pn2, J.de1, J.chb + nb, J.zz0 + J.q0, J.de, J.nen, p->ecuts, p->nval, J.nbsum,
@@ -615,7 +670,8 @@ static void sigma_key(const SigmaJob &J, std::vector<unsigned long long> &key) {
       (unsigned long long)p->nval, (unsigned long long)J.nbsum, (unsigned long long)J.nq,
       (unsigned long long)J.q0, (unsigned long long)J.pp.kdef, dbits(p->ecuts), dbits(J.de),
       dbits(J.pp.c0), dbits(J.pp.c1), s->gen, dbits(p->early_exit_eps),
-      (unsigned long long)(J.len != nullptr)};
+      (unsigned long long)(J.len != nullptr), (unsigned long long)(uintptr_t)J.basis,
+      (unsigned long long)J.ldb};
   key.insert(key.end(), std::begin(head), std::end(head));
   if (J.len) key.insert(key.end(), J.nact.begin(), J.nact.end());
   for (double c : J.pp.poly) key.push_back(dbits(c));

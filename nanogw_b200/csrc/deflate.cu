@@ -64,27 +64,36 @@ struct EigLanczosArgs {
   double *alpha, *beta;    // (m), (m + 1)
   unsigned *bar;           // barrier arrival counter, zero at launch
   int *status;
+  long long wait_cycles;   // bound of each barrier wait (SM clock cycles)
+  int skip_cta;            // test hook: this CTA skips its first arrival (-1: none)
 };
 
-// Grid barrier with a bounded wait: returns false (and sets *status = 2) when
-// the other CTAs have not all arrived within ~1 s of clock cycles.  The
-// counter only grows (zero at launch): thread 0 of each CTA adds 1 after a
-// gpu-scope fence (the CTA's writes, ordered by the CTA barrier, are released
-// with it) and polls with acquire loads until the count reaches its epoch
-// times the grid size.  No atomic result and no second release are waited for.
-__device__ __forceinline__ bool eig_grid_sync(unsigned *cnt, unsigned &target, int *status, int *sh_ok) {
+// Grid barrier with a bounded wait: returns false (and sets *status =
+// DEV_BARRIER_TIMEOUT) when the other CTAs have not all arrived within
+// `wait_cycles` SM clock cycles (about one second by default); every CTA then
+// leaves the kernel, so nothing of it stays in flight.  The counter only
+// grows (zero at launch): thread 0 of each CTA adds 1 after a gpu-scope fence
+// (the CTA's writes, ordered by the CTA barrier, are released with it) and
+// polls with acquire loads until the count reaches its epoch times the grid
+// size.  No atomic result and no second release are waited for.  `skip`
+// (a test hook) withholds this CTA's arrival at the first barrier, so that
+// every CTA's wait runs out.
+__device__ __forceinline__ bool eig_grid_sync(unsigned *cnt, unsigned &target, int *status, int *sh_ok,
+                                              long long wait_cycles, int skip_cta) {
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
+    const bool arrive = !(skip_cta == (int)blockIdx.x && target == 0);
     target += gridDim.x;
-    asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
+    if (arrive)
+      asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
     const long long t0 = clock64();
     while (true) {
       unsigned c;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(cnt) : "memory");
       if ((int)(c - target) >= 0) break;
-      if (clock64() - t0 > (1LL << 31)) {
-        atomicExch(status, 2);
+      if (clock64() - t0 > wait_cycles) {
+        atomicExch(status, (int)DEV_BARRIER_TIMEOUT);
         ok = 0;
         break;
       }
@@ -172,7 +181,7 @@ __global__ void __launch_bounds__(EIG_NT, 2) k_eig_lanczos(EigLanczosArgs a) {
       }
       if (i < n) a.pA[(size_t)ca * n + i] = acc;
     }
-    if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+    if (!eig_grid_sync(a.bar, target, a.status, &sh_ok, a.wait_cycles, a.skip_cta)) return;
     // ---- B: t2 partials ----
     for (int it = b; it < a.RG * a.KB; it += G) {
       const int rg = it % a.RG, kb = it / a.RG;
@@ -193,7 +202,7 @@ __global__ void __launch_bounds__(EIG_NT, 2) k_eig_lanczos(EigLanczosArgs a) {
         a.pB[(size_t)kb * n + i] = acc;
       }
     }
-    if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+    if (!eig_grid_sync(a.bar, target, a.status, &sh_ok, a.wait_cycles, a.skip_cta)) return;
     // ---- C: w = H v_j ----
     for (int i = tid; i < n; i += EIG_NT) {
       double t = 0.0;
@@ -238,7 +247,7 @@ __global__ void __launch_bounds__(EIG_NT, 2) k_eig_lanczos(EigLanczosArgs a) {
         }
       }
     }
-    if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+    if (!eig_grid_sync(a.bar, target, a.status, &sh_ok, a.wait_cycles, a.skip_cta)) return;
     // ---- D: two passes of classical Gram-Schmidt ----
     for (int p = 0; p < 2; ++p) {
       for (int k = b; k <= j; k += G) {
@@ -251,7 +260,7 @@ __global__ void __launch_bounds__(EIG_NT, 2) k_eig_lanczos(EigLanczosArgs a) {
           if (p == 0 && k == j) a.alpha[j] = d;
         }
       }
-      if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+      if (!eig_grid_sync(a.bar, target, a.status, &sh_ok, a.wait_cycles, a.skip_cta)) return;
       for (int k = tid; k <= j; k += EIG_NT) sh[k] = __ldcg(a.h + k);
       __syncthreads();
       // w -= V h over groups of 32 rows: warp wq sums k = wq, wq + 8, ...;
@@ -281,7 +290,7 @@ __global__ void __launch_bounds__(EIG_NT, 2) k_eig_lanczos(EigLanczosArgs a) {
         q = eig_block_sum(q, red);
         if (tid == 0) a.pE[b] = q;
       }
-      if (!eig_grid_sync(a.bar, target, a.status, &sh_ok)) return;
+      if (!eig_grid_sync(a.bar, target, a.status, &sh_ok, a.wait_cycles, a.skip_cta)) return;
     }
   }
   if (b == 0 && tid < 32) {
@@ -382,6 +391,14 @@ static int eig_lanczos_persistent(ngw_session *s, int tamm_d, int m, double *V, 
   a.V = V;
   a.alpha = dalpha;
   a.beta = dbeta;
+  // NGW_WAIT_CYCLES bounds each barrier wait (default 2^31 cycles, about one
+  // second); NGW_TEST_EIG_SKIP_ARRIVAL=<cta> makes that CTA withhold its first
+  // arrival so every wait runs out (tests of the timeout path only)
+  a.wait_cycles = 1LL << 31;
+  if (const char *e = getenv("NGW_WAIT_CYCLES"))
+    a.wait_cycles = std::min(std::max(atoll(e), 1LL << 10), 1LL << 34);
+  a.skip_cta = -1;
+  if (const char *e = getenv("NGW_TEST_EIG_SKIP_ARRIVAL")) a.skip_cta = atoi(e);
   const size_t bytes = ((size_t)a.CA * n + (size_t)a.KB * n + ncv + (m + 1) + G) * 8 + 64;
   char *ws = nullptr;
   NGW_TRY(dalloc(s, (void **)&ws, bytes));

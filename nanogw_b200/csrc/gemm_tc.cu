@@ -1727,7 +1727,11 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
   }
   if (op->tuned_nb != nb) {
     const TuneKey key{op->mu_pad, op->cv_pad, op->mu_k, op->kdef, op->n_isdf, op->ncv, nb, op->tda};
-    std::lock_guard<std::mutex> lk(g_tune_mu);
+    // The cache lookup and the nearest-shape reuse run under g_tune_mu; the
+    // tuning itself (device-exclusive, 0.3-1.5 s) runs without it, so other
+    // sessions' lookups do not wait behind one device's tuning.  Two sessions
+    // that miss on the same shape at once both tune it; the last result stays.
+    std::unique_lock<std::mutex> lk(g_tune_mu);
     auto use = [&](const TuneVal &v) {
       op->BN1 = v.bn1;
       op->var1 = v.var1;
@@ -1780,7 +1784,9 @@ int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1) {
         }
       }
     }
+    lk.unlock();
     NGW_TRY(autotune(s, nb));
+    lk.lock();
     g_tune[key] = TuneVal{op->BN1, op->var1, op->split1, op->BN2, op->var2, op->split2};
   }
   return NGW_OK;

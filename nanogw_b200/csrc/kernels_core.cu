@@ -5,6 +5,7 @@
 // pair index fastest, i.e. one chain's vector is contiguous.
 #include "ngw_internal.h"
 
+#include <algorithm>
 #include <cmath>
 
 namespace ngw {
@@ -414,6 +415,134 @@ void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb,
                                        eps);
   }
 #undef NGW_LSR
+}
+
+// ---------------------------------------------------------------------------
+// Lanczos step with full reorthogonalisation (optional form of the Sigma_c
+// chains; the reference recurrence has none).  Chain j keeps its Lanczos
+// vectors v_0 .. v_k in basis[j * ldb + q * ncv] (FP64).  Step k:
+//   w = w + t (k >= 1; at k = 0 w already holds p(H) v_0) ; a(k) = <w, v_k> ;
+//   if k + 1 < L:  w = w - a(k) v_k ; twice: h = V^T w, w = w - V h
+//   (classical Gram-Schmidt against v_0 .. v_k, applied twice) ; b(k+1) = ||w|| ;
+//   when prescale_next: w = w / b(k+1) (= v_{k+1}, also stored in the basis),
+//   v = -v b(k+1), hs = (R^1/2 or 1) w.
+// One CTA per chain; the dot products are summed eight at a time (warp
+// shuffles, then the eight warps' sums in a fixed order) and the update sums
+// run over q in ascending order, so the result is deterministic.
+constexpr int RG_Q = 8;
+
+__global__ void __launch_bounds__(LNT)
+    k_lanczos_reorth_step(double *__restrict__ w, double *__restrict__ v, const double *__restrict__ t,
+                          int ncv, int k, double *__restrict__ a, double *__restrict__ b, int niter,
+                          const double *__restrict__ s, double *__restrict__ hs, int tamm_d,
+                          int prescale_next, int *__restrict__ clen, double eps, double *__restrict__ basis,
+                          long long ldb) {
+  extern __shared__ double hq[];           // k + 1 Gram-Schmidt coefficients
+  __shared__ double sh[33];
+  __shared__ double red[LNT / 32][RG_Q];
+  const int j = blockIdx.x;
+  const int L = clen ? clen[j] : niter;
+  if (k >= L) return;
+  double *wj = w + (size_t)j * ncv;
+  double *vj = v + (size_t)j * ncv;
+  const double *tj = t ? t + (size_t)j * ncv : nullptr;
+  double *Vj = basis + (size_t)j * (size_t)ldb;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < ncv; i += LNT) {
+    double wi = wj[i];
+    if (tj) {
+      wi += tj[i];
+      wj[i] = wi;
+    }
+    acc += wi * vj[i];
+  }
+  const double ak = block_sum<LNT>(acc, sh);
+  if (threadIdx.x == 0) a[(size_t)j * niter + k] = ak;
+  if (k + 1 >= L) return;
+  for (int i = threadIdx.x; i < ncv; i += LNT) wj[i] = wj[i] - ak * vj[i];
+  __syncthreads();
+  for (int pass = 0; pass < 2; ++pass) {
+    // h_q = <v_q, w>, q = 0 .. k
+    for (int q0 = 0; q0 <= k; q0 += RG_Q) {
+      double d[RG_Q];
+#pragma unroll
+      for (int u = 0; u < RG_Q; ++u) d[u] = 0.0;
+      for (int i = threadIdx.x; i < ncv; i += LNT) {
+        const double wi = wj[i];
+#pragma unroll
+        for (int u = 0; u < RG_Q; ++u)
+          if (q0 + u <= k) d[u] += Vj[(size_t)(q0 + u) * ncv + i] * wi;
+      }
+#pragma unroll
+      for (int u = 0; u < RG_Q; ++u) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d[u] += __shfl_xor_sync(0xffffffffu, d[u], o);
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int u = 0; u < RG_Q; ++u) red[warp][u] = d[u];
+      }
+      __syncthreads();
+      if (threadIdx.x < RG_Q && q0 + (int)threadIdx.x <= k) {
+        double h = 0.0;
+#pragma unroll
+        for (int g = 0; g < LNT / 32; ++g) h += red[g][threadIdx.x];
+        hq[q0 + threadIdx.x] = h;
+      }
+      __syncthreads();
+    }
+    // w = w - V h
+    for (int i = threadIdx.x; i < ncv; i += LNT) {
+      double u = 0.0;
+      for (int q = 0; q <= k; ++q) u += hq[q] * Vj[(size_t)q * ncv + i];
+      wj[i] = wj[i] - u;
+    }
+    __syncthreads();
+  }
+  acc = 0.0;
+  for (int i = threadIdx.x; i < ncv; i += LNT) acc += wj[i] * wj[i];
+  const double bk1 = sqrt(block_sum<LNT>(acc, sh));
+  const bool stop = clen && eps > 0.0 && bk1 < eps;
+  if (threadIdx.x == 0) {
+    b[(size_t)j * niter + k + 1] = bk1;
+    if (stop) clen[j] = k + 1;
+  }
+  if (!prescale_next || stop) return;
+  double *vn = Vj + (size_t)(k + 1) * ncv;
+  double *hj = hs ? hs + (size_t)j * ncv : nullptr;
+  for (int i = threadIdx.x; i < ncv; i += LNT) {
+    const double wi = wj[i] / bk1;
+    wj[i] = wi;
+    vn[i] = wi;
+    vj[i] = -vj[i] * bk1;
+    if (hj) hj[i] = tamm_d ? wi : s[i] * wi;
+  }
+}
+
+void launch_lanczos_reorth_step(double *w, double *v, const double *t, int ncv, int nb, int k, double *a,
+                                double *b, int niter, const double *s, double *hs, int tamm_d,
+                                int prescale_next, int *clen, double eps, double *basis, long long ldb,
+                                cudaStream_t st) {
+  if (nb <= 0) return;
+  k_lanczos_reorth_step<<<nb, LNT, (size_t)(k + 1) * sizeof(double), st>>>(
+      w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next, clen, eps, basis, ldb);
+}
+
+// basis slot 0 of every chain = its normalised start vector
+__global__ void k_basis_init(const double *__restrict__ vec, int ncv, double *__restrict__ basis, long long ldb) {
+  const int j = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x)
+    basis[(size_t)j * (size_t)ldb + i] = vec[(size_t)j * ncv + i];
+}
+
+void launch_basis_init(const double *vec, int ncv, int nb, double *basis, long long ldb, cudaStream_t st) {
+  if (nb <= 0) return;
+  for (int j0 = 0; j0 < nb; j0 += 65535) {
+    const int n = std::min(65535, nb - j0);
+    k_basis_init<<<dim3(std::min(cdiv(ncv, 256), 16), n), 256, 0, st>>>(vec + (size_t)j0 * ncv, ncv,
+                                                                        basis + (size_t)j0 * (size_t)ldb, ldb);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -53,8 +53,12 @@ struct DBuf {
 };
 
 // Status word the kernels write when a bounded wait gives up or an index
-// check fails; read back after every synchronising call.
-enum DevStatus : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BOUNDS = 2 };
+// check fails; read back after every synchronising call.  DEV_TIMEOUT comes
+// from a tensor-core GEMM's mbarrier wait: the CTA gave up while TMA copies or
+// MMAs of its own may still have been in flight, so the session is refused
+// further work.  DEV_BARRIER_TIMEOUT comes from a grid barrier of a kernel
+// with nothing asynchronous in flight, which every CTA left cleanly.
+enum DevStatus : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BOUNDS = 2, DEV_BARRIER_TIMEOUT = 3 };
 
 struct MixedOperator;   // tcgen05 operand set (gemm_tc.cu)
 
@@ -98,6 +102,9 @@ struct ngw_session {
   void *cublas_ws = nullptr;
   void *cusolver = nullptr;    // cusolverDnHandle_t, created on first use
   bool use_graphs = true;
+  // set when a GEMM's bounded wait timed out: the session refuses further
+  // work (NGW_ERR_STATE) and has to be destroyed and created again
+  bool poisoned = false;
   // scratch (grown on demand)
   std::vector<ngw::DBuf> scratch;
   std::vector<void *> owned;
@@ -159,6 +166,11 @@ void launch_lanczos_first(double *w, const double *v, int ncv, int nb, double *a
 void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb, int k,
                          double *a, double *b, int niter, const double *s, double *hs,
                          int tamm_d, int prescale_next, int *clen, double eps, cudaStream_t st);
+void launch_lanczos_reorth_step(double *w, double *v, const double *t, int ncv, int nb, int k, double *a,
+                                double *b, int niter, const double *s, double *hs, int tamm_d,
+                                int prescale_next, int *clen, double eps, double *basis, long long ldb,
+                                cudaStream_t st);
+void launch_basis_init(const double *vec, int ncv, int nb, double *basis, long long ldb, cudaStream_t st);
 void launch_lanczos_prescale(double *w, double *v, int ncv, int nb, int k, const double *b,
                              int niter, const double *s, double *hs, int tamm_d, const int *clen,
                              cudaStream_t st);

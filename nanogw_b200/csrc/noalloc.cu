@@ -34,7 +34,11 @@ __global__ void k_qp_newton(int nqp, int nen, const double *__restrict__ sig,
 
 static __device__ __align__(256) double g_newton_scratch[NGW_NOALLOC_MAX_DOUBLES];
 
-// device address of g_newton_scratch, looked up once per device
+// device address of g_newton_scratch, looked up once per device and kept for
+// the life of the process: after cudaDeviceReset (or anything else that
+// destroys and recreates the device's primary context) the cached address is
+// stale, so a process that resets a device must not call
+// ngw_qp_newton_noalloc on it again
 static double *scratch_address(int device, int *rc) {
   static std::mutex mu;
   static double *addr[64] = {nullptr};

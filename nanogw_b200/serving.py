@@ -11,6 +11,16 @@ free (the operator then stays resident and is not re-uploaded).  Requests on
 different workers run concurrently on the device -- a new request starts as
 soon as a slot frees, it does not wait for a batch to form.
 
+Admission accounting: every worker's session keeps device memory between
+requests (operator, split-BF16 operands, eigenpairs, chain buffers); that
+memory counts against the budget whether the worker is busy or idle, measured
+with ``ngw_session_bytes`` once a request is done.  A request about to run
+reserves its footprint estimate (an upper bound of what the session will hold
+while serving it) on the worker it is routed to.  When the budget is short,
+idle workers other than the chosen one give their memory back (their session
+is recreated empty).  A request whose footprint alone exceeds the budget is
+refused with ``NGW_ERR_BUDGET`` and never runs.
+
 Latency = finish - arrival; throughput = QP states solved per second.
 """
 import heapq
@@ -20,6 +30,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from ._lib import NGW_ERR_BUDGET, NGWError
 from .api import RYD, Session
 
 
@@ -46,6 +57,7 @@ class SigmaRequest:
     worker: int = field(default=-1)
     sigma: np.ndarray = field(default=None)
     eqp: np.ndarray = field(default=None)
+    error: Exception = field(default=None)
 
     @property
     def nmem(self):
@@ -65,20 +77,43 @@ class SigmaRequest:
 
 
 class SigmaServer:
-    def __init__(self, device=0, workers=2, precision="mixed", hbm_budget_gb=150.0, solver=None):
-        """`solver(worker, request)` replaces the device solve (host-logic tests)."""
+    def __init__(self, device=0, workers=2, precision="mixed", hbm_budget_gb=150.0, solver=None,
+                 session_bytes=None):
+        """`solver(worker, request)` replaces the device solve and
+        `session_bytes(worker)` the device-memory query (host-logic tests)."""
         self.device = device
         self.precision = precision
         self.budget = int(hbm_budget_gb * (1 << 30))
         self.solver = solver
+        self._session_bytes = session_bytes
         self.sessions = [] if solver else [Session(device, precision) for _ in range(workers)]
         self.nworkers = workers
         self.resident = [None] * workers          # mol_id held by each worker
+        self.held = [0] * workers                 # device bytes each worker's session holds
         self.peak_used = 0
+        self.released = 0                         # idle sessions emptied to make room
 
     def close(self):
         for s in self.sessions:
             s.close()
+
+    def worker_bytes(self, w):
+        """Device bytes worker w's session holds now (``ngw_session_bytes``)."""
+        if self._session_bytes is not None:
+            return int(self._session_bytes(w))
+        if self.solver:
+            return 0
+        return self.sessions[w].device_bytes
+
+    def release(self, w):
+        """Give an idle worker's device memory back: its session is recreated
+        empty (the autotuner's tile cache is process-wide and stays)."""
+        if not self.solver:
+            self.sessions[w].close()
+            self.sessions[w] = Session(self.device, self.precision)
+        self.resident[w] = None
+        self.held[w] = 0
+        self.released += 1
 
     def _solve(self, w, req):
         if self.solver:
@@ -101,21 +136,29 @@ class SigmaServer:
 
     def run(self, requests, realtime=True):
         """Serve `requests` (arrival times in seconds from the start).  With
-        realtime=False every request is available at t=0 (closed loop)."""
+        realtime=False every request is available at t=0 (closed loop).
+        Requests larger than the whole budget are refused (``req.error`` is
+        an NGWError with code NGW_ERR_BUDGET) and counted in ``refused``."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         lock = threading.Condition()
         free = list(range(self.nworkers))
         inflight = {}
-        used = [0]
+        reserved = [0] * self.nworkers
         pending = []          # arrived, not admitted: heap of (arrival, rid, req)
         t0 = time.perf_counter()
         errors = []
+        refused = []
+
+        def used():
+            return sum(max(h, r) for h, r in zip(self.held, reserved))
 
         def worker_done(w, req):
+            held = self.worker_bytes(w)
             with lock:
                 req.finish = time.perf_counter() - t0
                 free.append(w)
-                used[0] -= req.footprint_bytes()
+                self.held[w] = held
+                reserved[w] = 0
                 del inflight[req.rid]
                 lock.notify_all()
 
@@ -123,6 +166,7 @@ class SigmaServer:
             try:
                 self._solve(w, req)
             except Exception as e:       # keep serving; report at the end
+                req.error = e
                 errors.append((req.rid, repr(e)))
             worker_done(w, req)
 
@@ -138,14 +182,27 @@ class SigmaServer:
                 while pending and free:
                     _, _, req = pending[0]
                     need = req.footprint_bytes()
-                    if used[0] + need > self.budget and inflight:
-                        break
-                    heapq.heappop(pending)
+                    if need > self.budget:
+                        heapq.heappop(pending)
+                        req.error = NGWError(NGW_ERR_BUDGET, f"request {req.rid} needs {need} bytes, more "
+                                                             f"than the {self.budget}-byte budget")
+                        req.start = req.finish = time.perf_counter() - t0
+                        refused.append(req.rid)
+                        continue
                     # prefer a free worker that already holds this molecule
                     w = next((x for x in free if self.resident[x] == req.mol_id), free[0])
+                    reserved[w] = need
+                    if used() > self.budget:
+                        # idle sessions other than w give their memory back
+                        for x in free:
+                            if x != w and self.held[x] > 0 and used() > self.budget:
+                                self.release(x)
+                    if used() > self.budget:
+                        reserved[w] = 0
+                        break                    # wait for memory held by running requests
+                    heapq.heappop(pending)
                     free.remove(w)
-                    used[0] += need
-                    self.peak_used = max(self.peak_used, used[0])
+                    self.peak_used = max(self.peak_used, used())
                     inflight[req.rid] = req
                     req.start = time.perf_counter() - t0
                     req.worker = w
@@ -165,9 +222,10 @@ class SigmaServer:
         wall = time.perf_counter() - t0
         if errors:
             raise RuntimeError(f"{len(errors)} requests failed, first: {errors[0]}")
-        lat = np.array([r.finish - r.arrival for r in reqs])
-        solves = sum(len(r.qp_bands) for r in reqs)
-        return {"requests": len(reqs), "solves": solves, "wall_s": wall,
+        done = [r for r in reqs if r.error is None]
+        lat = np.array([r.finish - r.arrival for r in done]) if done else np.zeros(1)
+        solves = sum(len(r.qp_bands) for r in done)
+        return {"requests": len(done), "refused": len(refused), "solves": solves, "wall_s": wall,
                 "solves_per_s": solves / wall,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3)}

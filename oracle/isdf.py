@@ -61,18 +61,28 @@ def coulomb_0d(nfft, h, trunc):
     return 8.0 * np.pi * v
 
 
-def poisson(rho_cols, grid_idx, nfft, vcoul):
+def poisson(rho_cols, grid_idx, nfft, vcoul, workers=None):
     """v_c * rho for each column: pack on the box, FFT, multiply, FFT back,
-    unpack, scale by 1/N^3 (numpy's ifft already divides).
-    rho_cols: (ngrid, ncol); grid_idx: (ngrid, 3) integer coordinates."""
+    unpack, scale by 1/N^3 (the inverse transform already divides).
+    rho_cols: (ngrid, ncol); grid_idx: (ngrid, 3) integer coordinates.
+    ``workers``: threads for scipy's FFT (None: numpy's single-threaded FFT);
+    both are pocketfft and agree to rounding."""
     out = np.empty_like(rho_cols)
     ix = np.mod(grid_idx, nfft)
+    vh = vcoul[:, :, : nfft // 2 + 1]
+    if workers is None:
+        fwd = np.fft.rfftn
+        inv = lambda f: np.fft.irfftn(f, s=(nfft, nfft, nfft), axes=(0, 1, 2))   # noqa: E731
+    else:
+        import scipy.fft as sfft
+        fwd = lambda b: sfft.rfftn(b, workers=workers)                                # noqa: E731
+        inv = lambda f: sfft.irfftn(f, s=(nfft, nfft, nfft), workers=workers)         # noqa: E731
     for k in range(rho_cols.shape[1]):
         box = np.zeros((nfft, nfft, nfft))
         box[ix[:, 0], ix[:, 1], ix[:, 2]] = rho_cols[:, k]
-        f = np.fft.rfftn(box)
-        f *= vcoul[:, :, : nfft // 2 + 1]
-        r = np.fft.irfftn(f, s=(nfft, nfft, nfft), axes=(0, 1, 2))
+        f = fwd(box)
+        f *= vh
+        r = inv(f)
         out[:, k] = r[ix[:, 0], ix[:, 1], ix[:, 2]]
     return out
 

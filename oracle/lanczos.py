@@ -57,8 +57,18 @@ def polynomial_matvec_isdf(vec, polynomial, cmtrx, mmtrx, sqrtR, matvec=None):
     return hvec
 
 
+def _gram_schmidt_twice(basis, w, sel, k):
+    """w -= V (V^T w), twice, with V the chains' vectors v_0 .. v_k
+    (basis: (blksz, niter + 1, ncv); w: (ncv, len(sel)))."""
+    Vs = basis[:, : k + 1, :] if len(sel) == basis.shape[0] else basis[sel, : k + 1, :]
+    for _ in range(2):
+        h = np.matmul(Vs, w.T[:, :, None])                       # (nsel, k+1, 1)
+        w = w - np.matmul(Vs.transpose(0, 2, 1), h)[:, :, 0].T
+    return w
+
+
 def lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=None, lengths=None,
-                       return_lengths=False):
+                       return_lengths=False, reorth=False):
     """Lanczos alpha/beta for a block of independent chains.
 
     Follows ``shared/lanczos_spectra_lowcomsym.F90:67-166`` exactly (no
@@ -68,6 +78,9 @@ def lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=None, lengths
     at the top of step k when ``|b_k| < eps``, as the single-vector routine
     does (``shared/lanczos_spectra.f90:57-58``); the tail the reference leaves
     uninitialised is zero here and the chain's effective length is k.
+    ``reorth`` (not in the reference): after ``w -= a_k v_k`` every chain's w
+    is orthogonalised against its v_0 .. v_k by classical Gram-Schmidt applied
+    twice, before ``b_{k+1} = ||w||``.
     Returns (a, b) with shape (niter, blksz) [, effective lengths].
     """
     v0 = np.asarray(v0, dtype=np.float64)
@@ -81,9 +94,15 @@ def lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=None, lengths
     b = np.zeros((niter, blksz))
     vec = v0 / v0_norm[None, :]
     b[0, :] = 1.0
+    basis = None
+    if reorth:
+        basis = np.zeros((blksz, niter + 1, v0.shape[0]))
+        basis[:, 0, :] = vec.T
     wvec = apply_h(vec)
     a[0] = np.einsum("ij,ij->j", wvec, vec)
     wvec = wvec - a[0][None, :] * vec
+    if reorth:
+        wvec = _gram_schmidt_twice(basis, wvec, np.arange(blksz), 0)
     if niter >= 2:
         b[1] = np.where(L >= 2, np.sqrt(np.einsum("ij,ij->j", wvec, wvec)), 0.0)
     for k in range(1, niter):
@@ -98,11 +117,15 @@ def lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=None, lengths
         w = wvec[:, sel] / b[k, sel][None, :]
         v = -vec[:, sel] * b[k, sel][None, :]
         v, w = w, v
+        if reorth:
+            basis[sel, k, :] = v.T
         w = w + apply_h(v)
         a[k, sel] = np.einsum("ij,ij->j", w, v)
         more = k + 1 < L[sel]
         if more.any():
             w[:, more] = w[:, more] - a[k, sel][more][None, :] * v[:, more]
+            if reorth:
+                w[:, more] = _gram_schmidt_twice(basis, w[:, more], sel[more], k)
             b[k + 1, sel[more]] = np.sqrt(np.einsum("ij,ij->j", w[:, more], w[:, more]))
         vec[:, sel] = v
         wvec[:, sel] = w
@@ -152,7 +175,7 @@ def perturbed(apply_h, rel, seed=1):
 
 def lanczos_spectra_isdf(v0, v0_norm, zz, niter, polynomial, cmtrx, mmtrx, sqrtR,
                          tamm_d=False, perturb=0.0, lengths=None, early_exit_eps=None,
-                         return_lengths=False):
+                         return_lengths=False, reorth=False):
     """``lanczos_spectra_isdf_lowcomsym`` (``shared/lanczos_spectra_lowcomsym.F90:7-190``):
     the spectra <P|1/(zz-p(H))|P> for a block of start vectors; per-chain
     lengths and the single-vector form's exit (``shared/lanczos_spectra.f90:57-58``)
@@ -166,7 +189,7 @@ def lanczos_spectra_isdf(v0, v0_norm, zz, niter, polynomial, cmtrx, mmtrx, sqrtR
         def apply_h(x):
             return polynomial_matvec_isdf(x, polynomial, cmtrx, mmtrx, sqrtR, matvec=mv)
     a, b, leff = lanczos_recurrence(apply_h, v0, v0_norm, niter, early_exit_eps=early_exit_eps,
-                                    lengths=lengths, return_lengths=True)
+                                    lengths=lengths, return_lengths=True, reorth=reorth)
     spec = continued_fraction(a, b, zz, lengths=leff)
     if return_lengths:
         return spec, a, b, leff

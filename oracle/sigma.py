@@ -54,7 +54,7 @@ def energy_grid(e1_m, deltae, nen):
 
 def sigma_c_state(psi_intp, mmtrx, e1, nval, m1, nen, deltae, ecuts, niter,
                   polynomial, tamm_d=False, bands=None, return_ab=False, perturb=0.0,
-                  lengths=None, early_exit_eps=None):
+                  lengths=None, early_exit_eps=None, reorth=False):
     """Sigma_c(omega) (Ry, complex, length nen) of QP band ``m1`` (1-based),
     summed over ``bands`` (default: all bands 1..nmem).  ``lengths``: optional
     per-band-chain Lanczos lengths; ``early_exit_eps``: per-chain exit.
@@ -78,7 +78,7 @@ def sigma_c_state(psi_intp, mmtrx, e1, nval, m1, nen, deltae, ecuts, niter,
     ezz[:nen, :] = (-zz[:, None] + e1[bands - 1][None, :]) * eta[None, :] + 1j * ecuts
     spectra, a, b = L.lanczos_spectra_isdf(p, pnorm, ezz, niter, polynomial, cm, mmtrx, sr,
                                            tamm_d=tamm_d, perturb=perturb, lengths=lengths,
-                                           early_exit_eps=early_exit_eps)
+                                           early_exit_eps=early_exit_eps, reorth=reorth)
     if tamm_d:
         # 2.0**0.5 is a default-real (single precision) expression in the Fortran
         sqrt2 = float(np.sqrt(np.float32(2.0)))

@@ -8,7 +8,7 @@ container that has the NanoGW tree; the fixtures are committed).
 * libxc_lda.npz      <- LIB/libxc/testsuite/lda_x.data, lda_c_pz.data :
   (rhoa, rhob, zk, vrhoa, vrhob, v2rhoa2, v2rhoab, v2rhob2) per point.
 
-Usage: python tests/golden/make_golden.py [/path/to/NanoGW]
+Usage: python tests/golden/make_golden.py /path/to/NanoGW
 """
 import os
 import re
@@ -16,7 +16,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py /path/to/NanoGW  (the reference source tree)")
+REF = sys.argv[1]
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -102,3 +102,36 @@ def test_mixed_plan_recomputes_after_query(small_system):
         s.operator_eigenpairs(kmax=4, msteps=30)
         b = s.calculate_sigma_lanczos(S.e1, S.nval, qp, 21, 2.0, 0.02, 12, S.poly)
     assert np.array_equal(a, b)
+
+
+def test_barrier_wait_runs_out_and_session_recovers(small_system):
+    """The persistent eigen kernel's grid barrier with a short wait bound
+    (NGW_WAIT_CYCLES, ~1 ms) and one CTA withholding its first arrival
+    (NGW_TEST_EIG_SKIP_ARRIVAL): every CTA's wait runs out, the kernel
+    returns, the call reports NGW_ERR_TIMEOUT, and the same session then
+    computes the eigenpairs and a mixed-precision solve exactly as a fresh
+    session does.  Nothing asynchronous is in flight in this kernel."""
+    from nanogw_b200._lib import NGW_ERR_TIMEOUT
+    S = small_system
+    with ngw.Session(0, "mixed") as s:
+        s.set_isdf(S.psi_intp, S.M)
+        s.set_pairs(S.cvpair, S.sqrtR)
+        os.environ["NGW_WAIT_CYCLES"] = str(1 << 21)
+        os.environ["NGW_TEST_EIG_SKIP_ARRIVAL"] = "0"
+        try:
+            with pytest.raises(ngw.NGWError) as ei:
+                s.operator_eigenpairs(kmax=8, msteps=64)
+        finally:
+            del os.environ["NGW_WAIT_CYCLES"]
+            del os.environ["NGW_TEST_EIG_SKIP_ARRIVAL"]
+        assert ei.value.code == NGW_ERR_TIMEOUT
+        vals, res = s.operator_eigenpairs(kmax=8, msteps=64)
+        qp = np.array([S.nval, S.nval + 1], dtype=np.int32)
+        sig = s.calculate_sigma_lanczos(S.e1, S.nval, qp, 41, 2.0, 0.02, 12, S.poly)
+    with ngw.Session(0, "mixed") as f:
+        f.set_isdf(S.psi_intp, S.M)
+        f.set_pairs(S.cvpair, S.sqrtR)
+        vals_f, res_f = f.operator_eigenpairs(kmax=8, msteps=64)
+        sig_f = f.calculate_sigma_lanczos(S.e1, S.nval, qp, 41, 2.0, 0.02, 12, S.poly)
+    assert np.array_equal(vals, vals_f) and np.array_equal(res, res_f)
+    assert np.array_equal(sig, sig_f)

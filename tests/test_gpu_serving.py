@@ -56,3 +56,18 @@ def test_alone_equals_in_mix(requests, precision):
         # same kernels, same tile choice, same summation order: identical bits
         assert np.array_equal(r.sigma, a.sigma), (r.rid, np.max(np.abs(r.sigma - a.sigma)))
         assert np.array_equal(r.eqp, a.eqp)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_footprint_bounds_session_bytes(requests, precision):
+    """The admission estimate is an upper bound of what the session holds
+    (``ngw_session_bytes``) after serving the request, and the server's
+    accounting holds the measured bytes of its idle worker."""
+    for r in requests:
+        srv = SigmaServer(workers=1, precision=precision)
+        rr = _clone(r)
+        srv.run([rr], realtime=False)
+        measured = srv.sessions[0].device_bytes
+        assert srv.held[0] == measured > 0
+        assert rr.footprint_bytes() >= measured, (r.rid, rr.footprint_bytes(), measured)
+        srv.close()

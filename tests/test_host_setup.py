@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from nanogw_b200 import host, pipeline, polyfit, synth
 from nanogw_b200.api import lowcomsym_pairs, sqrt_r
@@ -93,3 +94,19 @@ def test_abi_reports_errors_without_device():
     rc = L.ngw_session_create(999, ctypes.byref(h))
     assert rc != 0 and not h.value
     assert L.ngw_last_error()
+
+
+@pytest.mark.parametrize("nocc,nemp_factor", [(8, 4), (20, 3), (48, 4), (96, 4), (140, 4), (160, 4)])
+def test_product_polynomial_equals_oracle_sweep(nocc, nemp_factor):
+    """The product's polynomial (the reference's nx = 20..300 sweep, last
+    candidate with error below 1e3) equals the oracle's bit for bit at the
+    batched and serving sizes."""
+    from nanogw_b200.polyfit import sigma_polynomial as product
+    from oracle.polyfit import sigma_polynomial as reference
+    rng = np.random.default_rng(nocc)
+    e1 = np.sort(np.concatenate([rng.uniform(-0.75, -0.25, nocc),
+                                 rng.uniform(-0.15, 0.5, nemp_factor * nocc)])) * 2.0
+    p, emin, emax, nx = product(e1, nocc, len(e1), 12, return_nx=True)
+    q, qmin, qmax, _ = reference(e1, nocc, len(e1), 12)
+    assert (emin, emax) == (qmin, qmax)
+    assert np.array_equal(p, q)

@@ -52,3 +52,51 @@ def test_arrivals_respected_and_routing():
     # request 1 reuses the worker that already holds molecule 7
     assert reqs[1].worker == reqs[0].worker
     assert st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_oversize_request_refused_with_budget_error():
+    from nanogw_b200._lib import NGW_ERR_BUDGET
+    ran = []
+
+    def solver(w, req):
+        ran.append(req.rid)
+
+    small = _req(0, 1, 0.0)
+    big = _req(1, 2, 0.0, n=512, nmem=200, nval=40)
+    srv = SigmaServer(workers=2, hbm_budget_gb=1.5 * small.footprint_bytes() / (1 << 30), solver=solver)
+    assert big.footprint_bytes() > srv.budget
+    st = srv.run([small, big], realtime=False)     # nothing in flight when `big` is considered
+    assert ran == [0]
+    assert st["refused"] == 1 and st["requests"] == 1
+    assert big.error is not None and big.error.code == NGW_ERR_BUDGET
+
+
+def test_idle_resident_memory_counts_and_is_released():
+    """Memory an idle worker's session still holds (measured, as
+    ngw_session_bytes reports it) counts against the budget; when a new
+    request does not fit, idle sessions other than the chosen worker are
+    emptied first."""
+    held = {}
+
+    def solver(w, req):
+        held[w] = req.footprint_bytes()      # the session keeps what it used
+        time.sleep(0.01)
+
+    def session_bytes(w):
+        return held.get(w, 0)
+
+    reqs = [_req(i, 10 + i, 0.0) for i in range(3)]
+    one = reqs[0].footprint_bytes()
+    srv = SigmaServer(workers=3, hbm_budget_gb=2.5 * one / (1 << 30), solver=solver,
+                      session_bytes=session_bytes)
+    orig_release = srv.release
+
+    def release(w):
+        held[w] = 0
+        orig_release(w)
+    srv.release = release
+    st = srv.run(reqs, realtime=False)
+    assert st["requests"] == 3 and st["refused"] == 0
+    assert srv.released >= 1                 # an idle session gave its memory back
+    assert srv.peak_used <= srv.budget
+    assert sum(srv.held) <= srv.budget
