@@ -157,35 +157,47 @@ def random_operator(n_isdf, nocc, nemp, seed):
     return psi, m, e1
 
 
-def batched_workload(local, nmol, nqp, seed=2024, nocc_range=(20, 140)):
-    """Uneven molecules in one batch (the batched configuration: n_occ in
-    nocc_range, n_empty = 3-4 n_occ, n_isdf = 8 n_occ, per-chain Lanczos
-    lengths 100-300 seeded per chain), random operators of those dimensions.
-    Times one ngw_sigma_lanczos_batch call (graph replay) against the same
-    solves issued one molecule after another, both mixed precision."""
+def batched_workload(local, nmol, nqp, seed=2024, fp64_max_nocc=80):
+    """Uneven molecules in one batch (the batched configuration): 8 synthetic
+    molecules built as the 12-atom one with 6-40 atoms, n_occ growing with
+    the atom count from 20 to 140, n_empty = 3-4 n_occ, grid radius 8-14 bohr
+    at h = 0.3, n_isdf = 8 n_occ (device CVT, ISDF fit, Coulomb kernel),
+    per-chain Lanczos lengths 100-300 seeded per chain, ``nqp`` QP states per
+    molecule.  Times one ngw_sigma_lanczos_batch call (graph replay) against
+    the same solves issued one molecule after another, both mixed precision,
+    and states every QP energy's error against the plain FP64 path
+    (Sigma_x - V_xc = -2 eV, Newton to 1e-7 eV) for the molecules with
+    n_occ <= fp64_max_nocc."""
     import nanogw_b200 as ngw
+    from nanogw_b200 import pipeline, synth
     from nanogw_b200.api import lowcomsym_pairs, sqrt_r
     from nanogw_b200.polyfit import sigma_polynomial
     rng = np.random.default_rng(seed)
-    sessions, reqs, dims = [], [], []
+    sessions, reqs, dims, ops = [], [], [], []
+    t = time.perf_counter()
     for i in range(nmol):
-        nocc = int(rng.integers(nocc_range[0], nocc_range[1] + 1))
-        nemp = int(nocc * rng.uniform(3.0, 4.0))
-        n_isdf = 8 * nocc
-        psi, m, e1 = random_operator(n_isdf, nocc, nemp, seed + 1 + i)
+        n_atoms = int(rng.integers(6, 41))
+        frac = (n_atoms - 6) / 34.0
+        nocc = int(round(20 + 120 * frac))
+        nemp = int(round(nocc * rng.uniform(3.0, 4.0)))
+        arad = float(4.0 * (n_atoms / 12.0) ** (1.0 / 3.0))
+        mol = synth.make_molecule(n_atoms, arad, 8.0 + 6.0 * frac, 0.3, nocc, nemp, seed + 1 + i)
+        qp = pipeline.qp_bands_near_gap(mol.nval, nqp)
         s = ngw.Session(local, "mixed")
-        s.set_isdf(psi, m)
-        cv = lowcomsym_pairs(nocc, nocc + nemp)
-        s.set_pairs(cv, sqrt_r(e1, cv))
-        poly, _, _ = sigma_polynomial(e1, nocc, nocc + nemp, 12)
-        nq = min(nqp, nocc + nemp)
-        qp = np.arange(nocc - nq // 2 + 1, nocc - nq // 2 + 1 + nq, dtype=np.int32)
-        lens = rng.integers(100, 301, size=(nq, nocc + nemp))
-        reqs.append(dict(e1=e1, nval=nocc, qp_bands=qp, nen=400, deltae=4.0, ecuts=0.02, niter=300,
+        op = pipeline.build_operator(mol, 8 * nocc, s, qp_bands=qp, seed=seed + 1 + i)
+        s.set_isdf(op.psi_intp, op.mmtrx)
+        cv = lowcomsym_pairs(op.nval, op.nmem)
+        s.set_pairs(cv, sqrt_r(op.e1, cv))
+        poly, _, _ = sigma_polynomial(op.e1, op.nval, op.nmem, 12)
+        lens = rng.integers(100, 301, size=(nqp, op.nmem))
+        reqs.append(dict(e1=op.e1, nval=op.nval, qp_bands=qp, nen=400, deltae=4.0, ecuts=0.02, niter=300,
                          polynomial=poly, chain_niter=lens))
         sessions.append(s)
-        dims.append({"n_occ": nocc, "n_empty": nemp, "n_isdf": n_isdf, "ncv": int(len(cv)),
-                     "chains": int(nq * (nocc + nemp)), "chain_steps": int(lens.sum())})
+        ops.append(op)
+        dims.append({"n_atoms": n_atoms, "n_occ": nocc, "n_empty": nemp, "n_isdf": int(op.n_isdf),
+                     "grid_points": int(mol.psi.shape[0]), "ncv": int(len(cv)),
+                     "chains": int(nqp * op.nmem), "chain_steps": int(lens.sum())})
+    setup_s = time.perf_counter() - t
     import torch
     solves = sum(len(r["qp_bands"]) for r in reqs)
     for s, r in zip(sessions, reqs):          # tunes every shape, warms the per-session graphs
@@ -193,20 +205,36 @@ def batched_workload(local, nmol, nqp, seed=2024, nocc_range=(20, 140)):
             s.calculate_sigma_lanczos(**r)
     torch.cuda.synchronize()
     t = time.perf_counter()
-    for s, r in zip(sessions, reqs):
-        s.calculate_sigma_lanczos(**r)
+    seq_sig = [s.calculate_sigma_lanczos(**r) for s, r in zip(sessions, reqs)]
     seq = time.perf_counter() - t
     for _ in range(2):                        # eager + capture of the batch graph
         ngw.sigma_lanczos_batch(sessions, reqs)
     t = time.perf_counter()
-    ngw.sigma_lanczos_batch(sessions, reqs)
+    bat_sig = ngw.sigma_lanczos_batch(sessions, reqs)
     bat = time.perf_counter() - t
+    identical = all(np.array_equal(a, b) for a, b in zip(seq_sig, bat_sig))
+    errs = []
+    for s, r, sig, d in zip(sessions, reqs, bat_sig, dims):
+        if d["n_occ"] > fp64_max_nocc:
+            errs.append(None)
+            continue
+        s.set_precision("fp64")
+        s64 = s.calculate_sigma_lanczos(**r)
+        s.set_precision("mixed")
+        e1 = r["e1"][r["qp_bands"] - 1] * RYD
+        em = s.qp_newton(sig * RYD, e1, e1, r["deltae"] * RYD, -12.0, -10.0, 1e-7)[0]
+        ef = s.qp_newton(s64 * RYD, e1, e1, r["deltae"] * RYD, -12.0, -10.0, 1e-7)[0]
+        errs.append(round(float(np.max(np.abs(em - ef)) * 1e3), 5))
     for s in sessions:
         s.close()
-    return {"workload": f"{nmol} uneven molecules, {nqp} QP states each, per-chain lengths 100-300",
-            "values": "random operators of the molecules' dimensions (timing only)",
-            "solves": solves, "batched_solves_per_s": solves / bat, "sequential_solves_per_s": solves / seq,
-            "batched_s": bat, "sequential_s": seq, "molecules": dims}
+    return {"workload": f"{nmol} uneven synthetic molecules (6-40 atoms, n_occ 20-140), {nqp} QP states each, "
+                        f"per-chain lengths 100-300",
+            "values": "seeded synthetic molecules (device CVT, ISDF fit and Coulomb kernel)",
+            "setup_s": setup_s, "solves": solves, "batched_solves_per_s": solves / bat,
+            "sequential_solves_per_s": solves / seq, "batched_s": bat, "sequential_s": seq,
+            "batched_equals_sequential": identical,
+            "qp_err_mev_vs_fp64": {"rule": f"molecules with n_occ <= {fp64_max_nocc}", "per_molecule": errs},
+            "molecules": dims}
 
 
 def serving_molecule(sess, rid, rng, nocc_range, seed):
@@ -308,6 +336,87 @@ def serving_workload(local, nreq, workers, seed=77, nocc_range=(8, 160), load=0.
                            "speedup_vs_fp64": mixed_sub["solves_per_s"] / f64_sub["solves_per_s"],
                            "qp_err_mev_per_request": [round(x, 5) for x in errs],
                            "qp_err_mev_max": max(errs) if errs else None}}
+    return out
+
+
+LARGE = dict(name="60-atom molecule, 240 occ + 960 empty, 4800 ISDF points, grid radius 16 bohr at h = 0.3, "
+                 "300 Lanczos steps, 800 energies", n_atoms=60, atom_radius=10.0, grid_radius=16.0, h=0.3,
+             n_occ=240, n_empty=960, n_isdf=4800, niter=300, nen=800, deltae=4.0, ecuts=0.02, npoly=12, seed=31)
+
+
+def large_workload(local, fp64_chains=128):
+    """The large single molecule end to end on one GPU: synthetic molecule
+    (host), CVT points, ISDF fit, batched FFT-Poisson over the 2x-padded box
+    in column chunks, Coulomb kernel (device), then Sigma_c in mixed
+    precision for the QP state at the top of the valence band over all 1200
+    band chains (timed), and -- the plain FP64 path takes minutes per state
+    here -- both forms on the same state summed over the first
+    ``fp64_chains`` bands only, for the QP error (Sigma_x - V_xc = -2 eV,
+    Newton to 1e-7 eV)."""
+    import nanogw_b200 as ngw
+    from nanogw_b200 import host, pipeline, synth
+    from nanogw_b200.polyfit import sigma_polynomial
+    wl = dict(LARGE)
+    out = {"workload": wl["name"]}
+    t = time.perf_counter()
+    mol = synth.make_molecule(wl["n_atoms"], wl["atom_radius"], wl["grid_radius"], wl["h"], wl["n_occ"],
+                              wl["n_empty"], wl["seed"])
+    out["setup_s"] = {"synthetic_molecule_host": time.perf_counter() - t}
+    out["grid_points"] = int(mol.psi.shape[0])
+    qp = pipeline.qp_bands_near_gap(mol.nval, 32)
+    nfft = pipeline.fft_box_size(mol.rmax, mol.h)
+    out["fft_box"] = nfft
+    sess = ngw.Session(local, "fp64")
+    try:
+        torch_sync = __import__("torch").cuda.synchronize
+        t = time.perf_counter()
+        init = synth.cvt_initial_points(mol.grid, wl["n_isdf"], wl["seed"])
+        intp, _, iters = host.cvt(mol.grid, mol.rho, init, session=sess)
+        intp = host.dedup_points(intp, mol.rho)
+        out["setup_s"]["cvt_device"] = time.perf_counter() - t
+        out["cvt_iterations"] = iters
+        out["n_isdf"] = int(len(intp))
+        mv = max([mol.nval] + [int(b) for b in qp])
+        t = time.perf_counter()
+        psi_intp, M, _ = sess.build_isdf_kernel(mol.psi, mol.grid_idx, intp, mv, nfft, mol.h, 2.0 * mol.rmax)
+        torch_sync()
+        out["setup_s"]["isdf_fit_poisson_coulomb_device"] = time.perf_counter() - t
+        e1 = mol.e1.copy()
+        poly, _, _ = sigma_polynomial(e1, mol.nval, mol.nmem, wl["npoly"])
+        cv = ngw.lowcomsym_pairs(mol.nval, mol.nmem)
+        sess.set_isdf(psi_intp, M)
+        sess.set_pairs(cv, ngw.sqrt_r(e1, cv))
+        out["ncv"] = int(len(cv))
+        m = np.array([mol.nval], dtype=np.int32)
+        e1q = e1[m - 1] * RYD
+        args = (e1, mol.nval, m, wl["nen"], wl["deltae"], wl["ecuts"], wl["niter"], poly)
+        # mixed precision, the whole state (all band chains); the first call
+        # builds the split operator and deflation eigenpairs and tunes the tiles
+        sess.set_precision("mixed")
+        t = time.perf_counter()
+        sess.calculate_sigma_lanczos(*args)
+        first = time.perf_counter() - t
+        t = time.perf_counter()
+        sig_full = sess.calculate_sigma_lanczos(*args)
+        full = time.perf_counter() - t
+        eq_full = sess.qp_newton(sig_full * RYD, e1q, e1q, wl["deltae"] * RYD, -12.0, -10.0, 1e-7)[0]
+        out["mixed_full_state"] = {"chains": int(mol.nmem), "s_per_solve": full, "solves_per_s": 1.0 / full,
+                                   "first_call_s": first, "eqp_ev": float(eq_full[0])}
+        # both forms on the same band subset
+        res = {}
+        for prec in ("mixed", "fp64"):
+            sess.set_precision(prec)
+            t = time.perf_counter()
+            sg = sess.calculate_sigma_lanczos(*args, nbands_sum=fp64_chains)
+            dt = time.perf_counter() - t
+            res[prec] = (sess.qp_newton(sg * RYD, e1q, e1q, wl["deltae"] * RYD, -12.0, -10.0, 1e-7)[0], dt)
+        out["subset"] = {"rule": f"QP band {int(m[0])}, Sigma_c summed over bands 1..{fp64_chains}",
+                         "fp64_s": res["fp64"][1], "mixed_s": res["mixed"][1],
+                         "speedup_vs_fp64": res["fp64"][1] / res["mixed"][1],
+                         "qp_err_mev": float(abs(res["mixed"][0][0] - res["fp64"][0][0]) * 1e3)}
+        out["device_bytes"] = sess.device_bytes
+    finally:
+        sess.close()
     return out
 
 
@@ -466,7 +575,7 @@ def main():
     ap.add_argument("--scan-chains", default="1024,2048")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the large-operator GEMM line of the default run")
-    ap.add_argument("--workload", default="12atom", choices=["12atom", "batched", "serving"],
+    ap.add_argument("--workload", default="12atom", choices=["12atom", "batched", "serving", "large"],
                     help="batched: uneven molecules in one graph launch; serving: request stream")
     ap.add_argument("--batched-qp", type=int, default=2)
     ap.add_argument("--serving-requests", type=int, default=32)
@@ -501,6 +610,8 @@ def main():
         if rank == 0:
             if args.workload == "batched":
                 res = batched_workload(local, 8, args.batched_qp)
+            elif args.workload == "large":
+                res = large_workload(local)
             else:
                 res = serving_workload(local, args.serving_requests, args.serving_workers,
                                        fp64_max_nocc=args.serving_fp64_max_nocc)

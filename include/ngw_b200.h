@@ -192,6 +192,18 @@ int ngw_qp_newton_noalloc(int nqp, int nen, const double *sigma_c_ev, const doub
                           int *ierr, void *stream);
 
 /* ---- measurement ---- */
+/* FP64 GEMM on the FP64 tensor cores, the kernel behind every FP64 contraction
+ * of this library except the plain FP64 matvec (which stays on cuBLAS as the
+ * comparison path): C = alpha op(A) op(B) + beta C with column-major DEVICE
+ * pointers and cuBLAS's argument meaning (transa/transb 0 = N, 1 = T).  An
+ * optional device workspace (ws, ws_bytes; 64 m n doubles cover every choice)
+ * lets small tile grids split K, summed in a fixed order.  Ordered on
+ * `stream` (cudaStream_t, NULL = default), no synchronisation.  No reference
+ * counterpart (the reference calls BLAS dgemm): used by the tests and the
+ * benchmark's FP64 GEMM line. */
+int ngw_dgemm(int transa, int transb, int m, int n, int k, double alpha, const double *A, int lda,
+              const double *B, int ldb, double beta, double *C, int ldc, double *ws, long long ws_bytes,
+              void *stream);
 /* Average device time (us) of one launch of each mixed-precision GEMM for nb
  * chains (GEMM1: T = C_isdf S, GEMM2: Z = (M C_isdf)^T T with its Clenshaw
  * epilogue), from CUDA events around `reps` back-to-back launches on the

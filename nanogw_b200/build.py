@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels_core.cu", "gemm_tc.cu", "deflate.cu", "abi.cu", "poisson.cu", "noalloc.cu", "isdf_fit.cu",
+CU_SOURCES = ["kernels_core.cu", "gemm_tc.cu", "dgemm.cu", "lu.cu", "deflate.cu", "abi.cu", "poisson.cu", "noalloc.cu", "isdf_fit.cu",
               "exchange.cu", "cvt_device.cu", "fft3d.cu"]
 CXX_SOURCES = ["host_setup.cpp", "parsec_io.cpp"]
 

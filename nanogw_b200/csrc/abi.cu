@@ -157,7 +157,7 @@ enum {
   SL_IN = 0, SL_OUT, SL_HS, SL_T1, SL_T2, SL_Z, SL_VEC, SL_WVEC, SL_TMP, SL_A, SL_B, SL_ZZ,
   SL_SPEC, SL_CMN, SL_CM, SL_P, SL_P2, SL_PN2, SL_PN, SL_CHB, SL_CHQ, SL_E1, SL_ZZ0, SL_SIG,
   SL_KR, SL_KC, SL_KM, SL_B1, SL_B2, SL_QPW, SL_QPIO, SL_SPECS, SL_CLEN, SL_LEN, SL_SLOT, SL_BASIS,
-  SL_NUM
+  SL_DGWS, SL_NUM
 };
 
 // ---------------------------------------------------------------------------
@@ -475,6 +475,8 @@ struct SigmaJob {
   double *de1, *zz0, *sig, *cmn, *cm, *P, *P2, *pn2, *pn, *V, *W, *hs, *tmp, *a, *b, *S;
   double *basis = nullptr;     // Krylov bases (reorth): chain j at basis + j * ldb
   long long ldb = 0;
+  double *dgws = nullptr;      // split-K workspace of the start-vector GEMMs
+  size_t dgws_bytes = 0;
   int *chb, *chq, *clen, *dlen, *dslot;
   // current block
   int q0 = 0, nq = 0, nb = 0;
@@ -572,6 +574,8 @@ static int sigma_prepare(SigmaJob &J, ngw_session *s, const ngw_sigma_params *p,
   NGW_TRY(scratch(s, SL_CLEN, (size_t)nb_max * 4, (void **)&J.clen));
   NGW_TRY(scratch(s, SL_LEN, (size_t)nb_max * 4, (void **)&J.dlen));
   NGW_TRY(scratch(s, SL_SLOT, (size_t)nb_max * 4, (void **)&J.dslot));
+  J.dgws_bytes = (size_t)4 * n * nb_max * 8;   // up to 4 K slices of the N_mu x chains product
+  NGW_TRY(scratch(s, SL_DGWS, J.dgws_bytes, (void **)&J.dgws));
   if (p->reorth) {
     J.ldb = (long long)(niter + 1) * ncv;
     NGW_TRY(scratch(s, SL_BASIS, (size_t)nb_max * (size_t)J.ldb * 8, (void **)&J.basis));
@@ -638,10 +642,10 @@ static int sigma_region(SigmaJob &J) {
   const double one = 1.0, zero = 0.0;
   // start vectors  P = sqrtR * C^T M (psi_m psi_n)   (F90z:578-709), FP64
   launch_pair_gather_cols(s->d_psi, n, J.chb, J.chb + nb, nb, J.cmn, s->stream);
-  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, n, nb, n, &one, s->d_M, n, J.cmn, n, &zero,
-                         J.cm, n));
-  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, ncv, nb, n, &one, s->d_C, n, J.cm, n, &zero,
-                         J.P, ncv));
+  NGW_CUDA(dgemm(s->stream, false, false, n, nb, n, one, s->d_M, n, J.cmn, n, zero, J.cm, n, J.dgws,
+                 J.dgws_bytes));
+  NGW_CUDA(dgemm(s->stream, true, false, ncv, nb, n, one, s->d_C, n, J.cm, n, zero, J.P, ncv, J.dgws,
+                 J.dgws_bytes));
   launch_norms(J.P, ncv, nb, s->d_sqrtR, tamm_d, J.P2, J.pn2, s->stream);
   NGW_CUDA(cudaMemsetAsync(J.a, 0, (size_t)niter * nb * 8, s->stream));
   NGW_CUDA(cudaMemsetAsync(J.b, 0, (size_t)niter * nb * 8, s->stream));
@@ -681,7 +685,7 @@ static void sigma_key(const SigmaJob &J, std::vector<unsigned long long> &key) {
                           (const void *)J.hs, (const void *)J.tmp, (const void *)J.a, (const void *)J.b,
                           (const void *)J.S, (const void *)J.chb, (const void *)J.chq, (const void *)J.de1,
                           (const void *)J.zz0, (const void *)J.sig, (const void *)s->mixed,
-                          (const void *)J.clen, (const void *)J.dlen, (const void *)J.dslot})
+                          (const void *)J.clen, (const void *)J.dlen, (const void *)J.dslot, (const void *)J.dgws})
     key.push_back((unsigned long long)(uintptr_t)ptr);
   if (s->mixed) {
     int tune[4];
@@ -1066,10 +1070,8 @@ int ngw_k_integrate_isdf(ngw_session *s, int kflag, const int *rows, int nrow, c
   launch_pair_gather_cols(s->d_psi, n, db + 2 * nrow, db + 2 * nrow + ncol, ncol, cc, s->stream);
   launch_k_combine(s->d_M, s->d_Mxc, n, kflag, km, s->stream);
   const double one = 1.0, zero = 0.0;
-  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, n, nrow, n, &one, km, n, cr, n, &zero,
-                         tmp, n));
-  NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, nrow, ncol, n, &one, tmp, n, cc, n,
-                         &zero, out, nrow));
+  NGW_CUDA(dgemm(s->stream, false, false, n, nrow, n, one, km, n, cr, n, zero, tmp, n));
+  NGW_CUDA(dgemm(s->stream, true, false, nrow, ncol, n, one, tmp, n, cc, n, zero, out, nrow));
   NGW_CUDA(cudaMemcpyAsync(kmat, out, (size_t)nrow * ncol * 8, cudaMemcpyDeviceToHost, s->stream));
   NGW_CUDA(cudaStreamSynchronize(s->stream));
   return check_status(s);

@@ -20,8 +20,6 @@
 #include <utility>
 #include <vector>
 
-#include <cusolverDn.h>
-
 #include "ngw_internal.h"
 
 namespace ngw {
@@ -299,62 +297,149 @@ __global__ void __launch_bounds__(EIG_NT, 2) k_eig_lanczos(EigLanczosArgs a) {
   }
 }
 
-// Eigen-decomposition of the small symmetric Lanczos matrix T (column-major
-// n x n) on the device with cuSOLVER's divide-and-conquer solver: ascending
-// eigenvalues to w, orthonormal eigenvectors as the columns of V.
-static int sym_eig(ngw_session *s, const std::vector<double> &T, int n, std::vector<double> &w,
-                   std::vector<double> &V) {
-  void *hv = nullptr;
-  NGW_TRY(session_cusolver(s, &hv));
-  cusolverDnHandle_t h = (cusolverDnHandle_t)hv;
-  double *dA = nullptr, *dW = nullptr, *work = nullptr;
-  int *info = nullptr;
-  int lwork = 0, rc = NGW_OK;
-  const size_t ab = (size_t)n * n * 8;
-  do {
-    if ((rc = dalloc(s, (void **)&dA, ab)) || (rc = dalloc(s, (void **)&dW, (size_t)n * 8)) ||
-        (rc = dalloc(s, (void **)&info, 4)))
-      break;
-    if (cudaMemcpyAsync(dA, T.data(), ab, cudaMemcpyHostToDevice, s->stream) != cudaSuccess) {
-      set_error("copy of the Lanczos matrix failed");
-      rc = NGW_ERR_CUDA;
-      break;
+// Eigen-pairs of the small symmetric tridiagonal Lanczos matrix T (diagonal
+// a[0..n), off-diagonal b[0..n-1) coupling i and i+1) on the host:
+//  * all eigenvalues and the LAST component of every eigenvector by the
+//    implicit QL iteration with Wilkinson-type shifts (Bowdler, Martin,
+//    Reinsch and Wilkinson, "The QR and QL algorithms for symmetric
+//    matrices", Numer. Math. 11 (1968)); the plane rotations are applied to
+//    the last row of the eigenvector matrix only, so this is O(n^2);
+//  * the eigenvectors of the kvec largest eigenvalues by inverse iteration
+//    on T - theta I (tridiagonal LU with partial pivoting), each
+//    re-orthogonalised against the vectors already found for eigenvalues
+//    within 1e-3 |T| of it (modified Gram-Schmidt), signs fixed so the
+//    largest-magnitude component is positive.
+// Returns false when the QL iteration does not converge.
+static bool tridiag_eig(const std::vector<double> &a, const std::vector<double> &b, int n, int kvec,
+                        std::vector<double> &w, std::vector<double> &last, std::vector<double> &Y) {
+  std::vector<double> d(a.begin(), a.begin() + n), e(n, 0.0), z(n, 0.0);
+  for (int i = 0; i + 1 < n; ++i) e[i] = b[i];
+  z[n - 1] = 1.0;
+  const double eps = 2.220446049250313e-16;
+  for (int l = 0; l < n; ++l) {
+    int iter = 0, m;
+    do {
+      for (m = l; m < n - 1; ++m) {
+        const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= eps * dd) break;
+      }
+      if (m != l) {
+        if (iter++ == 100) return false;
+        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+        double r = std::hypot(g, 1.0);
+        g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? std::fabs(r) : -std::fabs(r)));
+        double sn = 1.0, c = 1.0, p = 0.0;
+        int i;
+        for (i = m - 1; i >= l; --i) {
+          double f = sn * e[i];
+          const double bb = c * e[i];
+          r = std::hypot(f, g);
+          e[i + 1] = r;
+          if (r == 0.0) {
+            d[i + 1] -= p;
+            e[m] = 0.0;
+            break;
+          }
+          sn = f / r;
+          c = g / r;
+          g = d[i + 1] - p;
+          r = (d[i] - g) * sn + 2.0 * c * bb;
+          p = sn * r;
+          d[i + 1] = g + p;
+          g = c * r - bb;
+          f = z[i + 1];
+          z[i + 1] = sn * z[i] + c * f;
+          z[i] = c * z[i] - sn * f;
+        }
+        if (r == 0.0 && i >= l) continue;
+        d[l] -= p;
+        e[l] = g;
+        e[m] = 0.0;
+      }
+    } while (m != l);
+  }
+  std::vector<int> ord(n);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return d[x] > d[y]; });
+  w.resize(n);
+  last.resize(n);
+  double tnorm = 0.0;
+  for (int i = 0; i < n; ++i) {
+    w[i] = d[ord[i]];
+    last[i] = z[ord[i]];
+    tnorm = std::max(tnorm, std::fabs(a[i]) + (i > 0 ? std::fabs(b[i - 1]) : 0.0) +
+                                (i + 1 < n ? std::fabs(b[i]) : 0.0));
+  }
+  // inverse iteration for the kvec largest
+  kvec = std::min(kvec, n);
+  Y.assign((size_t)n * kvec, 0.0);
+  std::vector<double> dl(n), dm(n), du(n), du2(n), x(n);
+  std::vector<int> piv(n);
+  for (int c = 0; c < kvec; ++c) {
+    // shift slightly off the eigenvalue so T - theta I stays nonsingular
+    const double theta = w[c] + 8.0 * eps * std::max(tnorm, 1e-300);
+    // LU with partial pivoting of the tridiagonal T - theta I (rows swapped
+    // at most with the next one; du2 the second superdiagonal fill-in)
+    for (int i = 0; i < n; ++i) {
+      dm[i] = a[i] - theta;
+      du[i] = i + 1 < n ? b[i] : 0.0;
+      dl[i] = i + 1 < n ? b[i] : 0.0;
+      du2[i] = 0.0;
     }
-    if (cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dA, n, dW,
-                                    &lwork) != CUSOLVER_STATUS_SUCCESS) {
-      set_error("cusolverDnDsyevd_bufferSize failed");
-      rc = NGW_ERR_CUDA;
-      break;
+    for (int i = 0; i + 1 < n; ++i) {
+      if (std::fabs(dm[i]) >= std::fabs(dl[i])) {
+        piv[i] = i;
+        if (dm[i] == 0.0) dm[i] = eps * std::max(tnorm, 1e-300);
+        const double f = dl[i] / dm[i];
+        dl[i] = f;
+        dm[i + 1] -= f * du[i];
+      } else {
+        piv[i] = i + 1;
+        const double f = dm[i] / dl[i];
+        dm[i] = dl[i];
+        dl[i] = f;
+        const double t = du[i];
+        du[i] = dm[i + 1];
+        dm[i + 1] = t - f * dm[i + 1];
+        if (i + 2 < n) {
+          du2[i] = du[i + 1];
+          du[i + 1] = -f * du[i + 1];
+        }
+      }
     }
-    if ((rc = dalloc(s, (void **)&work, (size_t)std::max(lwork, 1) * 8))) break;
-    if (cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dA, n, dW, work, lwork,
-                         info) != CUSOLVER_STATUS_SUCCESS) {
-      set_error("cusolverDnDsyevd failed");
-      rc = NGW_ERR_CUDA;
-      break;
+    if (dm[n - 1] == 0.0) dm[n - 1] = eps * std::max(tnorm, 1e-300);
+    piv[n - 1] = n - 1;
+    for (int i = 0; i < n; ++i) x[i] = 1.0 / std::sqrt((double)n) * (1.0 + 0.01 * ((i * 7919 + c * 104729) % 13));
+    for (int itn = 0; itn < 4; ++itn) {
+      // solve (T - theta I) y = x: apply L^{-1} with the row interchanges, then U^{-1}
+      for (int i = 0; i + 1 < n; ++i) {
+        if (piv[i] != i) std::swap(x[i], x[i + 1]);
+        x[i + 1] -= dl[i] * x[i];
+      }
+      x[n - 1] /= dm[n - 1];
+      if (n >= 2) x[n - 2] = (x[n - 2] - du[n - 2] * x[n - 1]) / dm[n - 2];
+      for (int i = n - 3; i >= 0; --i) x[i] = (x[i] - du[i] * x[i + 1] - du2[i] * x[i + 2]) / dm[i];
+      // orthogonalise against vectors of nearby eigenvalues, normalise
+      for (int q = 0; q < c; ++q) {
+        if (std::fabs(w[q] - w[c]) > 1e-3 * tnorm) continue;
+        const double *yq = &Y[(size_t)q * n];
+        double dot = 0.0;
+        for (int i = 0; i < n; ++i) dot += yq[i] * x[i];
+        for (int i = 0; i < n; ++i) x[i] -= dot * yq[i];
+      }
+      double nrm = 0.0;
+      for (int i = 0; i < n; ++i) nrm += x[i] * x[i];
+      nrm = std::sqrt(nrm);
+      if (!(nrm > 0.0)) return false;
+      for (int i = 0; i < n; ++i) x[i] /= nrm;
     }
-    int hinfo = 0;
-    w.resize(n);
-    V.resize((size_t)n * n);
-    if (cudaMemcpyAsync(w.data(), dW, (size_t)n * 8, cudaMemcpyDeviceToHost, s->stream) ||
-        cudaMemcpyAsync(V.data(), dA, ab, cudaMemcpyDeviceToHost, s->stream) ||
-        cudaMemcpyAsync(&hinfo, info, 4, cudaMemcpyDeviceToHost, s->stream) ||
-        cudaStreamSynchronize(s->stream)) {
-      set_error("copy of the Ritz pairs failed");
-      rc = NGW_ERR_CUDA;
-      break;
-    }
-    if (hinfo != 0) {
-      set_error("symmetric eigen-solve of the Lanczos matrix did not converge (info %d)", hinfo);
-      rc = NGW_ERR_NOCONV;
-    }
-  } while (0);
-  cudaStreamSynchronize(s->stream);
-  dfree(s, dA, ab);
-  dfree(s, dW, (size_t)n * 8);
-  dfree(s, info, 4);
-  if (work) dfree(s, work, (size_t)std::max(lwork, 1) * 8);
-  return rc;
+    int imax = 0;
+    for (int i = 1; i < n; ++i)
+      if (std::fabs(x[i]) > std::fabs(x[imax])) imax = i;
+    const double sg = x[imax] < 0.0 ? -1.0 : 1.0;
+    for (int i = 0; i < n; ++i) Y[(size_t)c * n + i] = sg * x[i];
+  }
+  return true;
 }
 
 // The Lanczos loop of compute_top_eigs as one persistent kernel.  *done is
@@ -534,30 +619,18 @@ int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
       mm = j + 1;
       break;
     }
-  // Ritz pairs of the tridiagonal
-  std::vector<double> T((size_t)mm * mm, 0.0), ev, Y;
-  for (int i = 0; i < mm; ++i) {
-    T[(size_t)i * mm + i] = alpha[i];
-    if (i + 1 < mm) {
-      T[(size_t)(i + 1) * mm + i] = beta[i + 1];
-      T[(size_t)i * mm + i + 1] = beta[i + 1];
-    }
-  }
-  NGW_TRY(sym_eig(s, T, mm, ev, Y));
-  std::vector<int> ord(mm);
-  std::iota(ord.begin(), ord.end(), 0);
-  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return ev[x] > ev[y]; });
+  // Ritz pairs of the tridiagonal: all values with their residual bounds
+  // |beta_mm y_i(mm)|, vectors of the kmax largest
   const int k = std::min(kmax, mm);
-  s->eig_vals.assign(mm, 0.0);
-  s->eig_res.assign(mm, 0.0);
-  for (int i = 0; i < mm; ++i) {
-    s->eig_vals[i] = ev[ord[i]];
-    s->eig_res[i] = std::fabs(beta[mm] * Y[(size_t)ord[i] * mm + (mm - 1)]);
+  std::vector<double> ev, lastc, Yk;
+  if (!tridiag_eig(alpha, std::vector<double>(beta.begin() + 1, beta.begin() + mm), mm, k, ev, lastc, Yk)) {
+    set_error("eigenpair Lanczos: the tridiagonal QL iteration did not converge");
+    return NGW_ERR_NOCONV;
   }
+  s->eig_vals.assign(ev.begin(), ev.end());
+  s->eig_res.assign(mm, 0.0);
+  for (int i = 0; i < mm; ++i) s->eig_res[i] = std::fabs(beta[mm] * lastc[i]);
   // Ritz vectors U = V Y_k
-  std::vector<double> Yk((size_t)mm * k);
-  for (int c = 0; c < k; ++c)
-    for (int r = 0; r < mm; ++r) Yk[(size_t)c * mm + r] = Y[(size_t)ord[c] * mm + r];
   double *dY = nullptr;
   NGW_TRY(tmp.alloc((void **)&dY, (size_t)mm * k * 8));
   const size_t ubytes = (size_t)ncv * std::max(k, 1) * 8;
@@ -571,9 +644,12 @@ int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps) {
     s->eig_U_bytes = ubytes;
   }
   NGW_CUDA(cudaMemcpyAsync(dY, Yk.data(), (size_t)mm * k * 8, cudaMemcpyHostToDevice, s->stream));
-  if (k > 0)
-    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, ncv, k, mm, &one, V, ncv, dY, mm, &zero,
-                           s->eig_U, ncv));
+  if (k > 0) {
+    double *dws = nullptr;
+    const size_t wsb = (size_t)4 * ncv * k * 8;   // up to 4 K slices
+    NGW_TRY(tmp.alloc((void **)&dws, wsb));
+    NGW_CUDA(dgemm(s->stream, false, false, ncv, k, mm, one, V, ncv, dY, mm, zero, s->eig_U, ncv, dws, wsb));
+  }
   NGW_CUDA(cudaStreamSynchronize(s->stream));
   s->eig_k = k;
   s->eig_tda = tamm_d;

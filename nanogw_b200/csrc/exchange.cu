@@ -94,7 +94,7 @@ extern "C" int ngw_fock_exchange(ngw_session *s, int ngrid, int nmem, const doub
   const size_t psib = (size_t)ngrid * nmem * 8;
   const int total = nsig * maxv;
   const int chunk = std::min(total, 256);
-  double *dpsi = nullptr, *dps = nullptr, *drho = nullptr, *dv = nullptr, *dg2 = nullptr;
+  double *dpsi = nullptr, *dps = nullptr, *drho = nullptr, *dv = nullptr, *dg2 = nullptr, *dws = nullptr;
   int *dg = nullptr, *dab = nullptr;
   int rc = NGW_OK;
   const double fac = (double)ntrans / (h * h * h);
@@ -104,7 +104,8 @@ extern "C" int ngw_fock_exchange(ngw_session *s, int ngrid, int nmem, const doub
     if (dalloc(s, (void **)&dpsi, psib) || dalloc(s, (void **)&dps, (size_t)ngrid * nsig * 8) ||
         dalloc(s, (void **)&drho, (size_t)ngrid * chunk * 8) || dalloc(s, (void **)&dv, (size_t)ngrid * chunk * 8) ||
         dalloc(s, (void **)&dg2, (size_t)nsig * chunk * 8) || dalloc(s, (void **)&dg, (size_t)3 * ngrid * 4) ||
-        dalloc(s, (void **)&dab, (size_t)2 * chunk * 4)) {
+        dalloc(s, (void **)&dab, (size_t)2 * chunk * 4) ||
+        dalloc(s, (void **)&dws, dgemm_ws_bytes(nsig, chunk, ngrid))) {
       rc = NGW_ERR_OOM;
       break;
     }
@@ -138,9 +139,9 @@ extern "C" int ngw_fock_exchange(ngw_session *s, int ngrid, int nmem, const doub
       if ((rc = poisson_apply(s, ngrid, nc, drho, dg, nfft, h, trunc, dv)) != NGW_OK) break;
       k_grid_mul_band<<<dim3(bx, ygrid(nc)), 256, 0, s->stream>>>(dv, dpsi, ngrid, dab, nc);
       const double one = 1.0, zero = 0.0;
-      if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, nsig, nc, ngrid, &one, dps, ngrid, dv, ngrid, &zero,
-                      dg2, nsig) != CUBLAS_STATUS_SUCCESS) {
-        set_error("cublasDgemm (exchange projection) failed");
+      if (dgemm(s->stream, true, false, nsig, nc, ngrid, one, dps, ngrid, dv, ngrid, zero, dg2, nsig, dws,
+                dgemm_ws_bytes(nsig, chunk, ngrid)) != cudaSuccess) {
+        set_error("FP64 GEMM (exchange projection) failed");
         rc = NGW_ERR_CUDA;
         break;
       }
@@ -165,6 +166,7 @@ extern "C" int ngw_fock_exchange(ngw_session *s, int ngrid, int nmem, const doub
   dfree(s, dg2, (size_t)nsig * chunk * 8);
   dfree(s, dg, (size_t)3 * ngrid * 4);
   dfree(s, dab, (size_t)2 * chunk * 4);
+  dfree(s, dws, dgemm_ws_bytes(nsig, chunk, ngrid));
   if (rc != NGW_OK) return rc;
   for (int jj = 0; jj < nsig; ++jj)
     for (int ii = 0; ii < jj; ++ii) kx[jj + (size_t)ii * nsig] = kx[ii + (size_t)jj * nsig];
@@ -181,14 +183,15 @@ extern "C" int ngw_vxc_matrix(ngw_session *s, int ngrid, int nmem, const double 
   if (int e = check_density(ngrid, rho, "ngw_vxc_matrix")) return e;
   NGW_CUDA(cudaSetDevice(s->device));
   double *dps = nullptr, *drho = nullptr, *dvx = nullptr, *dvc = nullptr, *dw = nullptr, *dmx = nullptr,
-         *dmc = nullptr;
+         *dmc = nullptr, *dws = nullptr;
   const size_t pb = (size_t)ngrid * nsig * 8, mb = (size_t)nsig * nsig * 8;
   int rc = NGW_OK;
   std::vector<double> mx((size_t)nsig * nsig), mc((size_t)nsig * nsig);
   do {
     if (dalloc(s, (void **)&dps, pb) || dalloc(s, (void **)&dw, pb) || dalloc(s, (void **)&drho, (size_t)ngrid * 8) ||
         dalloc(s, (void **)&dvx, (size_t)ngrid * 8) || dalloc(s, (void **)&dvc, (size_t)ngrid * 8) ||
-        dalloc(s, (void **)&dmx, mb) || dalloc(s, (void **)&dmc, mb)) {
+        dalloc(s, (void **)&dmx, mb) || dalloc(s, (void **)&dmc, mb) ||
+        dalloc(s, (void **)&dws, dgemm_ws_bytes(nsig, nsig, ngrid))) {
       rc = NGW_ERR_OOM;
       break;
     }
@@ -209,9 +212,9 @@ extern "C" int ngw_vxc_matrix(ngw_session *s, int ngrid, int nmem, const double 
     const double nt = (double)ntrans, zero = 0.0;
     for (int w = 0; w < 2 && rc == NGW_OK; ++w) {
       k_grid_scale_cols<<<dim3(bx, ygrid(nsig)), 256, 0, s->stream>>>(dps, w == 0 ? dvx : dvc, ngrid, nsig, dw);
-      if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, nsig, nsig, ngrid, &nt, dps, ngrid, dw, ngrid, &zero,
-                      w == 0 ? dmx : dmc, nsig) != CUBLAS_STATUS_SUCCESS) {
-        set_error("cublasDgemm (V_xc matrix) failed");
+      if (dgemm(s->stream, true, false, nsig, nsig, ngrid, nt, dps, ngrid, dw, ngrid, zero, w == 0 ? dmx : dmc,
+                nsig, dws, dgemm_ws_bytes(nsig, nsig, ngrid)) != cudaSuccess) {
+        set_error("FP64 GEMM (V_xc matrix) failed");
         rc = NGW_ERR_CUDA;
       }
     }
@@ -231,6 +234,7 @@ extern "C" int ngw_vxc_matrix(ngw_session *s, int ngrid, int nmem, const double 
   dfree(s, dvc, (size_t)ngrid * 8);
   dfree(s, dmx, mb);
   dfree(s, dmc, mb);
+  dfree(s, dws, dgemm_ws_bytes(nsig, nsig, ngrid));
   if (rc != NGW_OK) return rc;
   for (size_t i = 0; i < (size_t)nsig * nsig; ++i) {
     vxc[i] = mx[i] + mc[i];

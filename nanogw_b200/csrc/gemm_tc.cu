@@ -1407,17 +1407,12 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
     NGW_TRY(rc);
     NGW_CUDA(cudaGetLastError());
   }
-  // D = M * C (FP64, cuBLAS), then split into A3[cv][mu] with the -U/(4s) columns
+  // D = M * C (FP64 tensor-core GEMM), then split into A3[cv][mu] with the -U/(4s) columns
   PoolTmp td(s);
   NGW_CUDA(pool_alloc(s, &td.p, (size_t)s->n_isdf * s->ncv * sizeof(double)));
   double *D = static_cast<double *>(td.p);
-  cublasStatus_t cst = cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_N, s->n_isdf, s->ncv,
-                                   s->n_isdf, &one, s->d_M, s->n_isdf, s->d_C, s->n_isdf, &zero,
-                                   D, s->n_isdf);
-  if (cst != CUBLAS_STATUS_SUCCESS) {
-    set_error("cublasDgemm (M*C) failed %d", (int)cst);
-    return NGW_ERR_CUDA;
-  }
+  NGW_CUDA(dgemm(st, false, false, s->n_isdf, s->ncv, s->n_isdf, one, s->d_M, s->n_isdf, s->d_C, s->n_isdf,
+                 zero, D, s->n_isdf));
   {
     int bx = (s->n_isdf + kdef + 127) / 128;
     k_split_rows<<<dim3(bx, ygrid(s->ncv)), 128, 0, st>>>(D, s->n_isdf, s->ncv, s->eig_U, kdef,
@@ -1927,8 +1922,8 @@ int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const dou
   const int ncv = s->ncv, k = op->kdef;
   const double one = 1.0, zero = 0.0;
   if (k > 0)   // xo = U^T v (FP64); v_perp and the U p(Lambda) xo term are fused below
-    NGW_CUBLAS(cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, k, nb, ncv, &one, s->eig_U, ncv, v, ldv,
-                           &zero, op->xo, k));
+    NGW_CUDA(dgemm(st, true, false, k, nb, ncv, one, s->eig_U, ncv, v, ldv, zero, op->xo, k,
+                   reinterpret_cast<double *>(op->ws), op->ws_bytes));
   {
     int bx = (ncv + 255) / 256;
     if (bx > 16) bx = 16;

@@ -4,10 +4,10 @@
 //   A = P_intp * Q_intp (Hadamard, N_mu x N_mu)            (:574-576)
 //   B = P * Q           (Hadamard, N_mu x N_grid)          (:585-587)
 //   A Z = B  (LU with partial pivoting, pdgesv :617/:629); zeta = Z^T.
-// P and Q products are cuBLAS DGEMMs, the Hadamard products and the row
-// gather are kernels of this library, the LU is cuSOLVER getrf/getrs.
-#include <cusolverDn.h>
-
+// P and Q products run on the FP64 tensor-core GEMM, the Hadamard products,
+// the row gather and the transpose are kernels of this library, and the LU
+// factorisation with partial pivoting and its solve are this library's own
+// (lu.cu).
 #include <algorithm>
 #include <vector>
 
@@ -28,19 +28,42 @@ __global__ void k_hadamard(double *__restrict__ x, const double *__restrict__ y,
     x[i] = x[i] * y[i];
 }
 
+int lu_factor(ngw_session *s, int n, double *A, int lda, std::vector<int> &hipiv);
+int lu_solve(ngw_session *s, int n, int nrhs, const double *LU, int lda, const std::vector<int> &hipiv, double *B,
+             int ldb, double *work);
+
+// out (cols x rows) = in^T for a column-major rows x cols matrix, through
+// 32 x 32 shared-memory tiles (coalesced reads and writes)
+__global__ void k_transpose(const double *__restrict__ in, int rows, int cols, double *__restrict__ out) {
+  __shared__ double t[32][33];
+  for (int c0 = blockIdx.y * 32; c0 < cols; c0 += gridDim.y * 32)
+    for (int r0 = blockIdx.x * 32; r0 < rows; r0 += gridDim.x * 32) {
+      for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+        const int r = r0 + threadIdx.x, c = c0 + q;
+        if (r < rows && c < cols) t[q][threadIdx.x] = in[(size_t)c * rows + r];
+      }
+      __syncthreads();
+      for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+        const int c = c0 + threadIdx.x, r = r0 + q;
+        if (r < rows && c < cols) out[(size_t)r * cols + c] = t[threadIdx.x][q];
+      }
+      __syncthreads();
+    }
+}
+
+void launch_transpose(const double *in, int rows, int cols, double *out, cudaStream_t st) {
+  const dim3 grid((unsigned)std::min((rows + 31) / 32, 4096), (unsigned)std::min((cols + 31) / 32, 1024));
+  k_transpose<<<grid, dim3(32, 8), 0, st>>>(in, rows, cols, out);
+}
+
 int isdf_fit_device(ngw_session *s, int ngrid, int nmem, const double *d_psi, const int *d_intp,
                     int n_isdf, int mv, double *d_psi_intp, double *d_zeta_t) {
   // d_zeta_t receives Z = zeta^T (n_isdf x ngrid, column-major)
-  double *P = nullptr, *Q = nullptr, *Ai = nullptr, *Qi = nullptr, *work = nullptr;
-  int *ipiv = nullptr, *info = nullptr;
-  cusolverDnHandle_t sol = nullptr;
-  void *hv = nullptr;
+  double *P = nullptr, *Q = nullptr, *Ai = nullptr, *Qi = nullptr;
   int rc = NGW_OK;
   const size_t pb = (size_t)n_isdf * ngrid * 8, ab = (size_t)n_isdf * n_isdf * 8;
-  int lwork = 0;
   do {
-    if (dalloc(s, (void **)&Q, pb) || dalloc(s, (void **)&Ai, ab) || dalloc(s, (void **)&Qi, ab) ||
-        dalloc(s, (void **)&ipiv, (size_t)n_isdf * 4) || dalloc(s, (void **)&info, 4)) {
+    if (dalloc(s, (void **)&Q, pb) || dalloc(s, (void **)&Ai, ab) || dalloc(s, (void **)&Qi, ab)) {
       rc = NGW_ERR_OOM;
       break;
     }
@@ -48,56 +71,39 @@ int isdf_fit_device(ngw_session *s, int ngrid, int nmem, const double *d_psi, co
     k_gather_rows<<<dim3((n_isdf + 255) / 256, nmem), 256, 0, s->stream>>>(d_psi, ngrid, d_intp, n_isdf,
                                                                            nmem, d_psi_intp);
     const double one = 1.0, zero = 0.0;
-    // P = psi_intp[:, :mv] psi[:, :mv]^T ; Q = psi_intp psi^T
-    if (cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n_isdf, ngrid, mv, &one, d_psi_intp, n_isdf, d_psi,
-                    ngrid, &zero, P, n_isdf) != CUBLAS_STATUS_SUCCESS ||
-        cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n_isdf, ngrid, nmem, &one, d_psi_intp, n_isdf, d_psi,
-                    ngrid, &zero, Q, n_isdf) != CUBLAS_STATUS_SUCCESS ||
-        cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n_isdf, n_isdf, mv, &one, d_psi_intp, n_isdf,
-                    d_psi_intp, n_isdf, &zero, Ai, n_isdf) != CUBLAS_STATUS_SUCCESS ||
-        cublasDgemm(s->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n_isdf, n_isdf, nmem, &one, d_psi_intp, n_isdf,
-                    d_psi_intp, n_isdf, &zero, Qi, n_isdf) != CUBLAS_STATUS_SUCCESS) {
-      set_error("cublasDgemm (ISDF P/Q products) failed");
+    // P = psi_intp[:, :mv] psi[:, :mv]^T ; Q = psi_intp psi^T (FP64 tensor-core GEMMs)
+    if (dgemm(s->stream, false, true, n_isdf, ngrid, mv, one, d_psi_intp, n_isdf, d_psi, ngrid, zero, P,
+              n_isdf) != cudaSuccess ||
+        dgemm(s->stream, false, true, n_isdf, ngrid, nmem, one, d_psi_intp, n_isdf, d_psi, ngrid, zero, Q,
+              n_isdf) != cudaSuccess ||
+        dgemm(s->stream, false, true, n_isdf, n_isdf, mv, one, d_psi_intp, n_isdf, d_psi_intp, n_isdf, zero,
+              Ai, n_isdf) != cudaSuccess ||
+        dgemm(s->stream, false, true, n_isdf, n_isdf, nmem, one, d_psi_intp, n_isdf, d_psi_intp, n_isdf, zero,
+              Qi, n_isdf) != cudaSuccess) {
+      set_error("FP64 GEMM (ISDF P/Q products) failed");
       rc = NGW_ERR_CUDA;
       break;
     }
     k_hadamard<<<2048, 256, 0, s->stream>>>(P, Q, (size_t)n_isdf * ngrid);
     k_hadamard<<<256, 256, 0, s->stream>>>(Ai, Qi, (size_t)n_isdf * n_isdf);
-    if ((rc = session_cusolver(s, &hv)) != NGW_OK) break;
-    sol = (cusolverDnHandle_t)hv;
-    if (cusolverDnDgetrf_bufferSize(sol, n_isdf, n_isdf, Ai, n_isdf, &lwork) != CUSOLVER_STATUS_SUCCESS ||
-        dalloc(s, (void **)&work, (size_t)std::max(lwork, 1) * 8)) {
-      set_error("getrf workspace failed");
+    if (cudaGetLastError() != cudaSuccess) {
+      set_error("ISDF Hadamard kernels failed");
       rc = NGW_ERR_CUDA;
       break;
     }
-    if (cusolverDnDgetrf(sol, n_isdf, n_isdf, Ai, n_isdf, work, ipiv, info) != CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnDgetrs(sol, CUBLAS_OP_N, n_isdf, ngrid, Ai, n_isdf, ipiv, P, n_isdf, info) !=
-            CUSOLVER_STATUS_SUCCESS) {
-      set_error("cusolver getrf/getrs failed");
-      rc = NGW_ERR_CUDA;
-      break;
-    }
-    int hinfo = 0;
-    if (cudaMemcpyAsync(&hinfo, info, 4, cudaMemcpyDeviceToHost, s->stream) ||
-        cudaStreamSynchronize(s->stream)) {
-      set_error("ISDF solve failed to complete");
-      rc = NGW_ERR_CUDA;
-      break;
-    }
-    if (hinfo != 0) {
-      set_error("ISDF matrix A is singular (getrf info %d): duplicate interpolation points?", hinfo);
-      rc = NGW_ERR_ARG;
-      break;
-    }
+    // A Z = B: LU with partial pivoting, then the solve (Q is free again and
+    // serves as its workspace)
+    std::vector<int> piv;
+    rc = lu_factor(s, n_isdf, Ai, n_isdf, piv);
+    if (rc == NGW_ERR_ARG)
+      set_error("ISDF matrix A is singular (zero pivot): duplicate interpolation points?");
+    if (rc != NGW_OK) break;
+    rc = lu_solve(s, n_isdf, ngrid, Ai, n_isdf, piv, P, n_isdf, Q);
   } while (0);
   cudaStreamSynchronize(s->stream);
   dfree(s, Q, pb);
   dfree(s, Ai, ab);
   dfree(s, Qi, ab);
-  dfree(s, ipiv, (size_t)n_isdf * 4);
-  dfree(s, info, 4);
-  if (work) dfree(s, work, (size_t)std::max(lwork, 1) * 8);
   return rc;
 }
 
@@ -169,10 +175,9 @@ extern "C" int ngw_build_isdf_kernel(ngw_session *s, int ngrid, int nmem, const 
       rc = NGW_ERR_OOM;
       break;
     }
-    const double one = 1.0, zero = 0.0;
-    if (cublasDgeam(s->cublas, CUBLAS_OP_T, CUBLAS_OP_T, ngrid, n_isdf, &one, dzt, n_isdf, &zero, dzt, n_isdf,
-                    dz, ngrid) != CUBLAS_STATUS_SUCCESS) {
-      set_error("cublasDgeam (zeta transpose) failed");
+    launch_transpose(dzt, n_isdf, ngrid, dz, s->stream);
+    if (cudaGetLastError() != cudaSuccess) {
+      set_error("zeta transpose failed");
       rc = NGW_ERR_CUDA;
       break;
     }

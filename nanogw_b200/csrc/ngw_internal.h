@@ -146,6 +146,17 @@ void bump_generation(ngw_session *s);
 // session's cuSOLVER dense handle on the session stream (created on first use)
 int session_cusolver(ngw_session *s, void **handle);
 
+// ---- FP64 GEMM on the FP64 tensor cores (dgemm.cu) ----
+// C = alpha op(A) op(B) + beta C, column-major (cuBLAS conventions).  With a
+// workspace (ws, ws_bytes) shapes with a small tile grid split K into slices
+// summed in order; without one they run unsplit.  Launch-only: safe inside
+// stream capture once the kernel has run outside one.
+cudaError_t dgemm(cudaStream_t st, bool ta, bool tb, int m, int n, int k, double alpha, const double *A,
+                  int lda, const double *B, int ldb, double beta, double *C, int ldc, double *ws = nullptr,
+                  size_t ws_bytes = 0);
+// workspace that lets dgemm() choose any split for an m x n result
+size_t dgemm_ws_bytes(int m, int n, int k);
+
 // ---- FP64 path kernels (kernels_core.cu) ----
 void launch_pair_gather_f64(const double *psi, int n_isdf, const int *cvpair, int ncv,
                             double *C, cudaStream_t st);

@@ -105,7 +105,10 @@ int poisson_apply(ngw_session *s, int ngrid, int ncol, const double *drho, const
   const int n = nfft;
   const size_t bsz = (size_t)n * n * n;
   const size_t csz = (size_t)n * n * (n / 2 + 1);
+  // columns per FFT pass: a 2 GiB box + spectrum budget (NGW_POISSON_BATCH
+  // fixes the count: tests of the chunked path at small sizes)
   int batch = (int)std::max<size_t>(1, (size_t)(2ull << 30) / (bsz * 8 + csz * 16));
+  if (const char *e = getenv("NGW_POISSON_BATCH")) batch = std::max(1, atoi(e));
   if (batch > ncol) batch = ncol;
   double *box = nullptr, *vtab = nullptr;
   cufftDoubleComplex *spec = nullptr;
@@ -194,7 +197,7 @@ int poisson_apply(ngw_session *s, int ngrid, int ncol, const double *drho, const
 // (ngrid x n_isdf, column-major) and grid coordinates (3 x ngrid).
 int coulomb_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const int *dg, int nfft,
                  double h, double trunc, double *dm) {
-  double *dvz = nullptr;
+  double *dvz = nullptr, *dws = nullptr;
   int rc = NGW_OK;
   do {
     if (dalloc(s, (void **)&dvz, (size_t)ngrid * n_isdf * 8)) {
@@ -204,15 +207,21 @@ int coulomb_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const 
     if ((rc = poisson_apply(s, ngrid, n_isdf, dz, dg, nfft, h, trunc, dvz)) != NGW_OK) break;
     const double nf = 1.0 / (h * h * h);
     const double zero = 0.0;
-    if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n_isdf, n_isdf, ngrid, &nf, dz, ngrid, dvz, ngrid,
-                    &zero, dm, n_isdf) != CUBLAS_STATUS_SUCCESS) {
-      set_error("cublasDgemm (zeta^T v zeta) failed");
+    const size_t wsb = (size_t)8 * n_isdf * n_isdf * 8;   // up to 8 K slices
+    if (dalloc(s, (void **)&dws, wsb)) {
+      rc = NGW_ERR_OOM;
+      break;
+    }
+    if (dgemm(s->stream, true, false, n_isdf, n_isdf, ngrid, nf, dz, ngrid, dvz, ngrid, zero, dm, n_isdf, dws,
+              wsb) != cudaSuccess) {
+      set_error("FP64 GEMM (zeta^T v zeta) failed");
       rc = NGW_ERR_CUDA;
       break;
     }
   } while (0);
   cudaStreamSynchronize(s->stream);
   dfree(s, dvz, (size_t)ngrid * n_isdf * 8);
+  dfree(s, dws, (size_t)8 * n_isdf * n_isdf * 8);
   return rc;
 }
 
@@ -293,11 +302,11 @@ __global__ void k_scale_cols_by(const double *__restrict__ z, const double *__re
 // M_xc = (ntrans / hcub) zeta^T (f_xc * zeta) from device-resident zeta and rho.
 int fxc_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const double *drho, double h,
              double *dm, double *dfxc) {
-  double *dfz = nullptr;
-  const size_t zb = (size_t)ngrid * n_isdf * 8;
+  double *dfz = nullptr, *dws = nullptr;
+  const size_t zb = (size_t)ngrid * n_isdf * 8, wsb = (size_t)8 * n_isdf * n_isdf * 8;
   int rc = NGW_OK;
   do {
-    if (dalloc(s, (void **)&dfz, zb)) {
+    if (dalloc(s, (void **)&dfz, zb) || dalloc(s, (void **)&dws, wsb)) {
       rc = NGW_ERR_OOM;
       break;
     }
@@ -305,15 +314,16 @@ int fxc_core(ngw_session *s, int ngrid, int n_isdf, const double *dz, const doub
     k_scale_cols_by<<<dim3(std::min(256, (ngrid + 255) / 256), n_isdf), 256, 0, s->stream>>>(
         dz, dfxc, ngrid, n_isdf, dfz);
     const double nf = 1.0 / (h * h * h), zero = 0.0;
-    if (cublasDgemm(s->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n_isdf, n_isdf, ngrid, &nf, dz, ngrid, dfz, ngrid,
-                    &zero, dm, n_isdf) != CUBLAS_STATUS_SUCCESS) {
-      set_error("cublasDgemm (zeta^T f zeta) failed");
+    if (dgemm(s->stream, true, false, n_isdf, n_isdf, ngrid, nf, dz, ngrid, dfz, ngrid, zero, dm, n_isdf, dws,
+              wsb) != cudaSuccess) {
+      set_error("FP64 GEMM (zeta^T f zeta) failed");
       rc = NGW_ERR_CUDA;
       break;
     }
   } while (0);
   cudaStreamSynchronize(s->stream);
   dfree(s, dfz, zb);
+  dfree(s, dws, wsb);
   return rc;
 }
 

