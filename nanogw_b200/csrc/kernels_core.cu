@@ -422,8 +422,10 @@ void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb,
 // chains; the reference recurrence has none).  Chain j keeps its Lanczos
 // vectors v_0 .. v_k in basis[j * ldb + q * ncv] (FP64).  Step k:
 //   w = w + t (k >= 1; at k = 0 w already holds p(H) v_0) ; a(k) = <w, v_k> ;
-//   if k + 1 < L:  w = w - a(k) v_k ; twice: h = V^T w, w = w - V h
-//   (classical Gram-Schmidt against v_0 .. v_k, applied twice) ; b(k+1) = ||w|| ;
+//   if k + 1 < L:  w = w - a(k) v_k ; h = V^T w, w = w - V h (classical
+//   Gram-Schmidt against v_0 .. v_k), repeated once when the pass shrank
+//   ||w|| below 1/sqrt(2) of its value (the "twice is enough" criterion of
+//   Daniel, Gragg, Kaufman and Stewart, Math. Comp. 30 (1976)) ; b(k+1) = ||w|| ;
 //   when prescale_next: w = w / b(k+1) (= v_{k+1}, also stored in the basis),
 //   v = -v b(k+1), hs = (R^1/2 or 1) w.
 // One CTA per chain; the dot products are summed eight at a time (warp
@@ -460,8 +462,14 @@ __global__ void __launch_bounds__(LNT)
   const double ak = block_sum<LNT>(acc, sh);
   if (threadIdx.x == 0) a[(size_t)j * niter + k] = ak;
   if (k + 1 >= L) return;
-  for (int i = threadIdx.x; i < ncv; i += LNT) wj[i] = wj[i] - ak * vj[i];
-  __syncthreads();
+  acc = 0.0;
+  for (int i = threadIdx.x; i < ncv; i += LNT) {
+    const double wi = wj[i] - ak * vj[i];
+    wj[i] = wi;
+    acc += wi * wi;
+  }
+  double nrm2 = block_sum<LNT>(acc, sh);   // ||w||^2 before the pass
+  double out2 = 0.0;                        // ||w||^2 after the last pass
   for (int pass = 0; pass < 2; ++pass) {
     // h_q = <v_q, w>, q = 0 .. k
     for (int q0 = 0; q0 <= k; q0 += RG_Q) {
@@ -492,17 +500,20 @@ __global__ void __launch_bounds__(LNT)
       }
       __syncthreads();
     }
-    // w = w - V h
+    // w = w - V h, and the new ||w||^2
+    acc = 0.0;
     for (int i = threadIdx.x; i < ncv; i += LNT) {
       double u = 0.0;
       for (int q = 0; q <= k; ++q) u += hq[q] * Vj[(size_t)q * ncv + i];
-      wj[i] = wj[i] - u;
+      const double wi = wj[i] - u;
+      wj[i] = wi;
+      acc += wi * wi;
     }
-    __syncthreads();
+    out2 = block_sum<LNT>(acc, sh);
+    if (out2 >= 0.5 * nrm2) break;   // the pass kept most of w: once is enough
+    nrm2 = out2;
   }
-  acc = 0.0;
-  for (int i = threadIdx.x; i < ncv; i += LNT) acc += wj[i] * wj[i];
-  const double bk1 = sqrt(block_sum<LNT>(acc, sh));
+  const double bk1 = sqrt(out2);
   const bool stop = clen && eps > 0.0 && bk1 < eps;
   if (threadIdx.x == 0) {
     b[(size_t)j * niter + k + 1] = bk1;

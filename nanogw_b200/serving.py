@@ -67,6 +67,12 @@ class SigmaRequest:
     def ncv(self):
         return self.nval * (self.nmem - self.nval)
 
+    def work(self):
+        """Matvec work of the request (chain-steps x the operator's size), the
+        ordering key of the largest-first policy."""
+        n = self.psi_intp.shape[0]
+        return float(len(self.qp_bands)) * self.nmem * self.niter * n * (2.0 * self.ncv + n)
+
     def footprint_bytes(self):
         """Device memory the request needs: operator (FP64 + split-BF16 +
         pair products) and Lanczos / Clenshaw state of all its chains."""
@@ -134,11 +140,17 @@ class SigmaServer:
         req.sigma = sig
         req.eqp = eqp
 
-    def run(self, requests, realtime=True):
+    def run(self, requests, realtime=True, policy="fifo"):
         """Serve `requests` (arrival times in seconds from the start).  With
         realtime=False every request is available at t=0 (closed loop).
+        Among the requests waiting for a slot, policy "fifo" admits the
+        earliest arrival first and "largest" the one with the most matvec
+        work first (longest-processing-time order: on a closed batch of
+        uneven requests the largest no longer starts last and runs alone).
         Requests larger than the whole budget are refused (``req.error`` is
         an NGWError with code NGW_ERR_BUDGET) and counted in ``refused``."""
+        if policy not in ("fifo", "largest"):
+            raise ValueError("policy must be 'fifo' or 'largest'")
         reqs = sorted(requests, key=lambda r: r.arrival)
         lock = threading.Condition()
         free = list(range(self.nworkers))
@@ -176,7 +188,8 @@ class SigmaServer:
             while i < len(reqs) or pending or inflight:
                 now = time.perf_counter() - t0
                 while i < len(reqs) and (not realtime or reqs[i].arrival <= now):
-                    heapq.heappush(pending, (reqs[i].arrival, reqs[i].rid, reqs[i]))
+                    key = reqs[i].arrival if policy == "fifo" else -reqs[i].work()
+                    heapq.heappush(pending, (key, reqs[i].rid, reqs[i]))
                     i += 1
                 admitted = False
                 while pending and free:

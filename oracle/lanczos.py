@@ -58,12 +58,23 @@ def polynomial_matvec_isdf(vec, polynomial, cmtrx, mmtrx, sqrtR, matvec=None):
 
 
 def _gram_schmidt_twice(basis, w, sel, k):
-    """w -= V (V^T w), twice, with V the chains' vectors v_0 .. v_k
-    (basis: (blksz, niter + 1, ncv); w: (ncv, len(sel)))."""
+    """w -= V (V^T w) with V the chains' vectors v_0 .. v_k (basis:
+    (blksz, niter + 1, ncv); w: (ncv, len(sel))), repeated once for the
+    chains whose pass shrank ||w|| below 1/sqrt(2) of its value ("twice is
+    enough": Daniel, Gragg, Kaufman and Stewart, Math. Comp. 30 (1976))."""
     Vs = basis[:, : k + 1, :] if len(sel) == basis.shape[0] else basis[sel, : k + 1, :]
+    before = np.einsum("ij,ij->j", w, w)
+    again = np.ones(w.shape[1], dtype=bool)
     for _ in range(2):
-        h = np.matmul(Vs, w.T[:, :, None])                       # (nsel, k+1, 1)
-        w = w - np.matmul(Vs.transpose(0, 2, 1), h)[:, :, 0].T
+        idx = np.nonzero(again)[0]
+        if len(idx) == 0:
+            break
+        V = Vs[idx]
+        h = np.matmul(V, w[:, idx].T[:, :, None])                # (n, k+1, 1)
+        w[:, idx] = w[:, idx] - np.matmul(V.transpose(0, 2, 1), h)[:, :, 0].T
+        after = np.einsum("ij,ij->j", w[:, idx], w[:, idx])
+        again[idx] = after < 0.5 * before[idx]
+        before[idx] = after
     return w
 
 

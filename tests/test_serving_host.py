@@ -100,3 +100,19 @@ def test_idle_resident_memory_counts_and_is_released():
     assert srv.released >= 1                 # an idle session gave its memory back
     assert srv.peak_used <= srv.budget
     assert sum(srv.held) <= srv.budget
+
+
+def test_largest_first_policy_orders_admission():
+    order = []
+
+    def solver(w, req):
+        order.append(req.rid)
+        time.sleep(0.01)
+
+    reqs = [_req(0, 1, 0.0, n=32), _req(1, 2, 0.0, n=128), _req(2, 3, 0.0, n=64)]
+    srv = SigmaServer(workers=1, solver=solver)
+    srv.run(reqs, realtime=False, policy="largest")
+    assert order == [1, 2, 0]
+    order.clear()
+    srv.run([_req(0, 1, 0.0, n=32), _req(1, 2, 0.0, n=128), _req(2, 3, 0.0, n=64)], realtime=False)
+    assert order == [0, 1, 2]
