@@ -27,6 +27,7 @@ int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const dou
 void mixed_free(ngw_session *s);
 void monomial_to_chebyshev(const double *poly_hl, int n, double lo, double hi, double *g);
 
+
 static thread_local char g_err[1024] = {0};
 
 void set_error(const char *fmt, ...) {
@@ -157,7 +158,7 @@ enum {
   SL_IN = 0, SL_OUT, SL_HS, SL_T1, SL_T2, SL_Z, SL_VEC, SL_WVEC, SL_TMP, SL_A, SL_B, SL_ZZ,
   SL_SPEC, SL_CMN, SL_CM, SL_P, SL_P2, SL_PN2, SL_PN, SL_CHB, SL_CHQ, SL_E1, SL_ZZ0, SL_SIG,
   SL_KR, SL_KC, SL_KM, SL_B1, SL_B2, SL_QPW, SL_QPIO, SL_SPECS, SL_CLEN, SL_LEN, SL_SLOT, SL_BASIS,
-  SL_DGWS, SL_NUM
+  SL_DGWS, SL_GROUP, SL_NUM
 };
 
 // ---------------------------------------------------------------------------
@@ -634,10 +635,11 @@ static int sigma_block_setup(SigmaJob &J, int q0) {
   return NGW_OK;
 }
 
-// The device work of one block, launch-only (graph-capturable).
-static int sigma_region(SigmaJob &J) {
+// The device work of one block, launch-only (graph-capturable), in three
+// parts: start vectors and chain set-up, the Lanczos recurrence, spectra and
+// the Sigma_c sum.
+static int sigma_start(SigmaJob &J) {
   ngw_session *s = J.s;
-  const ngw_sigma_params *p = J.p;
   const int n = J.n, ncv = J.ncv, nb = J.nb, niter = J.niter, tamm_d = J.tamm_d;
   const double one = 1.0, zero = 0.0;
   // start vectors  P = sqrtR * C^T M (psi_m psi_n)   (F90z:578-709), FP64
@@ -653,12 +655,80 @@ static int sigma_region(SigmaJob &J) {
   launch_sqrt_vec(J.pn2, J.pn, nb, s->stream);
   launch_lanczos_init(J.P2, ncv, J.pn, J.V, J.hs, s->d_sqrtR, ncv, nb, tamm_d, J.b, niter, J.dlen, J.clen,
                       s->stream);
-  NGW_TRY(lanczos_dev(s, J.pp, nb, niter, J.V, J.W, J.hs, J.tmp, J.a, J.b, J.clen, p->early_exit_eps,
-                      J.len ? &J.nact : nullptr, J.basis, J.ldb));
+  NGW_CUDA(cudaGetLastError());
+  return NGW_OK;
+}
+
+static int sigma_end(SigmaJob &J) {
+  ngw_session *s = J.s;
+  const ngw_sigma_params *p = J.p;
+  const int nb = J.nb, niter = J.niter, tamm_d = J.tamm_d;
   launch_sigma_spectra(J.a, J.b, niter, nb, J.de1, J.chb + nb, J.chq, J.zz0, J.de, J.nen, p->ecuts, p->nval,
                        J.S, J.clen, s->stream);
   launch_sigma_reduce(J.S, J.pn2, J.de1, J.chb + nb, J.zz0 + J.q0, J.de, J.nen, p->ecuts, p->nval, J.nbsum,
                       J.nq, tamm_d, J.sig + (size_t)2 * J.q0 * J.nen, 0, J.dslot, s->stream);
+  NGW_CUDA(cudaGetLastError());
+  return NGW_OK;
+}
+
+static int sigma_region(SigmaJob &J) {
+  NGW_TRY(sigma_start(J));
+  NGW_TRY(lanczos_dev(J.s, J.pp, J.nb, J.niter, J.V, J.W, J.hs, J.tmp, J.a, J.b, J.clen, J.p->early_exit_eps,
+                      J.len ? &J.nact : nullptr, J.basis, J.ldb));
+  return sigma_end(J);
+}
+
+// The Lanczos recurrences of several molecules (mixed precision) in lock
+// step, their p(C) v products through grouped GEMM launches (one GEMM1 and
+// one GEMM2 launch per Clenshaw term for all molecules still running), the
+// per-chain updates per molecule.  Same arithmetic per chain as lanczos_dev
+// with the grouped tiles.  Launch-only; everything on stream st.
+static int lanczos_grouped(std::vector<SigmaJob> &jobs, std::vector<GroupMember> &mem, const GroupPlan &P,
+                           cudaStream_t st) {
+  const int G = (int)jobs.size();
+  std::vector<double *> vec(G), wvec(G);
+  std::vector<const double *> vin(G);
+  for (int i = 0; i < G; ++i) vin[i] = jobs[i].V;
+  NGW_TRY(group_poly_apply(P, mem, 0, vin.data(), st));   // W = p(H) V
+  for (int i = 0; i < G; ++i) {
+    SigmaJob &J = jobs[i];
+    ngw_session *s = J.s;
+    const double eps = J.p->early_exit_eps;
+    if (J.basis) {
+      launch_lanczos_reorth_step(J.W, J.V, nullptr, s->ncv, J.nb, 0, J.a, J.b, J.niter, s->d_sqrtR, nullptr, 0,
+                                 J.niter >= 2 ? 1 : 0, J.clen, eps, J.basis, J.ldb, st);
+    } else {
+      launch_lanczos_first(J.W, J.V, s->ncv, J.nb, J.a, J.b, J.niter, J.clen, eps, st);
+      if (J.niter >= 2)
+        launch_lanczos_prescale(J.W, J.V, s->ncv, P.nv[(size_t)1 * G + i], 1, J.b, J.niter, s->d_sqrtR, nullptr,
+                                0, J.clen, st);
+    }
+    vec[i] = J.W;
+    wvec[i] = J.V;
+  }
+  for (int k = 1; k < P.steps; ++k) {
+    bool any = false;
+    for (int i = 0; i < G; ++i) {
+      vin[i] = vec[i];
+      any = any || P.nv[(size_t)k * G + i] > 0;
+    }
+    if (!any) break;
+    NGW_TRY(group_poly_apply(P, mem, k, vin.data(), st));   // tmp = p(H) vec
+    for (int i = 0; i < G; ++i) {
+      SigmaJob &J = jobs[i];
+      const int nk = P.nv[(size_t)k * G + i];
+      if (nk <= 0) continue;
+      ngw_session *s = J.s;
+      const double eps = J.p->early_exit_eps;
+      if (J.basis)
+        launch_lanczos_reorth_step(wvec[i], vec[i], J.tmp, s->ncv, nk, k, J.a, J.b, J.niter, s->d_sqrtR, nullptr,
+                                   0, (k + 1 < J.niter) ? 1 : 0, J.clen, eps, J.basis, J.ldb, st);
+      else
+        launch_lanczos_step(wvec[i], vec[i], J.tmp, s->ncv, nk, k, J.a, J.b, J.niter, s->d_sqrtR, nullptr, 0,
+                            (k + 1 < J.niter) ? 1 : 0, J.clen, eps, st);
+      if (k + 1 < J.niter) std::swap(vec[i], wvec[i]);
+    }
+  }
   NGW_CUDA(cudaGetLastError());
   return NGW_OK;
 }
@@ -1132,6 +1202,64 @@ int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_s
     NGW_TRY(sigma_block_setup(jobs[i], 0));
   }
   ngw_session *s0 = sessions[0];
+  // Grouped mode (default when every entry is mixed precision, not TDA, with
+  // one polynomial degree): the molecules' Lanczos recurrences run in lock
+  // step on session 0's stream and each Clenshaw term of their p(C) v is one
+  // grouped GEMM1 and one grouped GEMM2 launch over all of them.
+  // NGW_BATCH_MODE=branches keeps one graph branch per molecule.
+  bool grouped = count > 1;
+  if (const char *e = getenv("NGW_BATCH_MODE"))
+    if (std::string(e) == "branches") grouped = false;
+  for (int i = 0; i < count && grouped; ++i)
+    if (sessions[i]->precision != NGW_PREC_MIXED || jobs[i].tamm_d || jobs[i].pp.npoly != jobs[0].pp.npoly ||
+        (int)jobs[i].pp.cheb.size() != jobs[0].pp.npoly + 1)
+      grouped = false;
+  if (grouped) {
+    int steps = 0;
+    for (auto &J : jobs) steps = std::max(steps, J.niter);
+    std::vector<std::vector<int>> nact(count);
+    std::vector<GroupMember> mem(count);
+    for (int i = 0; i < count; ++i) {
+      SigmaJob &J = jobs[i];
+      nact[i].assign(steps, 0);
+      for (int k = 0; k < J.niter; ++k) nact[i][k] = J.len ? J.nact[k] : J.nb;
+      mem[i] = GroupMember{J.s, J.pp.cheb.data(), J.pp.c0, J.pp.c1, J.ncv, J.W, J.tmp, J.nb, nact[i].data()};
+    }
+    const int n = jobs[0].pp.npoly;
+    void *buf = nullptr;
+    NGW_TRY(scratch(s0, SL_GROUP, group_bytes(count, n, steps), &buf));
+    GroupPlan P;
+    NGW_TRY(group_build(mem, n, 0, steps, buf, s0->stream, P));
+    std::vector<unsigned long long> key = {0x6A0DBull, (unsigned long long)count, (unsigned long long)(uintptr_t)buf};
+    for (int i = 0; i < count; ++i) {
+      key.push_back((unsigned long long)(uintptr_t)sessions[i]);
+      sigma_key(jobs[i], key);
+    }
+    std::vector<cudaStream_t> saved(count);
+    for (int i = 0; i < count; ++i) {
+      saved[i] = sessions[i]->stream;
+      sessions[i]->stream = s0->stream;   // every launch of the batch on one stream
+    }
+    auto region = [&]() -> int {
+      for (int i = 0; i < count; ++i) NGW_TRY(sigma_start(jobs[i]));
+      NGW_TRY(lanczos_grouped(jobs, mem, P, s0->stream));
+      for (int i = 0; i < count; ++i) NGW_TRY(sigma_end(jobs[i]));
+      return NGW_OK;
+    };
+    int rc;
+    {
+      std::shared_lock<std::shared_mutex> busy(gpu_quiet_lock(s0->device));   // no tuning meanwhile
+      rc = run_graphed(s0, key, region);
+      if (rc == NGW_OK && cudaStreamSynchronize(s0->stream) != cudaSuccess) {
+        set_error("ngw_sigma_lanczos_batch: %s", cudaGetErrorString(cudaGetLastError()));
+        rc = NGW_ERR_CUDA;
+      }
+    }
+    for (int i = 0; i < count; ++i) sessions[i]->stream = saved[i];
+    NGW_TRY(rc);
+    for (int i = 0; i < count; ++i) NGW_TRY(sigma_finish(jobs[i], sigma_c[i]));
+    return NGW_OK;
+  }
   // one graph for the whole batch: entry i is a branch on its session's
   // stream, forked from and joined back into session 0's stream
   std::vector<unsigned long long> key = {0xBA7C4ull, (unsigned long long)count};

@@ -161,14 +161,15 @@ __device__ __forceinline__ void clen_store(const EpiParams &ep, const ClenCoef &
   }
 }
 
-// One 128 x BN output tile per CTA (split-K slice blockIdx.z): warp 0 issues
+// One 128 x BN output tile (rows m0.., columns n0.., split-K slice `split`,
+// `tile` its index for the split-K workspace) of a CTA: warp 0 issues
 // the TMA loads, warp 1 the MMAs into TMEM, then all 8 warps run the epilogue.
-template <int BN, int STAGES, int MINB, bool FUSED, bool CRED = false>
-__global__ void __launch_bounds__(NTHREADS, MINB)
-    k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
-              const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
-              const __grid_constant__ CUtensorMap tRx, const __grid_constant__ CUtensorMap tRb2,
-              const __grid_constant__ CUtensorMap tRv, GemmArgs ga, EpiParams ep, int *status) {
+template <int BN, int STAGES, bool FUSED, bool CRED>
+__device__ __forceinline__ void tc_gemm_tile(const CUtensorMap *tA_hi, const CUtensorMap *tA_lo,
+                                             const CUtensorMap *tB_hi, const CUtensorMap *tB_lo,
+                                             const CUtensorMap *tRx, const CUtensorMap *tRb2,
+                                             const CUtensorMap *tRv, const GemmArgs &ga, const EpiParams &ep,
+                                             int m0, int n0, int split, int tile, int *status) {
   // FUSED: one stage holds A_hi, A_lo, B_hi, B_lo of a k-block and carries all
   // three split products; otherwise one stage is one (A, B) pair of a segment.
   constexpr uint32_t A_BYTES = BM * BK * 2;
@@ -189,8 +190,6 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
   __shared__ uint32_t tmem_base_sh;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  const int split = blockIdx.z;
   const int total_kb = FUSED ? ga.num_kb : ga.num_kb * ga.nseg;
   const int kb_per = (total_kb + ga.nsplit - 1) / ga.nsplit;
   const int kb_begin = split * kb_per;
@@ -206,8 +205,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     for (int g = 0; g < 2; ++g)
       for (int r = 0; r < 4; ++r) tc::mbar_init(tc::smem_u32(&ring_bar[g][r]), 1);
     tc::fence_barrier_init();
-    tc::prefetch_tmap(&tA_hi);
-    tc::prefetch_tmap(&tB_hi);
+    tc::prefetch_tmap(tA_hi);
+    tc::prefetch_tmap(tB_hi);
   }
   if (warp == 2) {
     tc::tmem_alloc(tc::smem_u32(&tmem_base_sh), TMEM_COLS);
@@ -232,15 +231,15 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
       const uint32_t sa = tc::smem_u32(smem + s * STAGE_BYTES);
       tc::mbar_arrive_expect_tx(bar, STAGE_BYTES);
       if (FUSED) {
-        tc::tma_load_2d(sa, &tA_hi, bar, kbg * BK, m0);
-        tc::tma_load_2d(sa + A_BYTES, &tA_lo, bar, kbg * BK, m0);
-        tc::tma_load_2d(sa + 2 * A_BYTES, &tB_hi, bar, kbg * BK, n0);
-        tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tB_lo, bar, kbg * BK, n0);
+        tc::tma_load_2d(sa, tA_hi, bar, kbg * BK, m0);
+        tc::tma_load_2d(sa + A_BYTES, tA_lo, bar, kbg * BK, m0);
+        tc::tma_load_2d(sa + 2 * A_BYTES, tB_hi, bar, kbg * BK, n0);
+        tc::tma_load_2d(sa + 2 * A_BYTES + B_BYTES, tB_lo, bar, kbg * BK, n0);
       } else {
         const int seg = kbg / ga.num_kb;
         const int kb = kbg - seg * ga.num_kb;
-        const CUtensorMap *ta = (seg == 2) ? &tA_lo : &tA_hi;   // (hi,hi) (hi,lo) (lo,hi)
-        const CUtensorMap *tb = (seg == 1) ? &tB_lo : &tB_hi;
+        const CUtensorMap *ta = (seg == 2) ? tA_lo : tA_hi;   // (hi,hi) (hi,lo) (lo,hi)
+        const CUtensorMap *tb = (seg == 1) ? tB_lo : tB_hi;
         tc::tma_load_2d(sa, ta, bar, kb * BK, m0);
         tc::tma_load_2d(sa + A_BYTES, tb, bar, kb * BK, n0);
       }
@@ -375,7 +374,6 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     cl.sync();   // no CTA leaves while another still reads its shared memory
   } else if (ep.kind == EPI_SPLIT) {
     const bool partial = ga.nsplit > 1;
-    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
     float *wsl = partial ? ep.ws + ((size_t)tile * ga.nsplit + split) * (size_t)(BN * BM) : nullptr;
     for (int ch = 2 * ch_begin; ch < 2 * ch_end; ++ch) {
       const int c = ch * 8;
@@ -431,9 +429,9 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
         const int nc = n0 + c_first + 8 * q;
         tc::mbar_arrive_expect_tx(bar, bytes);
         // b_{k+1}, b_{k+2}: one more read each at most; v: read by every GEMM2 of the step
-        tc::tma_load_2d_hint(dst, &tRx, bar, m0, nc, pol_once);
-        if (ep.b2) tc::tma_load_2d_hint(dst + OP8, &tRb2, bar, m0, nc, pol_once);
-        if (ep.v) tc::tma_load_2d_hint(dst + 2 * OP8, &tRv, bar, m0, nc, pol_keep);
+        tc::tma_load_2d_hint(dst, tRx, bar, m0, nc, pol_once);
+        if (ep.b2) tc::tma_load_2d_hint(dst + OP8, tRb2, bar, m0, nc, pol_once);
+        if (ep.v) tc::tma_load_2d_hint(dst + 2 * OP8, tRv, bar, m0, nc, pol_keep);
       };
       if (leader)
         for (int q = 0; q < nq && q < RS; ++q) issue(q);
@@ -502,6 +500,68 @@ __global__ void __launch_bounds__(NTHREADS, MINB)
     tc::tc_fence_after();
     tc::tmem_dealloc(tmem_d, TMEM_COLS);
   }
+}
+
+
+template <int BN, int STAGES, int MINB, bool FUSED, bool CRED = false>
+__global__ void __launch_bounds__(NTHREADS, MINB)
+    k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
+              const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
+              const __grid_constant__ CUtensorMap tRx, const __grid_constant__ CUtensorMap tRb2,
+              const __grid_constant__ CUtensorMap tRv, GemmArgs ga, EpiParams ep, int *status) {
+  tc_gemm_tile<BN, STAGES, FUSED, CRED>(&tA_hi, &tA_lo, &tB_hi, &tB_lo, &tRx, &tRb2, &tRv, ga, ep,
+                                        blockIdx.x * BM, blockIdx.y * BN, blockIdx.z,
+                                        blockIdx.y * gridDim.x + blockIdx.x, status);
+}
+
+// ---------------------------------------------------------------------------
+// Grouped launch across molecules: one grid holds the tiles of several
+// problems (one per molecule of a batch), each with its own operand tensor
+// maps, shapes and epilogue in a device table.  Block b belongs to the entry
+// g with tb[g] <= b < tb[g+1]; its tile t = b - tb[g] is (t % tiles_m,
+// t / tiles_m).  nv[g] is the entry's chain count at this launch (chains that
+// finished are not scheduled).  Fused stages, 64-wide N tiles, no split-K:
+// the molecules together fill the GPU.  Per tile the arithmetic is that of
+// k_tc_gemm<64, 4, 1, true> (variant 3), so a pinned variant-3 single call
+// gives the same bits.
+struct __align__(64) GroupEntry {
+  CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
+  EpiParams ep;
+  GemmArgs ga;
+  int tiles_m;
+};
+
+constexpr int GBN = 64, GSTAGES = 4;
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_tc_gemm_grouped(const GroupEntry *__restrict__ tab, const int *__restrict__ tb, const int *__restrict__ nv,
+                      int ng, int *status) {
+  __shared__ EpiParams sep;
+  __shared__ GemmArgs sga;
+  __shared__ int sg, stile, stm;
+  if (threadIdx.x == 0) {
+    int g = 0;
+    while (g + 1 < ng && (int)blockIdx.x >= tb[g + 1]) ++g;
+    // the tensor maps sit in global memory (written by a host copy): order
+    // those writes before this thread's tensor-map reads (it is the thread
+    // that issues the TMA loads)
+    const GroupEntry *eg = tab + g;
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&eg->tA_hi) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&eg->tA_lo) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&eg->tB_hi) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&eg->tB_lo) : "memory");
+    sg = g;
+    stile = (int)blockIdx.x - tb[g];
+    stm = tab[g].tiles_m;
+    sep = tab[g].ep;
+    sep.Nv = nv[g];
+    sga = tab[g].ga;
+  }
+  __syncthreads();
+  const GroupEntry *e = tab + sg;
+  const int t = stile, tm = stm;
+  tc_gemm_tile<GBN, GSTAGES, true, false>(&e->tA_hi, &e->tA_lo, &e->tB_hi, &e->tB_lo, &e->tA_hi, &e->tA_hi,
+                                          &e->tA_hi, sga, sep, (t % tm) * BM, (t / tm) * GBN, 0, t, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -1904,6 +1964,24 @@ static int run_gemm2(ngw_session *s, int nb, const float *x, const float *b2, co
                      ga, ep, s->d_status, s->stream);
 }
 
+// Clenshaw start of p(C) v on stream st: xo = U^T v (deflated eigenpairs),
+// v_perp = v - U xo, b_n = g_n v_perp and the split operand of the first GEMM1.
+static int mixed_poly_start(ngw_session *s, int nb, const double *v, int ldv, double gn, int tda,
+                            cudaStream_t st) {
+  MixedOperator *op = s->mixed;
+  const int ncv = s->ncv, k = op->kdef;
+  if (k > 0)   // xo = U^T v (FP64); v_perp and the U p(Lambda) xo term are fused below
+    NGW_CUDA(dgemm(st, true, false, k, nb, ncv, 1.0, s->eig_U, ncv, v, ldv, 0.0, op->xo, k,
+                   reinterpret_cast<double *>(op->ws), op->ws_bytes));
+  int bx = (ncv + 255) / 256;
+  if (bx > 16) bx = 16;
+  k_cheb_start<<<dim3(bx, ygrid(nb)), 256, 0, st>>>(v, ldv, s->eig_U, op->xo, k, s->d_sqrtR, ncv, nb, gn, tda,
+                                                    op->vperp, op->bb[0], op->cv_pad, op->S_hi, op->S_lo,
+                                                    op->cv_pad);
+  NGW_CUDA(cudaGetLastError());
+  return NGW_OK;
+}
+
 // out64 (ncv x nb, ld ldv) = p(C) v with p given by Chebyshev coefficients
 // g[0..n] on [c0 - c1, c0 + c1] for the deflated part and U p(Lambda) U^T v
 // for the deflated eigenpairs.  Launch-only (no host synchronisation).
@@ -1918,20 +1996,7 @@ int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const dou
     set_error("polynomial degree must be >= 1");
     return NGW_ERR_ARG;
   }
-  cudaStream_t st = s->stream;
-  const int ncv = s->ncv, k = op->kdef;
-  const double one = 1.0, zero = 0.0;
-  if (k > 0)   // xo = U^T v (FP64); v_perp and the U p(Lambda) xo term are fused below
-    NGW_CUDA(dgemm(st, true, false, k, nb, ncv, one, s->eig_U, ncv, v, ldv, zero, op->xo, k,
-                   reinterpret_cast<double *>(op->ws), op->ws_bytes));
-  {
-    int bx = (ncv + 255) / 256;
-    if (bx > 16) bx = 16;
-    k_cheb_start<<<dim3(bx, ygrid(nb)), 256, 0, st>>>(v, ldv, s->eig_U, op->xo, k, s->d_sqrtR, ncv, nb, g[n],
-                                              tda, op->vperp, op->bb[0], op->cv_pad, op->S_hi,
-                                              op->S_lo, op->cv_pad);
-    NGW_CUDA(cudaGetLastError());
-  }
+  NGW_TRY(mixed_poly_start(s, nb, v, ldv, g[n], tda, s->stream));
   const float *vin = op->vperp;
   int cur = 0, prev = -1;   // slots of b_{k+1}, b_{k+2}
   for (int kk = n - 1; kk >= 1; --kk) {
@@ -1947,6 +2012,157 @@ int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const dou
   // final step: p(C) v = g_0 v_perp + Chat b_1 - b_2 + U p(Lambda) xo
   NGW_TRY(run_gemm2(s, nb, op->bb[cur], prev < 0 ? nullptr : op->bb[prev], vin, ldv, g[0],
                     1.0 / c1, c0, 1.0, tda, nullptr, out64, false, true));
+  return NGW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// p(C) v for several molecules with the GEMMs grouped: per Clenshaw term one
+// grouped GEMM1 and one grouped GEMM2 over every molecule still running
+// (k_tc_gemm_grouped), the Clenshaw start per molecule.  The tables are
+// built once per batch (group_build) and read by the kernels at execution
+// time, so a captured graph replays them.
+size_t group_bytes(int G, int n, int steps) {
+  return (size_t)(1 + 2 * n) * G * sizeof(GroupEntry) + (size_t)steps * (3 * G + 2) * sizeof(int) + 256;
+}
+
+// Fill the tables into buf (device, group_bytes() long).  The members' chain
+// buffers must be prepared for their chain counts.
+int group_build(std::vector<GroupMember> &mem, int n, int tda, int steps, void *buf, cudaStream_t st,
+                GroupPlan &P) {
+  const int G = (int)mem.size();
+  P.G = G;
+  P.n = n;
+  P.tda = tda;
+  P.steps = steps;
+  std::vector<GroupEntry> tab((size_t)(1 + 2 * n) * G);
+  for (int i = 0; i < G; ++i) {
+    ngw_session *s = mem[i].s;
+    MixedOperator *op = s->mixed;
+    if (!op || op->nb_cap < mem[i].nb) {
+      set_error("grouped Sigma_c: chain buffers of member %d not prepared", i);
+      return NGW_ERR_STATE;
+    }
+    // GEMM1: [T; q] = A1 S, split output, no split-K
+    GroupEntry &e1 = tab[i];
+    std::memset(&e1, 0, sizeof(e1));
+    e1.tA_hi = op->tA1hi;
+    e1.tA_lo = op->tA1lo;
+    NGW_TRY(make_tmap(&e1.tB_hi, op->S_hi, op->nb_pad, op->cv_pad, GBN));
+    NGW_TRY(make_tmap(&e1.tB_lo, op->S_lo, op->nb_pad, op->cv_pad, GBN));
+    e1.ga.num_kb = op->cv_pad / BK;
+    e1.ga.nseg = 3;
+    e1.ga.nsplit = 1;
+    e1.ep.kind = EPI_SPLIT;
+    e1.ep.Mv = op->n_isdf + op->kdef;
+    e1.ep.out_hi = op->T_hi;
+    e1.ep.out_lo = op->T_lo;
+    e1.ep.ldo = op->mu_k;
+    e1.tiles_m = op->mu_pad / BM;
+    // GEMM2 terms, the Clenshaw rotation of mixed_poly_apply
+    CUtensorMap thi, tlo;
+    NGW_TRY(make_tmap(&thi, op->T_hi, op->nb_pad, op->mu_k, GBN));
+    NGW_TRY(make_tmap(&tlo, op->T_lo, op->nb_pad, op->mu_k, GBN));
+    for (int set = 0; set < 2; ++set) {
+      int cur = 0, prev = -1;
+      for (int t = 0; t < n; ++t) {
+        GroupEntry &e = tab[(size_t)G + ((size_t)set * n + t) * G + i];
+        std::memset(&e, 0, sizeof(e));
+        e.tA_hi = op->tA3hi;
+        e.tA_lo = op->tA3lo;
+        e.tB_hi = thi;
+        e.tB_lo = tlo;
+        e.ga.num_kb = op->mu_k / BK;
+        e.ga.nseg = 3;
+        e.ga.nsplit = 1;
+        e.tiles_m = op->cv_pad / BM;
+        EpiParams &ep = e.ep;
+        ep.kind = EPI_CLENSHAW;
+        ep.Mv = op->ncv;
+        ep.s = s->d_sqrtR;
+        ep.x = op->bb[cur];
+        ep.b2 = prev < 0 ? nullptr : op->bb[prev];
+        ep.v = op->vperp;
+        ep.ldx = op->cv_pad;
+        ep.ldv = mem[i].ldv;
+        ep.c0 = mem[i].c0;
+        ep.beta = 1.0;
+        ep.tda = tda;
+        ep.lds = op->cv_pad;
+        ep.ring = 0;
+        if (t < n - 1) {
+          const int kk = n - 1 - t;
+          const int outb = (prev < 0) ? 1 : 3 - cur - prev;
+          ep.gamma = mem[i].g[kk];
+          ep.alpha = 2.0 / mem[i].c1;
+          ep.out32 = op->bb[outb];
+          ep.s_hi = op->S_hi;
+          ep.s_lo = op->S_lo;
+          prev = cur;
+          cur = outb;
+        } else {
+          ep.gamma = mem[i].g[0];
+          ep.alpha = 1.0 / mem[i].c1;
+          ep.out64 = set == 0 ? mem[i].out_first : mem[i].out_later;
+          if (op->kdef > 0) {
+            ep.Up = op->Up;
+            ep.xo = op->xo;
+            ep.kdef = op->kdef;
+          }
+        }
+      }
+    }
+  }
+  // per-step chain counts and tile ranges
+  std::vector<int> hs((size_t)steps * (3 * G + 2));
+  P.tiles1.assign(steps, 0);
+  P.tiles2.assign(steps, 0);
+  P.nv.assign((size_t)steps * G, 0);
+  for (int k = 0; k < steps; ++k) {
+    int *nvk = hs.data() + (size_t)k * (3 * G + 2), *tb1 = nvk + G, *tb2 = tb1 + G + 1;
+    tb1[0] = tb2[0] = 0;
+    for (int i = 0; i < G; ++i) {
+      const int nk = (k == 0 || !mem[i].nact) ? mem[i].nb : mem[i].nact[k];
+      nvk[i] = nk;
+      P.nv[(size_t)k * G + i] = nk;
+      const int tn = (nk + GBN - 1) / GBN;
+      tb1[i + 1] = tb1[i] + tab[i].tiles_m * tn;
+      tb2[i + 1] = tb2[i] + tab[(size_t)G + i].tiles_m * tn;
+    }
+    P.tiles1[k] = tb1[G];
+    P.tiles2[k] = tb2[G];
+  }
+  char *b = static_cast<char *>(buf);
+  b = reinterpret_cast<char *>(((uintptr_t)b + 127) & ~(uintptr_t)127);
+  P.d_tab = reinterpret_cast<GroupEntry *>(b);
+  P.d_steps = reinterpret_cast<int *>(b + tab.size() * sizeof(GroupEntry));
+  NGW_CUDA(cudaMemcpyAsync(P.d_tab, tab.data(), tab.size() * sizeof(GroupEntry), cudaMemcpyHostToDevice, st));
+  NGW_CUDA(cudaMemcpyAsync(P.d_steps, hs.data(), hs.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  NGW_CUDA(cudaStreamSynchronize(st));
+  return NGW_OK;
+}
+
+// p(C) v of every member at Lanczos step k (vin[i]: its v, ld mem[i].ldv),
+// all on stream st.  Launch-only.
+int group_poly_apply(const GroupPlan &P, std::vector<GroupMember> &mem, int k, const double *const *vin,
+                     cudaStream_t st) {
+  const int G = P.G, n = P.n;
+  const int *nvk = P.d_steps + (size_t)k * (3 * G + 2), *tb1 = nvk + G, *tb2 = tb1 + G + 1;
+  for (int i = 0; i < G; ++i) {
+    const int nk = P.nv[(size_t)k * G + i];
+    if (nk > 0) NGW_TRY(mixed_poly_start(mem[i].s, nk, vin[i], mem[i].ldv, mem[i].g[n], P.tda, st));
+  }
+  if (P.tiles1[k] == 0) return NGW_OK;
+  constexpr size_t smem = (size_t)GSTAGES * (BM * BK * 2 + GBN * BK * 2) * 2 + 1024;
+  static std::atomic<unsigned long long> attr{0};
+  NGW_CUDA(smem_limit_once(k_tc_gemm_grouped, (int)smem, attr));
+  int *status = mem[0].s->d_status;
+  const int set = k == 0 ? 0 : 1;
+  for (int t = 0; t < n; ++t) {
+    NGW_CUDA(launch_pdl(k_tc_gemm_grouped, dim3(P.tiles1[k]), dim3(NTHREADS), smem, st,
+                        (const GroupEntry *)P.d_tab, tb1, nvk, G, status));
+    NGW_CUDA(launch_pdl(k_tc_gemm_grouped, dim3(P.tiles2[k]), dim3(NTHREADS), smem, st,
+                        (const GroupEntry *)(P.d_tab + G + ((size_t)set * n + t) * G), tb2, nvk, G, status));
+  }
   return NGW_OK;
 }
 

@@ -146,6 +146,31 @@ void bump_generation(ngw_session *s);
 // session's cuSOLVER dense handle on the session stream (created on first use)
 int session_cusolver(ngw_session *s, void **handle);
 
+// ---- grouped mixed-precision p(C) v across molecules (gemm_tc.cu) ----
+struct GroupEntry;           // one problem of a grouped tcgen05 GEMM launch (device table)
+struct GroupMember {         // one molecule of the group
+  ngw_session *s;
+  const double *g;           // Chebyshev coefficients g[0..n]
+  double c0, c1;             // the Chebyshev interval [c0 - c1, c0 + c1]
+  int ldv;                   // leading dimension of v / out64 (ncv)
+  double *out_first;         // out64 of the step-0 product
+  double *out_later;         // out64 of the later products
+  int nb;                    // chains at step 0
+  const int *nact;           // chains still running at step k (nullptr: nb every step)
+};
+struct GroupPlan {           // device tables of a group (built by group_build)
+  int G = 0, n = 0, tda = 0, steps = 0;
+  GroupEntry *d_tab = nullptr;
+  int *d_steps = nullptr;
+  std::vector<int> tiles1, tiles2;   // launch sizes per step
+  std::vector<int> nv;               // [steps][G] chains per member
+};
+size_t group_bytes(int G, int n, int steps);
+int group_build(std::vector<GroupMember> &mem, int n, int tda, int steps, void *buf, cudaStream_t st,
+                GroupPlan &P);
+int group_poly_apply(const GroupPlan &P, std::vector<GroupMember> &mem, int k, const double *const *vin,
+                     cudaStream_t st);
+
 // ---- FP64 GEMM on the FP64 tensor cores (dgemm.cu) ----
 // C = alpha op(A) op(B) + beta C, column-major (cuBLAS conventions).  With a
 // workspace (ws, ws_bytes) shapes with a small tile grid split K into slices

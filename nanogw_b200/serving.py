@@ -84,9 +84,19 @@ class SigmaRequest:
 
 class SigmaServer:
     def __init__(self, device=0, workers=2, precision="mixed", hbm_budget_gb=150.0, solver=None,
-                 session_bytes=None):
+                 session_bytes=None, group_work=0.0, group_max=8):
         """`solver(worker, request)` replaces the device solve and
-        `session_bytes(worker)` the device-memory query (host-logic tests)."""
+        `session_bytes(worker)` the device-memory query (host-logic tests).
+
+        group_work > 0 (mixed precision): a waiting request whose matvec work
+        (``SigmaRequest.work``) is at most group_work is admitted together with
+        up to group_max - 1 other such waiting requests, one free worker each,
+        and the group runs as one grouped batch (``sigma_lanczos_batch``: one
+        GEMM launch per Clenshaw term across the group's molecules).  Small
+        molecules' GEMMs are a few tiles each; grouped they fill the GPU."""
+        self.group_work = float(group_work) if precision == "mixed" else 0.0
+        self.group_max = max(1, int(group_max))
+        self.groups = 0                           # groups of two or more requests run
         self.device = device
         self.precision = precision
         self.budget = int(hbm_budget_gb * (1 << 30))
@@ -140,6 +150,27 @@ class SigmaServer:
         req.sigma = sig
         req.eqp = eqp
 
+    def _solve_group(self, ws, reqs):
+        if self.solver:
+            for w, r in zip(ws, reqs):
+                self._solve(w, r)
+            return
+        from .api import lowcomsym_pairs, sigma_lanczos_batch, sqrt_r
+        for w, r in zip(ws, reqs):
+            s = self.sessions[w]
+            if self.resident[w] != r.mol_id:
+                s.set_isdf(r.psi_intp, r.mmtrx)
+                cv = lowcomsym_pairs(r.nval, r.nmem)
+                s.set_pairs(cv, sqrt_r(r.e1, cv))
+                self.resident[w] = r.mol_id
+        sigs = sigma_lanczos_batch([self.sessions[w] for w in ws],
+                                   [dict(e1=r.e1, nval=r.nval, qp_bands=r.qp_bands, nen=r.nen, deltae=r.deltae,
+                                         ecuts=r.ecuts, niter=r.niter, polynomial=r.polynomial) for r in reqs])
+        for w, r, sig in zip(ws, reqs, sigs):
+            e1 = r.e1[r.qp_bands - 1] * RYD
+            r.eqp = self.sessions[w].qp_newton(sig * RYD, e1, e1, r.deltae * RYD, r.sigx_ev, r.vxc_ev)[0]
+            r.sigma = sig
+
     def run(self, requests, realtime=True, policy="fifo"):
         """Serve `requests` (arrival times in seconds from the start).  With
         realtime=False every request is available at t=0 (closed loop).
@@ -182,6 +213,16 @@ class SigmaServer:
                 errors.append((req.rid, repr(e)))
             worker_done(w, req)
 
+        def work_group(ws, rs):
+            try:
+                self._solve_group(ws, rs)
+            except Exception as e:
+                for r in rs:
+                    r.error = e
+                    errors.append((r.rid, repr(e)))
+            for w, r in zip(ws, rs):
+                worker_done(w, r)
+
         threads = []
         i = 0
         with lock:
@@ -215,11 +256,37 @@ class SigmaServer:
                         break                    # wait for memory held by running requests
                     heapq.heappop(pending)
                     free.remove(w)
+                    group_w, group_r = [w], [req]
+                    if self.group_work > 0 and req.work() <= self.group_work:
+                        # other small waiting requests join, one free worker each
+                        aside = []
+                        while pending and free and len(group_r) < self.group_max:
+                            item = heapq.heappop(pending)
+                            r2 = item[2]
+                            if r2.work() > self.group_work or r2.footprint_bytes() > self.budget:
+                                aside.append(item)
+                                continue
+                            w2 = next((x for x in free if self.resident[x] == r2.mol_id), free[0])
+                            reserved[w2] = r2.footprint_bytes()
+                            if used() > self.budget:
+                                reserved[w2] = 0
+                                aside.append(item)
+                                break
+                            free.remove(w2)
+                            group_w.append(w2)
+                            group_r.append(r2)
+                        for item in aside:
+                            heapq.heappush(pending, item)
                     self.peak_used = max(self.peak_used, used())
-                    inflight[req.rid] = req
-                    req.start = time.perf_counter() - t0
-                    req.worker = w
-                    th = threading.Thread(target=work, args=(w, req), daemon=True)
+                    for w2, r2 in zip(group_w, group_r):
+                        inflight[r2.rid] = r2
+                        r2.start = time.perf_counter() - t0
+                        r2.worker = w2
+                    if len(group_r) > 1:
+                        self.groups += 1
+                        th = threading.Thread(target=work_group, args=(group_w, group_r), daemon=True)
+                    else:
+                        th = threading.Thread(target=work, args=(w, req), daemon=True)
                     threads.append(th)
                     th.start()
                     admitted = True

@@ -1,7 +1,19 @@
-"""Batched Sigma_c across molecules of uneven size (ngw_sigma_lanczos_batch):
-one graph whose branches are the molecules' solves.  Each entry is
-bit-identical to the same session's single call, through the eager first
-call, the capture and the replays; per-chain lengths ride along."""
+"""Batched Sigma_c across molecules of uneven size (ngw_sigma_lanczos_batch).
+
+* Branch mode (NGW_BATCH_MODE=branches, and every FP64 batch): one graph
+  whose branches are the molecules' solves; each entry bit-identical to the
+  same session's single call, through the eager first call, the capture and
+  the replays.
+* Grouped mode (the default for mixed precision): the molecules' recurrences
+  in lock step, each Clenshaw term one grouped GEMM1 and one grouped GEMM2
+  launch over all of them.  With the single calls pinned to the grouped
+  tiles (64-wide, fused stages, no split-K) the results are bit-identical;
+  with the single calls on their own tuned tiles they agree to the mixed
+  form's rounding (QP energies within 1 meV).
+Per-chain lengths ride along (entry 1), so the grouped launches shrink as
+that molecule's chains finish."""
+import os
+
 import numpy as np
 import pytest
 
@@ -27,8 +39,21 @@ def molecules():
             _molecule(33, 5, 5.5, 10, 30, 110)]
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_batch_equals_single_calls(molecules, precision):
+@pytest.fixture()
+def env():
+    saved = dict(os.environ)
+    yield os.environ
+    os.environ.clear()
+    os.environ.update(saved)
+
+
+@pytest.mark.parametrize("precision,mode", [("fp64", "branches"), ("mixed", "branches"),
+                                            ("mixed", "grouped_pinned")])
+def test_batch_equals_single_calls(molecules, precision, mode, env):
+    if mode == "branches":
+        env["NGW_BATCH_MODE"] = "branches"
+    else:
+        env["NGW_TILES"] = "64,3,1,64,3"      # the grouped launches' tiles for the single calls
     sessions = []
     reqs = []
     try:
@@ -65,3 +90,34 @@ def test_batch_rejects_repeated_session(molecules):
         with pytest.raises(ngw.NGWError) as e:
             ngw.sigma_lanczos_batch([s, s], [req, req])
         assert e.value.code == ngw._lib.NGW_ERR_ARG
+
+
+def test_grouped_batch_matches_tuned_single_calls(molecules):
+    """Default grouped batch against single calls on their own tuned tiles:
+    the same polynomial, deflation and FP64 recurrence, only the BF16 tile
+    arithmetic differs -> QP energies within 1 meV."""
+    RYD = 13.60569193
+    sessions, reqs = [], []
+    try:
+        for op, poly in molecules:
+            s = ngw.Session(0, "mixed")
+            s.set_isdf(op.psi_intp, op.mmtrx)
+            cv, sr = op.pairs()
+            s.set_pairs(cv, sr)
+            qp = pipeline.qp_bands_near_gap(op.nval, 4)
+            reqs.append(dict(e1=op.e1, nval=op.nval, qp_bands=qp, nen=101, deltae=3.0, ecuts=0.02, niter=40,
+                             polynomial=poly))
+            sessions.append(s)
+        single = [s.calculate_sigma_lanczos(**r) for s, r in zip(sessions, reqs)]
+        for _ in range(3):
+            got = ngw.sigma_lanczos_batch(sessions, reqs)
+        for s, r, g, a in zip(sessions, reqs, got, single):
+            e1 = r["e1"][r["qp_bands"] - 1] * RYD
+            eg = s.qp_newton(g * RYD, e1, e1, r["deltae"] * RYD, -5.0, -4.0, 1e-7)[0]
+            ea = s.qp_newton(a * RYD, e1, e1, r["deltae"] * RYD, -5.0, -4.0, 1e-7)[0]
+            err = np.abs(eg - ea) * 1e3
+            print("grouped vs single QP (meV):", err)
+            assert np.all(err < 1.0)
+    finally:
+        for s in sessions:
+            s.close()

@@ -71,3 +71,26 @@ def test_footprint_bounds_session_bytes(requests, precision):
         assert srv.held[0] == measured > 0
         assert rr.footprint_bytes() >= measured, (r.rid, rr.footprint_bytes(), measured)
         srv.close()
+
+
+def test_grouped_small_requests_within_1mev(requests):
+    """Small requests admitted together run as one grouped batch (one GEMM
+    launch per Clenshaw term across their molecules, 64-wide tiles); each
+    QP energy within 1 meV of the same request served alone on its tuned
+    tiles."""
+    alone = {}
+    for r in requests:
+        srv = SigmaServer(workers=1, precision="mixed")
+        rr = _clone(r)
+        srv.run([rr], realtime=False)
+        srv.close()
+        alone[r.mol_id] = rr.eqp
+    mix = [_clone(r) for r in requests]
+    srv = SigmaServer(workers=3, precision="mixed", group_work=1e30)
+    st = srv.run(mix, realtime=False)
+    groups = srv.groups
+    srv.close()
+    assert st["requests"] == 3 and groups == 1
+    for r in mix:
+        err = np.abs(r.eqp - alone[r.mol_id]) * 1e3
+        assert np.all(err < 1.0), (r.rid, err)

@@ -116,3 +116,24 @@ def test_largest_first_policy_orders_admission():
     order.clear()
     srv.run([_req(0, 1, 0.0, n=32), _req(1, 2, 0.0, n=128), _req(2, 3, 0.0, n=64)], realtime=False)
     assert order == [0, 1, 2]
+
+
+def test_small_requests_grouped():
+    """With group_work set, small waiting requests are admitted together
+    (one free worker each) and run as one group; large ones alone."""
+    seen = []
+
+    def solver(w, req):
+        seen.append((req.rid, w))
+        time.sleep(0.01)
+
+    reqs = [_req(0, 1, 0.0, n=32), _req(1, 2, 0.0, n=32), _req(2, 3, 0.0, n=256), _req(3, 4, 0.0, n=32)]
+    small = reqs[0].work()
+    srv = SigmaServer(workers=4, solver=solver, group_work=2.0 * small, group_max=8)
+    srv.precision = "mixed"
+    st = srv.run(reqs, realtime=False)
+    assert st["requests"] == 4
+    assert srv.groups == 1
+    assert len({w for _, w in seen}) == 4          # every request on its own worker
+    grouped = [r for r in reqs if r.rid in (0, 1, 3)]
+    assert len({round(r.start, 3) for r in grouped}) == 1   # admitted together
