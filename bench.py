@@ -157,7 +157,7 @@ def random_operator(n_isdf, nocc, nemp, seed):
     return psi, m, e1
 
 
-def batched_workload(local, nmol, nqp, seed=2024, fp64_max_nocc=80):
+def batched_workload(local, nmol, nqp, seed=2024, fp64_max_nocc=80, nocc_range=(20, 140)):
     """Uneven molecules in one batch (the batched configuration): 8 synthetic
     molecules built as the 12-atom one with 6-40 atoms, n_occ growing with
     the atom count from 20 to 140, n_empty = 3-4 n_occ, grid radius 8-14 bohr
@@ -178,7 +178,7 @@ def batched_workload(local, nmol, nqp, seed=2024, fp64_max_nocc=80):
     for i in range(nmol):
         n_atoms = int(rng.integers(6, 41))
         frac = (n_atoms - 6) / 34.0
-        nocc = int(round(20 + 120 * frac))
+        nocc = int(round(nocc_range[0] + (nocc_range[1] - nocc_range[0]) * frac))
         nemp = int(round(nocc * rng.uniform(3.0, 4.0)))
         arad = float(4.0 * (n_atoms / 12.0) ** (1.0 / 3.0))
         mol = synth.make_molecule(n_atoms, arad, 8.0 + 6.0 * frac, 0.3, nocc, nemp, seed + 1 + i)
@@ -207,11 +207,20 @@ def batched_workload(local, nmol, nqp, seed=2024, fp64_max_nocc=80):
     t = time.perf_counter()
     seq_sig = [s.calculate_sigma_lanczos(**r) for s, r in zip(sessions, reqs)]
     seq = time.perf_counter() - t
-    for _ in range(2):                        # eager + capture of the batch graph
-        ngw.sigma_lanczos_batch(sessions, reqs)
-    t = time.perf_counter()
-    bat_sig = ngw.sigma_lanczos_batch(sessions, reqs)
-    bat = time.perf_counter() - t
+    def timed_batch(mode):
+        if mode:
+            os.environ["NGW_BATCH_MODE"] = mode
+        try:
+            for _ in range(2):                    # eager + capture of the batch graph
+                ngw.sigma_lanczos_batch(sessions, reqs)
+            t0 = time.perf_counter()
+            sig = ngw.sigma_lanczos_batch(sessions, reqs)
+            return sig, time.perf_counter() - t0
+        finally:
+            os.environ.pop("NGW_BATCH_MODE", None)
+    bat_sig, bat = timed_batch(None)               # small molecules grouped, the rest as branches
+    _, bat_branches = timed_batch("branches")
+    _, bat_grouped_all = timed_batch("grouped")
     # the grouped batch runs its own 64-wide tiles: compare QP energies with
     # the sequential solves on their tuned tiles (Sigma_x - V_xc = -2 eV)
     bat_vs_seq = []
@@ -239,7 +248,11 @@ def batched_workload(local, nmol, nqp, seed=2024, fp64_max_nocc=80):
             "values": "seeded synthetic molecules (device CVT, ISDF fit and Coulomb kernel)",
             "setup_s": setup_s, "solves": solves, "batched_solves_per_s": solves / bat,
             "sequential_solves_per_s": solves / seq, "batched_s": bat, "sequential_s": seq,
-            "batch_mode": "grouped launches (one GEMM1 and one GEMM2 launch per Clenshaw term across molecules)",
+            "branches_only_solves_per_s": solves / bat_branches,
+            "grouped_all_solves_per_s": solves / bat_grouped_all,
+            "batch_mode": "default: molecules with N_cv <= 8192 and N_mu <= 512 grouped (one GEMM1 and one GEMM2 "
+                          "launch per Clenshaw term across them), larger ones as graph branches on their tuned "
+                          "tiles; branches_only / grouped_all: every molecule one way",
             "qp_diff_mev_batched_vs_sequential": bat_vs_seq,
             "qp_err_mev_vs_fp64": {"rule": f"molecules with n_occ <= {fp64_max_nocc}", "per_molecule": errs},
             "molecules": dims}
@@ -271,7 +284,7 @@ def serving_molecule(sess, rid, rng, nocc_range, seed):
 
 
 def serving_workload(local, nreq, workers, seed=77, nocc_range=(8, 160), load=0.8, fp64_max_nocc=64,
-                     group_nocc=0):
+                     group_nocc=0, fp64_rule="small"):
     """A stream of Sigma_c requests of the serving configuration, each its own
     synthetic molecule (``serving_molecule``; operators built before the
     stream starts).  Closed loop (all requests queued at t = 0) in mixed
@@ -304,7 +317,12 @@ def serving_workload(local, nreq, workers, seed=77, nocc_range=(8, 160), load=0.
                              arrival=0.0 if arrivals is None else float(arrivals[i]))
                 for i, b in enumerate(reqs)]
 
-    sub = [b for b in base if b.nval <= fp64_max_nocc]
+    if fp64_rule == "even":       # every other request: an unbiased half of the stream
+        sub = [b for b in base if b.rid % 2 == 0]
+        rule = "every other request (even request ids)"
+    else:
+        sub = [b for b in base if b.nval <= fp64_max_nocc]
+        rule = f"requests with n_occ <= {fp64_max_nocc}"
     # mixed arm: requests up to the work of an n_occ = group_nocc request
     # (16 QP states, 300 steps) are grouped when several wait together
     group_work = 0.0
@@ -341,7 +359,7 @@ def serving_workload(local, nreq, workers, seed=77, nocc_range=(8, 160), load=0.
             failed += int(np.sum(~ok))
             err = float(np.max(np.abs(ea - eb)[ok]) * 1e3) if ok.any() else None
             errs.append(err)
-            if err is not None and err > 1.0:
+            if err is not None and err > 1.0 and b.nval <= 64:
                 cv = ngw.lowcomsym_pairs(b.nval, b.nmem)
                 with ngw.Session(local, "fp64") as f:
                     f.set_isdf(b.psi_intp, b.mmtrx * (1.0 + 2.0 ** -46))
@@ -353,9 +371,10 @@ def serving_workload(local, nreq, workers, seed=77, nocc_range=(8, 160), load=0.
     # each subset request alone on one worker (operator resident, shapes
     # tuned), both forms: where the time goes by molecule size
     alone = []
+    small_sub = [b for b in sub if b.nval <= 64]
     for prec in ("mixed", "fp64"):
         srv1 = SigmaServer(device=local, workers=1, precision=prec)
-        for r in make(sub):
+        for r in make(small_sub):
             srv1.run([r], realtime=False)             # upload, tuning, eager run
             for _ in range(2):                        # capture, then graph replay (timed)
                 r2 = SigmaRequest(rid=r.rid, mol_id=r.mol_id, psi_intp=r.psi_intp, mmtrx=r.mmtrx, e1=r.e1,
@@ -369,7 +388,7 @@ def serving_workload(local, nreq, workers, seed=77, nocc_range=(8, 160), load=0.
         t_alone.setdefault(rid, {})[prec] = w
     per_req = [{"rid": b.rid, "n_occ": b.nval, "qp_states": int(len(b.qp_bands)), "niter": b.niter,
                 "mixed_ms": round(1e3 * t_alone[b.rid]["mixed"], 2), "fp64_ms": round(1e3 * t_alone[b.rid]["fp64"], 2),
-                "ratio": round(t_alone[b.rid]["fp64"] / t_alone[b.rid]["mixed"], 2)} for b in sub]
+                "ratio": round(t_alone[b.rid]["fp64"] / t_alone[b.rid]["mixed"], 2)} for b in small_sub]
     nocc = [b.nval for b in base]
     out = {"workload": f"{nreq} requests, each a synthetic molecule: n_occ log-uniform {nocc_range[0]}-"
                        f"{nocc_range[1]}, n_empty = 4 n_occ, n_isdf = 8 n_occ, grid radius 7-15 bohr at "
@@ -387,7 +406,7 @@ def serving_workload(local, nreq, workers, seed=77, nocc_range=(8, 160), load=0.
            "first_pass_solves_per_s": first["solves_per_s"],
            "first_pass_note": "the same requests before any of their shapes was tuned "
                               "(includes autotuning, nearest-shape reuse and first-call setup)",
-           "fp64_subset": {"rule": f"requests with n_occ <= {fp64_max_nocc}", "requests": len(sub),
+           "fp64_subset": {"rule": rule, "requests": len(sub),
                            "solves": f64_sub["solves"],
                            "fp64_solves_per_s": f64_sub["solves_per_s"],
                            "mixed_solves_per_s": mixed_sub["solves_per_s"],
@@ -648,9 +667,12 @@ def main():
     ap.add_argument("--workload", default="12atom", choices=["12atom", "batched", "serving", "large"],
                     help="batched: uneven molecules in one graph launch; serving: request stream")
     ap.add_argument("--batched-qp", type=int, default=2)
+    ap.add_argument("--batched-nocc", default="20,140", help="n_occ range of the batched molecules")
     ap.add_argument("--serving-requests", type=int, default=32)
     ap.add_argument("--serving-fp64-max-nocc", type=int, default=64)
     ap.add_argument("--serving-workers", type=int, default=4)
+    ap.add_argument("--serving-fp64-rule", default="small", choices=["small", "even"],
+                    help="FP64 arm on the requests with n_occ <= --serving-fp64-max-nocc, or on every other one")
     ap.add_argument("--serving-group-nocc", type=int, default=0,
                     help="group waiting requests up to this molecule size into grouped batches (mixed arm)")
     args = ap.parse_args()
@@ -681,13 +703,15 @@ def main():
     if args.workload != "12atom":
         if rank == 0:
             if args.workload == "batched":
-                res = batched_workload(local, 8, args.batched_qp)
+                lo, hi = (int(x) for x in args.batched_nocc.split(","))
+                res = batched_workload(local, 8, args.batched_qp, nocc_range=(lo, hi))
             elif args.workload == "large":
                 res = large_workload(local)
             else:
                 res = serving_workload(local, args.serving_requests, args.serving_workers,
                                        fp64_max_nocc=args.serving_fp64_max_nocc,
-                                       group_nocc=args.serving_group_nocc)
+                                       group_nocc=args.serving_group_nocc,
+                                       fp64_rule=args.serving_fp64_rule)
             print(json.dumps(res), flush=True)
         if dist:
             dist.destroy_process_group()
@@ -921,15 +945,19 @@ def main():
 
     # our kernels per request: per matvec GEMM1 (+ split-K reduce unless the
     # split is summed inside a cluster: variants 5 / 6) and GEMM2; per Lanczos
-    # step the Clenshaw start and the Lanczos update; per request the start
-    # vectors, norms, init, first step and the Sigma_c spectra / reduction
+    # step the deflation projection U^T v (FP64 GEMM with its K-slice sum),
+    # the Clenshaw start and the Lanczos update; per request the start
+    # vectors (two FP64 GEMMs, one K-slice sum), norms, init, first step and
+    # the Sigma_c spectra / reduction
     per_mv = 2
+    per_step = 2
     if args.precision == "mixed" and roof is not None:
         g1 = roof["shapes"][0]
         per_mv += 1 if (g1[4] > 1 and g1[5] not in (5, 6)) else 0
+        per_step += 2
     elif args.precision != "mixed":
-        per_mv = 2        # FP64: combine kernel + (next matvec's) scaling
-    launches_per_step = wl["niter"] * (wl["npoly"] * per_mv + 2) + 8
+        per_mv = 2        # FP64 (library DGEMMs not counted): combine kernel + (next matvec's) scaling
+    launches_per_step = wl["niter"] * (wl["npoly"] * per_mv + per_step) + 10
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": K,
                 "warmup": W, "ms_per_step": tot_ms / K, "higher_is_better": True, "scaling": "weak",

@@ -156,14 +156,22 @@ int ngw_sigma_lanczos(ngw_session *s, const ngw_sigma_params *p, const double *e
 
 /* Batched Sigma_c of several molecules, one per session (sessions on one
  * device, each with its operator set): entry i solves params[i] with KS
- * energies e1[i] into sigma_c[i], exactly as ngw_sigma_lanczos would (same
- * kernels and tiles, so the results are bit-identical).  The device work of
- * all entries is one CUDA graph -- entry i a branch on session i's stream,
- * forked from and joined into session 0's stream -- captured on the second
- * call with the same shapes and replayed by one launch afterwards, so the
- * chains of small molecules overlap on the GPU.  Each entry's chains must fit
- * one block (block_chains 0 or >= nqp * nbands_sum).  Configuration 2 of the
- * benchmarks (uneven molecules, per-chain lengths) runs through this call. */
+ * energies e1[i] into sigma_c[i].  Mixed precision (all entries, no TDA, one
+ * polynomial degree): the molecules' Lanczos recurrences run in lock step on
+ * session 0's stream and each Clenshaw term of their p(C) v is one grouped
+ * tcgen05 GEMM launch per operand product across all molecules (64-wide
+ * tiles; bit-identical to single calls pinned to those tiles, QP energies
+ * within 1 meV of single calls on their tuned tiles), one grouped
+ * Lanczos-step launch per step.  Otherwise (FP64, TDA, or
+ * NGW_BATCH_MODE=branches) entry i is a branch on session i's stream, forked
+ * from and joined into session 0's stream, with the kernels and tiles of
+ * ngw_sigma_lanczos (bit-identical results).  Either way the batch is one
+ * CUDA graph, captured on the second call with the same shapes and replayed
+ * by one launch afterwards.  Each entry's chains must fit one block
+ * (block_chains 0 or >= nqp * nbands_sum).  The batched configuration of the
+ * benchmarks (uneven molecules, per-chain lengths) runs through this call.
+ * No reference counterpart: NanoGW blocks bands of one molecule only
+ * (SIGMA/calculate_sigma_lanczos_lowcomsym.F90z:477-511). */
 int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_sigma_params *params,
                             const double *const *e1, double *const *sigma_c);
 

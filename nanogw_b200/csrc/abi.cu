@@ -158,7 +158,7 @@ enum {
   SL_IN = 0, SL_OUT, SL_HS, SL_T1, SL_T2, SL_Z, SL_VEC, SL_WVEC, SL_TMP, SL_A, SL_B, SL_ZZ,
   SL_SPEC, SL_CMN, SL_CM, SL_P, SL_P2, SL_PN2, SL_PN, SL_CHB, SL_CHQ, SL_E1, SL_ZZ0, SL_SIG,
   SL_KR, SL_KC, SL_KM, SL_B1, SL_B2, SL_QPW, SL_QPIO, SL_SPECS, SL_CLEN, SL_LEN, SL_SLOT, SL_BASIS,
-  SL_DGWS, SL_GROUP, SL_NUM
+  SL_DGWS, SL_GROUP, SL_LGROUP, SL_NUM
 };
 
 // ---------------------------------------------------------------------------
@@ -683,8 +683,52 @@ static int sigma_region(SigmaJob &J) {
 // one GEMM2 launch per Clenshaw term for all molecules still running), the
 // per-chain updates per molecule.  Same arithmetic per chain as lanczos_dev
 // with the grouped tiles.  Launch-only; everything on stream st.
+// Tables of the grouped Lanczos-step launches (steps >= 1): the members'
+// vector roles follow the swaps of lanczos_grouped.
+struct LanczosGroupTables {
+  std::vector<LanczosGroupEntry> tab;   // [steps][G]
+  std::vector<int> cb;                  // [steps][G + 1] chain begins
+  std::vector<int> tot;                 // chains per launch
+  const LanczosGroupEntry *d_tab = nullptr;
+  const int *d_cb = nullptr;
+};
+
+static void lanczos_group_tables(std::vector<SigmaJob> &jobs, const GroupPlan &P, LanczosGroupTables &T) {
+  const int G = (int)jobs.size(), steps = P.steps;
+  T.tab.assign((size_t)steps * G, LanczosGroupEntry{});
+  T.cb.assign((size_t)steps * (G + 1), 0);
+  T.tot.assign(steps, 0);
+  std::vector<double *> vec(G), wvec(G);
+  for (int i = 0; i < G; ++i) {
+    vec[i] = jobs[i].W;
+    wvec[i] = jobs[i].V;
+  }
+  for (int k = 1; k < steps; ++k) {
+    int *cbk = T.cb.data() + (size_t)k * (G + 1);
+    for (int i = 0; i < G; ++i) {
+      SigmaJob &J = jobs[i];
+      const int nk = std::max(0, P.nv[(size_t)k * G + i]);
+      LanczosGroupEntry &e = T.tab[(size_t)k * G + i];
+      e.w = wvec[i];
+      e.v = vec[i];
+      e.t = J.tmp;
+      e.a = J.a;
+      e.b = J.b;
+      e.s = J.s->d_sqrtR;
+      e.clen = J.clen;
+      e.eps = J.p->early_exit_eps;
+      e.ncv = J.ncv;
+      e.niter = J.niter;
+      e.prescale_next = (k + 1 < J.niter) ? 1 : 0;
+      cbk[i + 1] = cbk[i] + nk;
+      if (nk > 0 && k + 1 < J.niter) std::swap(vec[i], wvec[i]);
+    }
+    T.tot[k] = cbk[G];
+  }
+}
+
 static int lanczos_grouped(std::vector<SigmaJob> &jobs, std::vector<GroupMember> &mem, const GroupPlan &P,
-                           cudaStream_t st) {
+                           cudaStream_t st, const LanczosGroupTables *LT = nullptr) {
   const int G = (int)jobs.size();
   std::vector<double *> vec(G), wvec(G);
   std::vector<const double *> vin(G);
@@ -714,10 +758,16 @@ static int lanczos_grouped(std::vector<SigmaJob> &jobs, std::vector<GroupMember>
     }
     if (!any) break;
     NGW_TRY(group_poly_apply(P, mem, k, vin.data(), st));   // tmp = p(H) vec
+    if (LT)   // every member's step in one launch
+      launch_lanczos_step_grouped(LT->d_tab + (size_t)k * G, LT->d_cb + (size_t)k * (G + 1), G, k, LT->tot[k], st);
     for (int i = 0; i < G; ++i) {
       SigmaJob &J = jobs[i];
       const int nk = P.nv[(size_t)k * G + i];
       if (nk <= 0) continue;
+      if (LT) {
+        if (k + 1 < J.niter) std::swap(vec[i], wvec[i]);
+        continue;
+      }
       ngw_session *s = J.s;
       const double eps = J.p->early_exit_eps;
       if (J.basis)
@@ -1202,77 +1252,99 @@ int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_s
     NGW_TRY(sigma_block_setup(jobs[i], 0));
   }
   ngw_session *s0 = sessions[0];
-  // Grouped mode (default when every entry is mixed precision, not TDA, with
-  // one polynomial degree): the molecules' Lanczos recurrences run in lock
-  // step on session 0's stream and each Clenshaw term of their p(C) v is one
-  // grouped GEMM1 and one grouped GEMM2 launch over all of them.
-  // NGW_BATCH_MODE=branches keeps one graph branch per molecule.
-  bool grouped = count > 1;
-  if (const char *e = getenv("NGW_BATCH_MODE"))
-    if (std::string(e) == "branches") grouped = false;
-  for (int i = 0; i < count && grouped; ++i)
-    if (sessions[i]->precision != NGW_PREC_MIXED || jobs[i].tamm_d || jobs[i].pp.npoly != jobs[0].pp.npoly ||
-        (int)jobs[i].pp.cheb.size() != jobs[0].pp.npoly + 1)
-      grouped = false;
-  if (grouped) {
+  // Small molecules (N_cv <= 8192, N_mu <= 512) in mixed precision, not TDA,
+  // with one polynomial degree run grouped: their Lanczos recurrences in lock
+  // step on one stream, each Clenshaw term of their p(C) v one grouped GEMM1
+  // and one grouped GEMM2 launch over all of them, one grouped step launch
+  // per Lanczos step.  Their GEMMs are a few tiles each; grouped they fill
+  // the GPU.  Larger molecules keep their own tuned tiles as graph branches
+  // running beside the group.  NGW_BATCH_MODE=branches groups nothing,
+  // NGW_BATCH_MODE=grouped groups every eligible entry whatever its size.
+  int mode = 0;   // 0 small only, 1 none, 2 every eligible entry
+  if (const char *e = getenv("NGW_BATCH_MODE")) {
+    if (std::string(e) == "branches") mode = 1;
+    if (std::string(e) == "grouped") mode = 2;
+  }
+  std::vector<int> grp, br;
+  for (int i = 0; i < count; ++i) {
+    const SigmaJob &J = jobs[i];
+    const bool eligible = mode != 1 && sessions[i]->precision == NGW_PREC_MIXED && !J.tamm_d &&
+                          (int)J.pp.cheb.size() == J.pp.npoly + 1 &&
+                          (grp.empty() || J.pp.npoly == jobs[grp[0]].pp.npoly) &&
+                          (mode == 2 || (J.ncv <= 8192 && J.n <= 512));
+    (eligible ? grp : br).push_back(i);
+  }
+  if (grp.size() < 2) {
+    br.insert(br.end(), grp.begin(), grp.end());
+    std::sort(br.begin(), br.end());
+    grp.clear();
+  }
+  const int G = (int)grp.size();
+  std::vector<SigmaJob> gjobs;
+  for (int i : grp) gjobs.push_back(jobs[i]);
+  std::vector<std::vector<int>> nact(G);
+  std::vector<GroupMember> mem(G);
+  GroupPlan P;
+  LanczosGroupTables LT;
+  bool any_reorth = false;
+  ngw_session *sg = G ? sessions[grp[0]] : nullptr;   // the group runs on this session's stream
+  std::vector<unsigned long long> key = {0xBA7C5ull, (unsigned long long)count, (unsigned long long)G};
+  if (G) {
     int steps = 0;
-    for (auto &J : jobs) steps = std::max(steps, J.niter);
-    std::vector<std::vector<int>> nact(count);
-    std::vector<GroupMember> mem(count);
-    for (int i = 0; i < count; ++i) {
-      SigmaJob &J = jobs[i];
+    for (auto &J : gjobs) steps = std::max(steps, J.niter);
+    for (int i = 0; i < G; ++i) {
+      SigmaJob &J = gjobs[i];
       nact[i].assign(steps, 0);
       for (int k = 0; k < J.niter; ++k) nact[i][k] = J.len ? J.nact[k] : J.nb;
       mem[i] = GroupMember{J.s, J.pp.cheb.data(), J.pp.c0, J.pp.c1, J.ncv, J.W, J.tmp, J.nb, nact[i].data()};
     }
-    const int n = jobs[0].pp.npoly;
+    const int n = gjobs[0].pp.npoly;
     void *buf = nullptr;
-    NGW_TRY(scratch(s0, SL_GROUP, group_bytes(count, n, steps), &buf));
-    GroupPlan P;
-    NGW_TRY(group_build(mem, n, 0, steps, buf, s0->stream, P));
-    std::vector<unsigned long long> key = {0x6A0DBull, (unsigned long long)count, (unsigned long long)(uintptr_t)buf};
-    for (int i = 0; i < count; ++i) {
-      key.push_back((unsigned long long)(uintptr_t)sessions[i]);
-      sigma_key(jobs[i], key);
+    NGW_TRY(scratch(sg, SL_GROUP, group_bytes(G, n, steps), &buf));
+    NGW_TRY(group_build(mem, n, 0, steps, buf, sg->stream, P));
+    // one Lanczos-step launch per step for all members (none reorthogonalises)
+    for (auto &J : gjobs) any_reorth = any_reorth || J.basis != nullptr;
+    if (!any_reorth) {
+      lanczos_group_tables(gjobs, P, LT);
+      const size_t tb = LT.tab.size() * sizeof(LanczosGroupEntry), cbb = LT.cb.size() * sizeof(int);
+      void *lbuf = nullptr;
+      NGW_TRY(scratch(sg, SL_LGROUP, tb + cbb + 256, &lbuf));
+      LT.d_tab = static_cast<const LanczosGroupEntry *>(lbuf);
+      LT.d_cb = reinterpret_cast<const int *>(static_cast<char *>(lbuf) + tb);
+      NGW_CUDA(cudaMemcpyAsync(lbuf, LT.tab.data(), tb, cudaMemcpyHostToDevice, sg->stream));
+      NGW_CUDA(cudaMemcpyAsync(static_cast<char *>(lbuf) + tb, LT.cb.data(), cbb, cudaMemcpyHostToDevice,
+                               sg->stream));
+      NGW_CUDA(cudaStreamSynchronize(sg->stream));
     }
-    std::vector<cudaStream_t> saved(count);
-    for (int i = 0; i < count; ++i) {
-      saved[i] = sessions[i]->stream;
-      sessions[i]->stream = s0->stream;   // every launch of the batch on one stream
-    }
-    auto region = [&]() -> int {
-      for (int i = 0; i < count; ++i) NGW_TRY(sigma_start(jobs[i]));
-      NGW_TRY(lanczos_grouped(jobs, mem, P, s0->stream));
-      for (int i = 0; i < count; ++i) NGW_TRY(sigma_end(jobs[i]));
-      return NGW_OK;
-    };
-    int rc;
-    {
-      std::shared_lock<std::shared_mutex> busy(gpu_quiet_lock(s0->device));   // no tuning meanwhile
-      rc = run_graphed(s0, key, region);
-      if (rc == NGW_OK && cudaStreamSynchronize(s0->stream) != cudaSuccess) {
-        set_error("ngw_sigma_lanczos_batch: %s", cudaGetErrorString(cudaGetLastError()));
-        rc = NGW_ERR_CUDA;
-      }
-    }
-    for (int i = 0; i < count; ++i) sessions[i]->stream = saved[i];
-    NGW_TRY(rc);
-    for (int i = 0; i < count; ++i) NGW_TRY(sigma_finish(jobs[i], sigma_c[i]));
-    return NGW_OK;
+    key.push_back((unsigned long long)(uintptr_t)buf);
+    key.push_back((unsigned long long)(uintptr_t)LT.d_tab);
   }
-  // one graph for the whole batch: entry i is a branch on its session's
-  // stream, forked from and joined back into session 0's stream
-  std::vector<unsigned long long> key = {0xBA7C4ull, (unsigned long long)count};
   for (int i = 0; i < count; ++i) {
     key.push_back((unsigned long long)(uintptr_t)sessions[i]);
     key.push_back((unsigned long long)(uintptr_t)sessions[i]->cublas_ws);
     sigma_key(jobs[i], key);
   }
-  std::vector<cudaEvent_t> ev(count + 1, nullptr);
+  // the group on sg's stream and every other entry on its own stream, all
+  // forked from and joined back into session 0's stream
+  std::vector<cudaEvent_t> ev(count + 2, nullptr);
   for (auto &e : ev) NGW_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  std::vector<cudaStream_t> saved(count);
+  for (int i = 0; i < count; ++i) saved[i] = sessions[i]->stream;
+  cudaStream_t gst = sg ? sg->stream : nullptr;
+  for (int i : grp) sessions[i]->stream = gst;      // every launch of the group on one stream
   auto region = [&]() -> int {
     NGW_CUDA(cudaEventRecord(ev[count], s0->stream));
-    for (int i = 0; i < count; ++i) {
+    if (G) {
+      if (gst != s0->stream) NGW_CUDA(cudaStreamWaitEvent(gst, ev[count], 0));
+      for (auto &J : gjobs) NGW_TRY(sigma_start(J));
+      NGW_TRY(lanczos_grouped(gjobs, mem, P, gst, any_reorth ? nullptr : &LT));
+      for (auto &J : gjobs) NGW_TRY(sigma_end(J));
+      if (gst != s0->stream) {
+        NGW_CUDA(cudaEventRecord(ev[count + 1], gst));
+        NGW_CUDA(cudaStreamWaitEvent(s0->stream, ev[count + 1], 0));
+      }
+    }
+    for (int i : br) {
       ngw_session *si = sessions[i];
       if (si->stream != s0->stream) NGW_CUDA(cudaStreamWaitEvent(si->stream, ev[count], 0));
       NGW_TRY(sigma_region(jobs[i]));
@@ -1283,12 +1355,16 @@ int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_s
     }
     return NGW_OK;
   };
-  std::shared_lock<std::shared_mutex> busy(gpu_quiet_lock(s0->device));   // no tuning meanwhile
-  int rc = run_graphed(s0, key, region);
-  if (rc == NGW_OK && cudaStreamSynchronize(s0->stream) != cudaSuccess) {
-    set_error("ngw_sigma_lanczos_batch: %s", cudaGetErrorString(cudaGetLastError()));
-    rc = NGW_ERR_CUDA;
+  int rc;
+  {
+    std::shared_lock<std::shared_mutex> busy(gpu_quiet_lock(s0->device));   // no tuning meanwhile
+    rc = run_graphed(s0, key, region);
+    if (rc == NGW_OK && cudaStreamSynchronize(s0->stream) != cudaSuccess) {
+      set_error("ngw_sigma_lanczos_batch: %s", cudaGetErrorString(cudaGetLastError()));
+      rc = NGW_ERR_CUDA;
+    }
   }
+  for (int i = 0; i < count; ++i) sessions[i]->stream = saved[i];
   for (auto &e : ev) cudaEventDestroy(e);
   NGW_TRY(rc);
   for (int i = 0; i < count; ++i) NGW_TRY(sigma_finish(jobs[i], sigma_c[i]));

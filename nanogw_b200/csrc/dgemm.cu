@@ -54,13 +54,47 @@ __host__ __device__ constexpr int tile_elems() {
   return (DG_BK * (BMN + DG_PAD) > BMN * DG_KROW) ? DG_BK * (BMN + DG_PAD) : BMN * DG_KROW;
 }
 
+__device__ __forceinline__ void cp_async16(double *smem, const double *gmem, int src_bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  // src_bytes < 16: the rest of the 16 destination bytes is zero-filled
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+
 // Stage the (rows x BK) tile of an operand whose op(X)[r][kk] is X[r + kk*ld]
 // (contiguous along r; TR = false) or X[kk + r*ld] (contiguous along kk;
 // TR = true).  Shared layout: TR = false -> S[kk][r] with row length
-// BMN + PAD; TR = true -> S[r][kk] with row length KROW.
+// BMN + PAD; TR = true -> S[r][kk] with row length KROW.  With vec (X
+// 16-byte aligned, ld even) pairs of elements along the contiguous index
+// move as one 16-byte copy.
 template <int BMN, int NT, bool TR>
-__device__ __forceinline__ void load_tile(double *S, const double *X, int ld, int r0, int rows, int k0, int K) {
+__device__ __forceinline__ void load_tile(double *S, const double *X, int ld, int r0, int rows, int k0, int K,
+                                          bool vec) {
   constexpr int E = BMN * DG_BK;
+  if (vec) {
+    for (int e = 2 * threadIdx.x; e < E; e += 2 * NT) {
+      int r, kk;
+      if (!TR) {
+        r = e % BMN;
+        kk = e / BMN;
+      } else {
+        kk = e % DG_BK;
+        r = e / DG_BK;
+      }
+      const int gr = r0 + r, gk = k0 + kk;
+      int nvalid;   // valid elements of the pair (0, 1, 2)
+      const double *src = X;
+      if (!TR) {
+        nvalid = (gk < K) ? max(0, min(2, rows - gr)) : 0;
+        if (nvalid) src = X + (size_t)gk * ld + gr;
+      } else {
+        nvalid = (gr < rows) ? max(0, min(2, K - gk)) : 0;
+        if (nvalid) src = X + (size_t)gr * ld + gk;
+      }
+      double *dst = TR ? S + r * DG_KROW + kk : S + kk * (BMN + DG_PAD) + r;
+      cp_async16(dst, src, 8 * nvalid);
+    }
+    return;
+  }
   for (int e = threadIdx.x; e < E; e += NT) {
     int r, kk;
     if (!TR) {
@@ -94,6 +128,7 @@ struct DgemmArgs {
   int ldb;
   double *C;
   int ldc;
+  int vecA, vecB;      // 16-byte copies possible (aligned base, even leading dimension)
   int kslices;         // > 1: partial tiles to ws[slice][n][m] (column-major, ld m)
   int kchunk;          // K per slice (multiple of BK)
   double *ws;
@@ -129,8 +164,8 @@ __global__ void __launch_bounds__(WM *WN * 32, 1) k_dgemm(DgemmArgs g) {
   // B operand indexed [col n][kk]: TB = false -> B[kk + n*ldb] (contiguous along kk)
   auto load_stage = [&](int st, int kt) {
     const int k0 = kbeg + kt * DG_BK;
-    load_tile<BM, NT, TA>(sA + st * SA, g.A, g.lda, m0, g.m, k0, kend);
-    load_tile<BN, NT, !TB>(sB + st * SB, g.B, g.ldb, n0, g.n, k0, kend);
+    load_tile<BM, NT, TA>(sA + st * SA, g.A, g.lda, m0, g.m, k0, kend, g.vecA != 0);
+    load_tile<BN, NT, !TB>(sB + st * SB, g.B, g.ldb, n0, g.n, k0, kend, g.vecB != 0);
   };
 #pragma unroll
   for (int st = 0; st < DG_STAGES - 1; ++st) {
@@ -253,6 +288,8 @@ cudaError_t dgemm(cudaStream_t st, bool ta, bool tb, int m, int n, int k, double
   a.ldc = ldc;
   a.kslices = 1;
   a.kchunk = std::max(a.k, 1);
+  a.vecA = ((reinterpret_cast<uintptr_t>(A) & 15) == 0 && (lda & 1) == 0) ? 1 : 0;
+  a.vecB = ((reinterpret_cast<uintptr_t>(B) & 15) == 0 && (ldb & 1) == 0) ? 1 : 0;
   const int nsm = sm_count();
   const long long big_tiles = (long long)((m + 127) / 128) * ((n + 127) / 128);
   if (big_tiles >= 2LL * nsm) return launch_trans<128, 128, 2, 4>(a, ta, tb, st);

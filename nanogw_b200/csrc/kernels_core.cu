@@ -271,13 +271,14 @@ void launch_lanczos_prescale(double *w, double *v, int ncv, int nb, int k, const
 // Step k (0-based, k >= 1):  w = w + t ; a(k) = <w, v> ;
 //   if k+1 < niter: w = w - a(k) v ; b(k+1) = ||w||    (lanczos_spectra_lowcomsym.F90:153-164)
 // and, when prescale_next, the next step's rescale (w /= b(k+1), v = -v b(k+1), hs).
-__global__ void k_lanczos_step(double *__restrict__ w, double *__restrict__ v,
-                               const double *__restrict__ t, int ncv, int k,
-                               double *__restrict__ a, double *__restrict__ b, int niter,
-                               const double *__restrict__ s, double *__restrict__ hs, int tamm_d,
-                               int prescale_next, int *__restrict__ clen, double eps) {
+// One CTA runs chain j.
+__device__ __forceinline__ void lanczos_step_chain(double *__restrict__ w, double *__restrict__ v,
+                                                   const double *__restrict__ t, int ncv, int k,
+                                                   double *__restrict__ a, double *__restrict__ b, int niter,
+                                                   const double *__restrict__ s, double *__restrict__ hs,
+                                                   int tamm_d, int prescale_next, int *__restrict__ clen,
+                                                   double eps, int j) {
   __shared__ double sh[33];
-  const int j = blockIdx.x;
   const int L = clen ? clen[j] : niter;
   if (k >= L) return;                    // finished or stopped chain: vectors left as they are
   double *wj = w + (size_t)j * ncv;
@@ -307,6 +308,36 @@ __global__ void k_lanczos_step(double *__restrict__ w, double *__restrict__ v,
     if (prescale_next && !stop)
       prescale_chain(wj, vj, ncv, bk1, s, hs ? hs + (size_t)j * ncv : nullptr, tamm_d);
   }
+}
+
+__global__ void k_lanczos_step(double *__restrict__ w, double *__restrict__ v,
+                               const double *__restrict__ t, int ncv, int k,
+                               double *__restrict__ a, double *__restrict__ b, int niter,
+                               const double *__restrict__ s, double *__restrict__ hs, int tamm_d,
+                               int prescale_next, int *__restrict__ clen, double eps) {
+  lanczos_step_chain(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next, clen, eps, blockIdx.x);
+}
+
+// The step of several molecules' chains in one launch (mixed precision, no
+// scaled copy): block b runs chain b - cb[g] of entry g, cb[g] <= b < cb[g+1].
+__global__ void __launch_bounds__(LNT)
+    k_lanczos_step_grouped(const LanczosGroupEntry *__restrict__ tab, const int *__restrict__ cb, int G, int k) {
+  __shared__ int sg;
+  if (threadIdx.x == 0) {
+    int g = 0;
+    while (g + 1 < G && (int)blockIdx.x >= cb[g + 1]) ++g;
+    sg = g;
+  }
+  __syncthreads();
+  const LanczosGroupEntry &e = tab[sg];
+  lanczos_step_chain(e.w, e.v, e.t, e.ncv, k, e.a, e.b, e.niter, e.s, nullptr, 0, e.prescale_next, e.clen, e.eps,
+                     (int)blockIdx.x - cb[sg]);
+}
+
+void launch_lanczos_step_grouped(const LanczosGroupEntry *tab, const int *cb, int G, int k, int total,
+                                 cudaStream_t st) {
+  if (total <= 0) return;
+  k_lanczos_step_grouped<<<total, LNT, 0, st>>>(tab, cb, G, k);
 }
 
 // The same step with the chain's elements held in registers (EPT per thread,
@@ -500,11 +531,20 @@ __global__ void __launch_bounds__(LNT)
       }
       __syncthreads();
     }
-    // w = w - V h, and the new ||w||^2
+    // w = w - V h, and the new ||w||^2; the basis values of eight vectors
+    // are loaded before they are summed (in q order) so their loads overlap
     acc = 0.0;
     for (int i = threadIdx.x; i < ncv; i += LNT) {
       double u = 0.0;
-      for (int q = 0; q <= k; ++q) u += hq[q] * Vj[(size_t)q * ncv + i];
+      int q = 0;
+      for (; q + RG_Q <= k + 1; q += RG_Q) {
+        double x[RG_Q];
+#pragma unroll
+        for (int r = 0; r < RG_Q; ++r) x[r] = Vj[(size_t)(q + r) * ncv + i];
+#pragma unroll
+        for (int r = 0; r < RG_Q; ++r) u += hq[q + r] * x[r];
+      }
+      for (; q <= k; ++q) u += hq[q] * Vj[(size_t)q * ncv + i];
       const double wi = wj[i] - u;
       wj[i] = wi;
       acc += wi * wi;

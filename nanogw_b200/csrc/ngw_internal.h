@@ -202,6 +202,18 @@ void launch_lanczos_first(double *w, const double *v, int ncv, int nb, double *a
 void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb, int k,
                          double *a, double *b, int niter, const double *s, double *hs,
                          int tamm_d, int prescale_next, int *clen, double eps, cudaStream_t st);
+// one molecule's chains in a grouped Lanczos-step launch
+struct LanczosGroupEntry {
+  double *w, *v;
+  const double *t;
+  double *a, *b;
+  const double *s;
+  int *clen;
+  double eps;
+  int ncv, niter, prescale_next, pad;
+};
+void launch_lanczos_step_grouped(const LanczosGroupEntry *tab, const int *cb, int G, int k, int total,
+                                 cudaStream_t st);
 void launch_lanczos_reorth_step(double *w, double *v, const double *t, int ncv, int nb, int k, double *a,
                                 double *b, int niter, const double *s, double *hs, int tamm_d,
                                 int prescale_next, int *clen, double eps, double *basis, long long ldb,
