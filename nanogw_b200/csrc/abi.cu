@@ -1252,17 +1252,18 @@ int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_s
     NGW_TRY(sigma_block_setup(jobs[i], 0));
   }
   ngw_session *s0 = sessions[0];
-  // Small molecules (N_cv <= 8192, N_mu <= 512) in mixed precision, not TDA,
-  // with one polynomial degree run grouped: their Lanczos recurrences in lock
-  // step on one stream, each Clenshaw term of their p(C) v one grouped GEMM1
-  // and one grouped GEMM2 launch over all of them, one grouped step launch
-  // per Lanczos step.  Their GEMMs are a few tiles each; grouped they fill
-  // the GPU.  Larger molecules keep their own tuned tiles as graph branches
-  // running beside the group.  NGW_BATCH_MODE=branches groups nothing,
-  // NGW_BATCH_MODE=grouped groups every eligible entry whatever its size.
-  int mode = 0;   // 0 small only, 1 none, 2 every eligible entry
+  // Entries run as graph branches on their own streams with their tuned
+  // tiles (the default: measured fastest, the branches of small molecules
+  // overlap on the GPU).  NGW_BATCH_MODE=grouped_small groups the small
+  // mixed-precision molecules (N_cv <= 8192, N_mu <= 512, not TDA, one
+  // polynomial degree), NGW_BATCH_MODE=grouped every eligible molecule: their
+  // Lanczos recurrences in lock step on one stream, each Clenshaw term of
+  // their p(C) v one grouped GEMM1 and one grouped GEMM2 launch over all of
+  // them, one grouped step launch per Lanczos step, the other entries as
+  // branches beside the group.
+  int mode = 1;   // 0 small only, 1 none, 2 every eligible entry
   if (const char *e = getenv("NGW_BATCH_MODE")) {
-    if (std::string(e) == "branches") mode = 1;
+    if (std::string(e) == "grouped_small") mode = 0;
     if (std::string(e) == "grouped") mode = 2;
   }
   std::vector<int> grp, br;

@@ -91,9 +91,9 @@ class SigmaServer:
         group_work > 0 (mixed precision): a waiting request whose matvec work
         (``SigmaRequest.work``) is at most group_work is admitted together with
         up to group_max - 1 other such waiting requests, one free worker each,
-        and the group runs as one grouped batch (``sigma_lanczos_batch``: one
-        GEMM launch per Clenshaw term across the group's molecules).  Small
-        molecules' GEMMs are a few tiles each; grouped they fill the GPU."""
+        and the group runs as one batch (``sigma_lanczos_batch``; its form
+        follows NGW_BATCH_MODE: graph branches by default, grouped GEMM
+        launches across the molecules with ``grouped``)."""
         self.group_work = float(group_work) if precision == "mixed" else 0.0
         self.group_max = max(1, int(group_max))
         self.groups = 0                           # groups of two or more requests run

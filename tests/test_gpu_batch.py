@@ -1,15 +1,15 @@
 """Batched Sigma_c across molecules of uneven size (ngw_sigma_lanczos_batch).
 
-* Branch mode (NGW_BATCH_MODE=branches, and every FP64 batch): one graph
-  whose branches are the molecules' solves; each entry bit-identical to the
-  same session's single call, through the eager first call, the capture and
-  the replays.
-* Grouped mode (the default for mixed precision): the molecules' recurrences
-  in lock step, each Clenshaw term one grouped GEMM1 and one grouped GEMM2
-  launch over all of them.  With the single calls pinned to the grouped
-  tiles (64-wide, fused stages, no split-K) the results are bit-identical;
-  with the single calls on their own tuned tiles they agree to the mixed
-  form's rounding (QP energies within 1 meV).
+* Branch mode (the default): one graph whose branches are the molecules'
+  solves; each entry bit-identical to the same session's single call,
+  through the eager first call, the capture and the replays.
+* Grouped mode (NGW_BATCH_MODE=grouped): the molecules' recurrences in lock
+  step, each Clenshaw term one grouped GEMM1 and one grouped GEMM2 launch
+  over all of them, one grouped Lanczos-step launch per step.  With the
+  single calls pinned to the grouped tiles (64-wide, fused stages, no
+  split-K) the results are bit-identical; with the single calls on their own
+  tuned tiles they agree to the mixed form's rounding (QP energies within
+  1 meV).
 Per-chain lengths ride along (entry 1), so the grouped launches shrink as
 that molecule's chains finish."""
 import os
@@ -50,9 +50,8 @@ def env():
 @pytest.mark.parametrize("precision,mode", [("fp64", "branches"), ("mixed", "branches"),
                                             ("mixed", "grouped_pinned")])
 def test_batch_equals_single_calls(molecules, precision, mode, env):
-    if mode == "branches":
-        env["NGW_BATCH_MODE"] = "branches"
-    else:
+    if mode == "grouped_pinned":
+        env["NGW_BATCH_MODE"] = "grouped"
         env["NGW_TILES"] = "64,3,1,64,3"      # the grouped launches' tiles for the single calls
     sessions = []
     reqs = []
@@ -92,11 +91,12 @@ def test_batch_rejects_repeated_session(molecules):
         assert e.value.code == ngw._lib.NGW_ERR_ARG
 
 
-def test_grouped_batch_matches_tuned_single_calls(molecules):
+def test_grouped_batch_matches_tuned_single_calls(molecules, env):
     """Default grouped batch against single calls on their own tuned tiles:
     the same polynomial, deflation and FP64 recurrence, only the BF16 tile
     arithmetic differs -> QP energies within 1 meV."""
     RYD = 13.60569193
+    env["NGW_BATCH_MODE"] = "grouped"
     sessions, reqs = [], []
     try:
         for op, poly in molecules:

@@ -73,11 +73,13 @@ def test_footprint_bounds_session_bytes(requests, precision):
         srv.close()
 
 
-def test_grouped_small_requests_within_1mev(requests):
-    """Small requests admitted together run as one grouped batch (one GEMM
-    launch per Clenshaw term across their molecules, 64-wide tiles); each
-    QP energy within 1 meV of the same request served alone on its tuned
-    tiles."""
+@pytest.mark.parametrize("mode", ["branches", "grouped"])
+def test_grouped_small_requests_within_1mev(requests, mode, monkeypatch):
+    """Small requests admitted together run as one batch -- graph branches,
+    or grouped GEMM launches across their molecules (64-wide tiles) with
+    NGW_BATCH_MODE=grouped; each QP energy within 1 meV of the same request
+    served alone on its tuned tiles."""
+    monkeypatch.setenv("NGW_BATCH_MODE", mode)
     alone = {}
     for r in requests:
         srv = SigmaServer(workers=1, precision="mixed")
