@@ -36,6 +36,9 @@ WORKLOAD = dict(name="12-atom molecule, 30 occ + 90 empty, 600 ISDF points, 150 
                 h=0.35, n_occ=30, n_empty=90, n_isdf=600, niter=150, n_qp=6, nen=400,
                 deltae=4.0, ecuts=0.02, npoly=12, seed=11)
 METRIC = "Sigma_c solves/s"
+# DRAM bytes (read + write) of one in-situ dense p(C) GEMM of the 12-atom
+# workload from an ncu capture, by tile choice "bn,variant"
+MEASURED_TRAFFIC_DENSE = {}
 # DRAM bytes (read + write) of one in-situ GEMM1 + GEMM2 pair of the 12-atom
 # workload from an ncu capture, by tile choice "bn1,var1,split1,bn2,var2"
 # (GEMM1 [+ split-K reduce] + GEMM2, current kernels; ncu --metrics
@@ -825,10 +828,28 @@ def main():
         tot_ms = float(tt.item())
     value = world * K * nq / (tot_ms / 1e3)
 
-    # ---- roofline of the dominant kernel (the two tcgen05 GEMMs) ----
+    # ---- roofline of the dominant kernel: the dense p(C) GEMM when the plan
+    # chose the dense operator, else the two tcgen05 GEMMs of a matvec ----
     nb = nq * op.nmem
     roof = None
-    if args.precision == "mixed":
+    dense = sess.profile_dense_gemm(nb, reps=50) if args.precision == "mixed" else None
+    if dense is not None:
+        us_d, (Md, Nd, Kd, BNd, vd) = dense
+        flops = 2.0 * Md * Nd * Kd
+        achieved = flops / (us_d * 1e-6) / 1e12
+        hbm, bf16, bf16s, src = load_peaks()
+        # algorithmic bytes of one launch: H hi + lo (4 B per element), the
+        # split chain vectors (4 B), the FP64 output (8 B)
+        alg_bytes = 4.0 * Md * Kd + 4.0 * Nd * Kd + 8.0 * Md * Nd
+        roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+                "frac": achieved / bf16, "traffic": MEASURED_TRAFFIC_DENSE.get(f"{BNd},{vd}"),
+                "traffic_note": "ncu dram__bytes_read+write of one dense GEMM in situ (--ncu-case); null "
+                                "when the tuned tiles differ from the profiled ones",
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "kernel": "k_tc_gemm (dense p(C) GEMM: H v, one per Lanczos step)",
+                "form": "dense", "us_per_launch": us_d, "shape": [Md, Nd, Kd, BNd, vd],
+                "peak_source": f"{src} (bf16 dense, burst)", "executed_bf16_frac": 3.0 * achieved / bf16}
+    elif args.precision == "mixed":
         us1, us2 = sess.profile_mixed_gemms(nb, reps=50)
         M1, N1, K1, BN1, sp1, M2, N2, K2, BN2, v1, v2, sp2, _ = sess.mixed_gemm_shapes(nb)
         flops = 2.0 * M1 * N1 * K1 + 2.0 * M2 * N2 * K2
@@ -846,7 +867,7 @@ def main():
                                 "(--ncu-case); null when the tuned tiles differ from the "
                                 "profiled ones",
                 "algorithmic_bytes_per_matvec": alg_bytes,
-                "kernel": "k_tc_gemm (GEMM1 + GEMM2 of one matvec)",
+                "kernel": "k_tc_gemm (GEMM1 + GEMM2 of one matvec)", "form": "factored",
                 "us_per_launch": [us1, us2], "shapes": [[M1, N1, K1, BN1, sp1, v1], [M2, N2, K2, BN2, sp2, v2]],
                 "tiles_env": tiles,
                 "peak_source": f"{src} (bf16 dense, burst)",
@@ -953,7 +974,12 @@ def main():
     # the Sigma_c spectra / reduction
     per_mv = 2
     per_step = 2
-    if args.precision == "mixed" and roof is not None:
+    if args.precision == "mixed" and roof is not None and roof["form"] == "dense":
+        # dense form: per Lanczos step U^T v (FP64 GEMM + its K-slice sum), the
+        # split of the chain vectors, the dense GEMM and the Lanczos update
+        per_mv = 0
+        per_step = 5
+    elif args.precision == "mixed" and roof is not None:
         g1 = roof["shapes"][0]
         per_mv += 1 if (g1[4] > 1 and g1[5] not in (5, 6)) else 0
         per_step += 2

@@ -221,6 +221,12 @@ int ngw_profile_mixed_gemms(ngw_session *s, int nb, int reps, double *us_gemm1, 
  * splitK2, 0} of the two GEMMs (valid sizes, N tile, split-K, kernel
  * variant; split-K > 1 of GEMM2 only with the cluster variants 5 / 6). */
 int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape);
+/* The mixed form's dense p(C) GEMM (built when the last mixed plan chose the
+ * dense form, small N_cv): mean device time of one launch for nb chains to
+ * *us and shape[5] = {M, N, K, N tile, variant}; NGW_ERR_STATE when the
+ * session's plan used the factored form.  No reference counterpart: used by
+ * the benchmark. */
+int ngw_profile_dense_gemm(ngw_session *s, int nb, int reps, double *us, int *shape);
 
 /* Top Ritz pairs of the Casida operator (tamm_d 0: C = R^2 + 4 R^1/2 K R^1/2,
  * 1: the TDA matrix A) from an FP64 Lanczos run of msteps steps with full

@@ -49,6 +49,7 @@ SIGNATURES = {
     "ngw_profile_mixed_gemms": (_I, [_P, _I, _I, _P, _P]),
     "ngw_dgemm": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P, ctypes.c_longlong, _P]),
     "ngw_mixed_gemm_shapes": (_I, [_P, _I, _P]),
+    "ngw_profile_dense_gemm": (_I, [_P, _I, _I, _P, _P]),
     "ngw_operator_eigenpairs": (_I, [_P, _I, _I, _I, _P, _P, _P]),
     "ngw_shell_sort": (_I, [_I, _P, _P]),
     "ngw_cvt": (_I, [_I, _P, _P, _I, _P, _I, _P, _P]),

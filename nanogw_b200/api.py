@@ -215,6 +215,17 @@ class Session:
         check(lib().ngw_profile_mixed_gemms(self._h, int(nb), int(reps), _p(t1), _p(t2)))
         return float(t1[0]), float(t2[0])
 
+    def profile_dense_gemm(self, nb, reps=20):
+        """(us, [M, N, K, N tile, variant]) of the dense p(C) GEMM, or None when
+        the session's last mixed plan used the factored form."""
+        us = np.zeros(1)
+        sh = np.zeros(5, dtype=np.int32)
+        rc = lib().ngw_profile_dense_gemm(self._h, int(nb), int(reps), _p(us), _p(sh))
+        if rc == _lib.NGW_ERR_STATE:
+            return None
+        check(rc)
+        return float(us[0]), [int(x) for x in sh]
+
     def mixed_gemm_shapes(self, nb):
         sh = np.zeros(13, dtype=np.int32)
         check(lib().ngw_mixed_gemm_shapes(self._h, int(nb), _p(sh)))

@@ -22,6 +22,11 @@ int mixed_set_deflation_values(ngw_session *s, const double *pvals);
 int compute_top_eigs(ngw_session *s, int tamm_d, int kmax, int msteps);
 void extern_mixed_tune(ngw_session *s, int *tune);
 int mixed_prepare_chains(ngw_session *s, int nb, int bn1, int bn2, int split1);
+bool mixed_dense_ready(ngw_session *s, const double *g, int n, double c0, double c1);
+void mixed_dense_mark(ngw_session *s, bool used);
+int mixed_dense_build(ngw_session *s, const double *g, int n, double c0, double c1);
+int mixed_dense_apply(ngw_session *s, int nb, const double *v, int ldv, double *out64);
+int mixed_prepare_dense(ngw_session *s, int nb);
 int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const double *g, int n,
                      double c0, double c1, int tda, double *out64);
 void mixed_free(ngw_session *s);
@@ -208,6 +213,7 @@ struct PolyPlan {
   std::vector<double> cheb;   // Chebyshev coefficients (mixed)
   double c0 = 0, c1 = 1;
   int kdef = 0;               // deflated eigenpairs (mixed)
+  bool dense = false;         // mixed: p(C) through the dense operator H (one GEMM per product)
 };
 
 // t = p(H) vec  (or A vec with TDA) on device, in the session's precision.
@@ -219,6 +225,7 @@ static int apply_poly(ngw_session *s, const PolyPlan &pp, int nb, const double *
       const double g[2] = {pp.c0, pp.c1};
       return mixed_poly_apply(s, nb, vec, s->ncv, g, 1, pp.c0, pp.c1, 1, t);
     }
+    if (pp.dense) return mixed_dense_apply(s, nb, vec, s->ncv, t);
     return mixed_poly_apply(s, nb, vec, s->ncv, pp.cheb.data(), pp.npoly, pp.c0, pp.c1, 0, t);
   }
   if (pp.tamm_d) return matvec_f64_dev(s, nb, hs, t, vec, 1, 0, 0.0, 0.0, nullptr);
@@ -334,7 +341,31 @@ static double poly_eval(const std::vector<double> &p, double x) {
 // deflated while |p(lambda_k)| exceeds 4x the largest |p| on [0, 1.05
 // lambda_{k+1}] (the reference's fit leaves that range), so the Clenshaw
 // recurrence only ever sees a spectrum on which p is bounded.
-static int plan_mixed(ngw_session *s, PolyPlan &pp, double lo_in, double hi_in) {
+// Dense or factored p(C) for a solve of `steps` products on nb chains: the
+// dense operator costs 2 p N_cv^3 FP64 multiply-adds to form (unless it is
+// already built for this polynomial) and 2 N_cv^2 split-BF16 ones per chain
+// and product; the factored form 4 p (N_mu + k) N_cv per chain and product in
+// 2 p launches.  Rates: the FP64 tensor-core GEMM ~25 TFLOP/s, the dense
+// split-BF16 GEMM ~0.9 PFLOP/s executed (x3 products), the factored pair
+// ~0.6 PFLOP/s executed plus ~5 us per launch.  NGW_DENSE=0 / 1 overrides
+// (1 within the memory cap: N_cv <= 16384).
+static bool want_dense(ngw_session *s, const PolyPlan &pp, int steps, int nb) {
+  if (pp.tamm_d || pp.npoly < 2) return false;
+  const double N = s->ncv, mu = s->n_isdf + pp.kdef, p = pp.npoly;
+  if (N > 16384) return false;
+  if (const char *e = getenv("NGW_DENSE")) {
+    if (e[0] == '0') return false;
+    if (e[0] == '1') return true;
+  }
+  if (steps < 1 || nb < 1) return false;
+  const bool built = mixed_dense_ready(s, pp.cheb.data(), pp.npoly, pp.c0, pp.c1);
+  const double form = built ? 0.0 : 2.0 * p * N * N * N / 25e12;
+  const double dense_step = 3.0 * 2.0 * N * N * nb / 0.9e15 + 10e-6;
+  const double fact_step = p * (3.0 * 4.0 * mu * N * nb / 0.6e15 + 10e-6);
+  return form + steps * dense_step < steps * fact_step;
+}
+
+static int plan_mixed(ngw_session *s, PolyPlan &pp, double lo_in, double hi_in, int steps, int nb) {
   const int tda = pp.tamm_d;
   PhaseTimer tm(s);
   if (hi_in > lo_in) {
@@ -382,11 +413,15 @@ static int plan_mixed(ngw_session *s, PolyPlan &pp, double lo_in, double hi_in) 
   std::vector<double> pv(pp.kdef);
   for (int j = 0; j < pp.kdef; ++j) pv[j] = tda ? s->eig_vals[j] : poly_eval(pp.poly, s->eig_vals[j]);
   NGW_TRY(mixed_set_deflation_values(s, pv.data()));
+  pp.dense = want_dense(s, pp, steps, nb);
+  if (pp.dense) NGW_TRY(mixed_dense_build(s, pp.cheb.data(), pp.npoly, pp.c0, pp.c1));
+  mixed_dense_mark(s, pp.dense);
+  tm.mark("dense_operator");
   return NGW_OK;
 }
 
 static int make_plan(ngw_session *s, PolyPlan &pp, const double *poly, int npoly, int tamm_d,
-                     double lo, double hi) {
+                     double lo, double hi, int steps = 1, int nb = 1) {
   pp.tamm_d = tamm_d;
   if (!tamm_d) {
     if (!poly || npoly < 1) {
@@ -403,7 +438,7 @@ static int make_plan(ngw_session *s, PolyPlan &pp, const double *poly, int npoly
     pp.npoly = 1;
     pp.poly = {1.0, 0.0};
   }
-  if (s->precision == NGW_PREC_MIXED) NGW_TRY(plan_mixed(s, pp, lo, hi));
+  if (s->precision == NGW_PREC_MIXED) NGW_TRY(plan_mixed(s, pp, lo, hi, steps, nb));
   return NGW_OK;
 }
 
@@ -528,7 +563,8 @@ static int sigma_prepare(SigmaJob &J, ngw_session *s, const ngw_sigma_params *p,
   J.tamm_d = p->tamm_d ? 1 : 0;
   // Chebyshev interval of the mixed form: from the operator's eigenpairs
   // unless given (cheb_lo < cheb_hi)
-  NGW_TRY(make_plan(s, J.pp, p->polynomial, p->npoly, J.tamm_d, p->cheb_lo, p->cheb_hi));
+  NGW_TRY(make_plan(s, J.pp, p->polynomial, p->npoly, J.tamm_d, p->cheb_lo, p->cheb_hi, p->niter,
+                    p->nqp * nbsum));
   // chain blocking: whole QP states per block
   J.nq_blk = p->nqp;
   if (p->block_chains > 0) J.nq_blk = std::max(1, std::min(p->nqp, p->block_chains / nbsum));
@@ -581,7 +617,10 @@ static int sigma_prepare(SigmaJob &J, ngw_session *s, const ngw_sigma_params *p,
     J.ldb = (long long)(niter + 1) * ncv;
     NGW_TRY(scratch(s, SL_BASIS, (size_t)nb_max * (size_t)J.ldb * 8, (void **)&J.basis));
   }
-  if (s->precision == NGW_PREC_MIXED) NGW_TRY(mixed_prepare_chains(s, nb_max, 0, 0, 0));
+  if (s->precision == NGW_PREC_MIXED) {
+    NGW_TRY(mixed_prepare_chains(s, nb_max, 0, 0, 0));
+    if (J.pp.dense) NGW_TRY(mixed_prepare_dense(s, nb_max));
+  }
   NGW_CUDA(cudaMemcpyAsync(J.de1, e1, (size_t)s->nmem * 8, cudaMemcpyHostToDevice, s->stream));
   // energy grid origin per QP state: en0 = e1(m) - deltae/2, step deltae/(nen-1)
   std::vector<double> hz0(p->nqp);
@@ -793,7 +832,7 @@ static void sigma_key(const SigmaJob &J, std::vector<unsigned long long> &key) {
       (unsigned long long)J.pp.npoly, (unsigned long long)J.tamm_d, (unsigned long long)J.nen,
       (unsigned long long)p->nval, (unsigned long long)J.nbsum, (unsigned long long)J.nq,
       (unsigned long long)J.q0, (unsigned long long)J.pp.kdef, dbits(p->ecuts), dbits(J.de),
-      dbits(J.pp.c0), dbits(J.pp.c1), s->gen, dbits(p->early_exit_eps),
+      dbits(J.pp.c0), dbits(J.pp.c1), s->gen, dbits(p->early_exit_eps), (unsigned long long)J.pp.dense,
       (unsigned long long)(J.len != nullptr), (unsigned long long)(uintptr_t)J.basis,
       (unsigned long long)J.ldb};
   key.insert(key.end(), std::begin(head), std::end(head));
@@ -808,7 +847,7 @@ static void sigma_key(const SigmaJob &J, std::vector<unsigned long long> &key) {
                           (const void *)J.clen, (const void *)J.dlen, (const void *)J.dslot, (const void *)J.dgws})
     key.push_back((unsigned long long)(uintptr_t)ptr);
   if (s->mixed) {
-    int tune[4];
+    int tune[6];
     extern_mixed_tune(s, tune);
     for (int t : tune) key.push_back((unsigned long long)t);
   }
@@ -1112,7 +1151,7 @@ int ngw_lanczos_spectra_isdf_masked(ngw_session *s, const double *v0, const doub
   NGW_CUDA(cudaSetDevice(s->device));
   const int ncv = s->ncv, nb = blksz;
   PolyPlan pp;
-  NGW_TRY(make_plan(s, pp, polynomial, npoly, tamm_d, 0.0, 0.0));
+  NGW_TRY(make_plan(s, pp, polynomial, npoly, tamm_d, 0.0, 0.0, niter, blksz));
   double *dv0, *V, *W, *hs, *tmp, *a, *b, *dzz, *dspec, *dnorm;
   NGW_TRY(scratch(s, SL_IN, (size_t)ncv * nb * 8, (void **)&dv0));
   NGW_TRY(scratch(s, SL_VEC, (size_t)ncv * nb * 8, (void **)&V));
@@ -1130,7 +1169,10 @@ int ngw_lanczos_spectra_isdf_masked(ngw_session *s, const double *v0, const doub
     NGW_TRY(scratch(s, SL_LEN, (size_t)nb * 4, (void **)&dlen));
     NGW_CUDA(cudaMemcpyAsync(dlen, chain_niter, (size_t)nb * 4, cudaMemcpyHostToDevice, s->stream));
   }
-  if (s->precision == NGW_PREC_MIXED) NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
+  if (s->precision == NGW_PREC_MIXED) {
+    NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
+    if (pp.dense) NGW_TRY(mixed_prepare_dense(s, nb));
+  }
   NGW_CUDA(cudaMemcpy2DAsync(dv0, (size_t)ncv * 8, v0, (size_t)ld * 8, (size_t)ncv * 8, nb,
                              cudaMemcpyHostToDevice, s->stream));
   NGW_CUDA(cudaMemcpyAsync(dnorm, v0_norm, (size_t)nb * 8, cudaMemcpyHostToDevice, s->stream));
@@ -1256,7 +1298,8 @@ int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_s
   // tiles (the default: measured fastest, the branches of small molecules
   // overlap on the GPU).  NGW_BATCH_MODE=grouped_small groups the small
   // mixed-precision molecules (N_cv <= 8192, N_mu <= 512, not TDA, one
-  // polynomial degree), NGW_BATCH_MODE=grouped every eligible molecule: their
+  // polynomial degree, factored p(C): entries whose plan chose the dense
+  // operator stay branches), NGW_BATCH_MODE=grouped every eligible molecule: their
   // Lanczos recurrences in lock step on one stream, each Clenshaw term of
   // their p(C) v one grouped GEMM1 and one grouped GEMM2 launch over all of
   // them, one grouped step launch per Lanczos step, the other entries as
@@ -1269,7 +1312,7 @@ int ngw_sigma_lanczos_batch(ngw_session *const *sessions, int count, const ngw_s
   std::vector<int> grp, br;
   for (int i = 0; i < count; ++i) {
     const SigmaJob &J = jobs[i];
-    const bool eligible = mode != 1 && sessions[i]->precision == NGW_PREC_MIXED && !J.tamm_d &&
+    const bool eligible = mode != 1 && sessions[i]->precision == NGW_PREC_MIXED && !J.tamm_d && !J.pp.dense &&
                           (int)J.pp.cheb.size() == J.pp.npoly + 1 &&
                           (grp.empty() || J.pp.npoly == jobs[grp[0]].pp.npoly) &&
                           (mode == 2 || (J.ncv <= 8192 && J.n <= 512));

@@ -72,6 +72,7 @@ struct EpiParams {
   bf16 *s_hi, *s_lo;     // split of (R^1/2 or 1) * out  [n * lds + m] (nullable)
   int lds;
   int ring;              // EPI_CLENSHAW in k_tc_gemm: operands through the TMA chunk ring
+  int dense;             // EPI_CLENSHAW as a plain product: out64 = z (+ deflated term), no operands
 };
 
 struct GemmArgs {
@@ -95,7 +96,7 @@ __device__ __forceinline__ void clenshaw_operands(const EpiParams &ep, bool mv, 
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     const size_t o = (size_t)(nbase + j) * ep.ldx + m;
-    x[j] = (j < nj) ? __ldg(ep.x + o) : 0.f;
+    x[j] = (j < nj && ep.x) ? __ldg(ep.x + o) : 0.f;
     b2[j] = (j < nj && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
     v[j] = (j < nj && ep.v) ? __ldg(ep.v + o) : 0.f;
   }
@@ -109,7 +110,7 @@ __device__ __forceinline__ void clenshaw_operands4(const EpiParams &ep, bool mv,
     const int nn = n + j * step;
     const bool ok = mv && nn < n_end && nn < ep.Nv;
     const size_t o = (size_t)nn * ep.ldx + m;
-    x[j] = ok ? __ldg(ep.x + o) : 0.f;
+    x[j] = (ok && ep.x) ? __ldg(ep.x + o) : 0.f;
     b2[j] = (ok && ep.b2) ? __ldg(ep.b2 + o) : 0.f;
     v[j] = (ok && ep.v) ? __ldg(ep.v + o) : 0.f;
   }
@@ -129,8 +130,17 @@ struct ClenCoef {
 };
 
 __device__ __forceinline__ ClenCoef clen_coef(const EpiParams &ep, double si) {
-  const double s2 = si * si;
   ClenCoef k;
+  if (ep.dense) {   // out = z
+    k.d = 0.f;
+    k.kz = 1.f;
+    k.sc = 1.f;
+    k.ga = 0.f;
+    k.al = 1.f;
+    k.mbe = 0.f;
+    return k;
+  }
+  const double s2 = si * si;
   k.d = (float)((ep.tda ? s2 : s2 * s2) - ep.c0);
   k.kz = (float)(ep.tda ? 2.0 : 4.0 * si);
   k.sc = (float)(ep.tda ? 1.0 : si);
@@ -1345,6 +1355,21 @@ struct MixedOperator {
   double *xo = nullptr;
   float *ws = nullptr;
   size_t buf_bytes = 0;
+  // dense form (small N_cv): H = P_perp p(Chat_perp) as one split-BF16 matrix
+  // H[m][k] (rows cv_pad, row length kpad), built in FP64 for the polynomial
+  // dense_g on [dense_c0 - dense_c1, dense_c0 + dense_c1]
+  bf16 *H_hi = nullptr, *H_lo = nullptr;
+  CUtensorMap tHhi, tHlo;
+  int kpad = 0;
+  bool dense_ok = false;
+  bool dense_last = false;      // the session's last mixed plan used H
+  std::vector<double> dense_g;
+  double dense_c0 = 0.0, dense_c1 = 0.0;
+  size_t dense_bytes = 0;
+  // dense GEMM tiles (N tile, variant), tuned per chain count; S_hi / S_lo
+  // as its B operand with that N tile
+  int BNd = 128, vard = 3, tuned_nbd = -1, maps_bnd = -1;
+  CUtensorMap tVhi, tVlo;
 };
 
 static int round_up(int a, int b) { return (a + b - 1) / b * b; }
@@ -1375,12 +1400,24 @@ static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
   op->maps_te_bn = -1;
   op->maps_ring = false;
   op->tuned_nb = -1;
+  op->maps_bnd = -1;
+  op->tuned_nbd = -1;
+}
+
+static void free_dense(ngw_session *s, MixedOperator *op) {
+  pool_free(s, op->H_hi);
+  pool_free(s, op->H_lo);
+  op->H_hi = op->H_lo = nullptr;
+  s->bytes -= op->dense_bytes;
+  op->dense_bytes = 0;
+  op->dense_ok = false;
 }
 
 void mixed_free(ngw_session *s) {
   MixedOperator *op = s->mixed;
   if (!op) return;
   free_chain_buffers(s, op);
+  free_dense(s, op);
   void *ptrs[] = {op->A1_hi, op->A1_lo, op->A3_hi, op->A3_lo, op->Up};
   for (void *p : ptrs)
     pool_free(s, p);
@@ -1398,6 +1435,8 @@ void extern_mixed_tune(ngw_session *s, int *tune) {
   tune[1] = op->split1;
   tune[2] = (op->BN2 * 16 + op->var2) * 16 + op->split2;
   tune[3] = op->nb_cap;
+  tune[4] = op->BNd * 16 + op->vard;
+  tune[5] = op->dense_ok ? 1 : 0;
 }
 
 int matvec_f64_dev_pub(ngw_session *s, int nb, double *hs, double *y, int tamm_d);
@@ -1437,6 +1476,7 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
     }
     s->bytes += op->op_bytes;
   }
+  op->dense_ok = false;   // H (if any) belongs to the previous operator values
   cudaStream_t st = s->stream;
   NGW_CUDA(cudaMemsetAsync(op->A1_hi, 0, a1, st));
   NGW_CUDA(cudaMemsetAsync(op->A1_lo, 0, a1, st));
@@ -2016,6 +2056,319 @@ int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const dou
 }
 
 // ---------------------------------------------------------------------------
+// Dense form of p(C) for small N_cv.  When N_cv is small against the ISDF
+// rank the operator itself is cheaper to apply than its factors:
+//   H = P_perp p(Chat_perp),  Chat_perp = (P_perp C P_perp - c0) / c1,
+// P_perp = I - U U^T (the deflated Ritz vectors), is formed once per operator
+// and polynomial in FP64 (C = R^2 + 4 R^1/2 (C_isdf^T M C_isdf) R^1/2, the
+// deflation as rank-k updates, then the Clenshaw recurrence of the vector
+// form with matrices: B_n = g_n P, B_k = g_k P + 2 Chat B_{k+1} - B_{k+2},
+// H = g_0 P + Chat B_1 - B_2, one FP64 tensor-core GEMM per term), split into
+// BF16 hi/lo rows, and every p(C) v of the Lanczos recurrence is then ONE
+// tcgen05 GEMM H v (split-BF16, FP32 accumulation) whose epilogue adds the
+// deflated eigenpairs' U p(Lambda) U^T v in FP64 -- the same quantity the
+// Clenshaw recurrence on vectors delivers, with 2 N_cv^2 instead of
+// 4 p (N_mu + k) N_cv multiply-adds per chain.
+
+// C(i, j) = 4 s_i K(i, j) s_j + delta_ij s_i^4   (s = R^1/2), in place
+__global__ void k_dense_casida(double *__restrict__ K, const double *__restrict__ s, int n) {
+  const size_t total = (size_t)n * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), j = (int)(e / n);
+    double v = 4.0 * s[i] * K[e] * s[j];
+    if (i == j) v += s[i] * s[i] * s[i] * s[i];
+    K[e] = v;
+  }
+}
+
+// A = (A - c0 I) * f  in place
+__global__ void k_dense_shift(double *__restrict__ A, int n, double c0, double f) {
+  const size_t total = (size_t)n * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), j = (int)(e / n);
+    A[e] = (A[e] - (i == j ? c0 : 0.0)) * f;
+  }
+}
+
+__global__ void k_dense_identity(double *__restrict__ A, int n) {
+  const size_t total = (size_t)n * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
+    A[e] = ((int)(e % n) == (int)(e / n)) ? 1.0 : 0.0;
+}
+
+// out = g P - b2 (b2 nullable)
+__global__ void k_dense_comb(const double *__restrict__ P, const double *__restrict__ b2, double g, size_t total,
+                             double *__restrict__ out) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
+    out[e] = g * P[e] - (b2 ? b2[e] : 0.0);
+}
+
+// columns of X (ncv x nb, leading dimension ldx, FP64) -> rows [j][cv] of
+// the split-BF16 pair (row length lds)
+__global__ void k_split_cols(const double *__restrict__ X, int ldx, int ncv, int nb, bf16 *__restrict__ hi,
+                             bf16 *__restrict__ lo, int lds) {
+  for (int j = blockIdx.y; j < nb; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
+      const double x = X[(size_t)j * ldx + i];
+      const bf16 h = __double2bfloat16(x);
+      hi[(size_t)j * lds + i] = h;
+      lo[(size_t)j * lds + i] = __double2bfloat16(x - (double)__bfloat162float(h));
+    }
+}
+
+static unsigned elem_blocks(size_t total) {
+  return (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+}
+
+void mixed_dense_mark(ngw_session *s, bool used) {
+  if (s->mixed) s->mixed->dense_last = used;
+}
+
+bool mixed_dense_ready(ngw_session *s, const double *g, int n, double c0, double c1) {
+  const MixedOperator *op = s->mixed;
+  if (!op || !op->dense_ok || op->dense_c0 != c0 || op->dense_c1 != c1 || (int)op->dense_g.size() != n + 1)
+    return false;
+  for (int i = 0; i <= n; ++i)
+    if (op->dense_g[i] != g[i]) return false;
+  return true;
+}
+
+int mixed_dense_build(ngw_session *s, const double *g, int n, double c0, double c1) {
+  MixedOperator *op = s->mixed;
+  if (!op || op->tda || n < 1 || c1 == 0.0) {
+    set_error("dense p(C): needs the mixed operator (not TDA) and a polynomial of degree >= 1");
+    return NGW_ERR_STATE;
+  }
+  if (mixed_dense_ready(s, g, n, c0, c1)) return NGW_OK;
+  const int N = s->ncv, ni = s->n_isdf, k = op->kdef;
+  const int kpad = round_up(N, BK);
+  const size_t hbytes = (size_t)op->cv_pad * kpad * sizeof(bf16);
+  if (!op->H_hi || op->kpad != kpad) {
+    bump_generation(s);
+    free_dense(s, op);
+    NGW_CUDA(pool_alloc(s, (void **)&op->H_hi, hbytes));
+    NGW_CUDA(pool_alloc(s, (void **)&op->H_lo, hbytes));
+    op->kpad = kpad;
+    op->dense_bytes = 2 * hbytes;
+    s->bytes += op->dense_bytes;
+  }
+  op->dense_ok = false;
+  cudaStream_t st = s->stream;
+  const size_t nn = (size_t)N * N;
+  PoolTmp tC(s), tP(s), tB0(s), tB1(s), tB2(s), tD(s), tG(s);
+  NGW_CUDA(pool_alloc(s, &tC.p, nn * 8));
+  NGW_CUDA(pool_alloc(s, &tP.p, nn * 8));
+  NGW_CUDA(pool_alloc(s, &tB0.p, nn * 8));
+  NGW_CUDA(pool_alloc(s, &tB1.p, nn * 8));
+  NGW_CUDA(pool_alloc(s, &tB2.p, nn * 8));
+  NGW_CUDA(pool_alloc(s, &tD.p, (size_t)ni * N * 8));
+  double *Cm = static_cast<double *>(tC.p), *P = static_cast<double *>(tP.p), *D = static_cast<double *>(tD.p);
+  double *buf[3] = {static_cast<double *>(tB0.p), static_cast<double *>(tB1.p), static_cast<double *>(tB2.p)};
+  // C = R^2 + 4 R^1/2 (C_isdf^T (M C_isdf)) R^1/2
+  NGW_CUDA(dgemm(st, false, false, ni, N, ni, 1.0, s->d_M, ni, s->d_C, ni, 0.0, D, ni));
+  NGW_CUDA(dgemm(st, true, false, N, N, ni, 1.0, s->d_C, ni, D, ni, 0.0, Cm, N));
+  k_dense_casida<<<elem_blocks(nn), 256, 0, st>>>(Cm, s->d_sqrtR, N);
+  k_dense_identity<<<elem_blocks(nn), 256, 0, st>>>(P, N);
+  NGW_CUDA(cudaGetLastError());
+  if (k > 0) {
+    // P C P = C - U G^T - Y U^T with G = C U, Y = G - U (U^T G); P = I - U U^T
+    NGW_CUDA(pool_alloc(s, &tG.p, ((size_t)2 * N * k + (size_t)k * k) * 8));
+    double *G = static_cast<double *>(tG.p), *Y = G + (size_t)N * k, *Wk = Y + (size_t)N * k;
+    const double *U = s->eig_U;
+    NGW_CUDA(dgemm(st, false, false, N, k, N, 1.0, Cm, N, U, N, 0.0, G, N));
+    NGW_CUDA(dgemm(st, true, false, k, k, N, 1.0, U, N, G, N, 0.0, Wk, k));
+    NGW_CUDA(cudaMemcpyAsync(Y, G, (size_t)N * k * 8, cudaMemcpyDeviceToDevice, st));
+    NGW_CUDA(dgemm(st, false, false, N, k, k, -1.0, U, N, Wk, k, 1.0, Y, N));
+    NGW_CUDA(dgemm(st, false, true, N, N, k, -1.0, U, N, G, N, 1.0, Cm, N));
+    NGW_CUDA(dgemm(st, false, true, N, N, k, -1.0, Y, N, U, N, 1.0, Cm, N));
+    NGW_CUDA(dgemm(st, false, true, N, N, k, -1.0, U, N, U, N, 1.0, P, N));
+  }
+  k_dense_shift<<<elem_blocks(nn), 256, 0, st>>>(Cm, N, c0, 1.0 / c1);
+  NGW_CUDA(cudaGetLastError());
+  // matrix Clenshaw, the buffer roles rotating as in mixed_poly_apply
+  int i1 = 0, i2 = -1;
+  k_dense_comb<<<elem_blocks(nn), 256, 0, st>>>(P, nullptr, g[n], nn, buf[0]);
+  for (int kk = n - 1; kk >= 0; --kk) {
+    const int io = (i2 < 0) ? 1 : 3 - i1 - i2;
+    k_dense_comb<<<elem_blocks(nn), 256, 0, st>>>(P, i2 < 0 ? nullptr : buf[i2], g[kk], nn, buf[io]);
+    NGW_CUDA(cudaGetLastError());
+    NGW_CUDA(dgemm(st, false, false, N, N, N, kk > 0 ? 2.0 : 1.0, Cm, N, buf[i1], N, 1.0, buf[io], N));
+    i2 = i1;
+    i1 = io;
+  }
+  // H (buf[i1]) -> split BF16 rows H[m][k]; padding rows / columns zero
+  NGW_CUDA(cudaMemsetAsync(op->H_hi, 0, hbytes, st));
+  NGW_CUDA(cudaMemsetAsync(op->H_lo, 0, hbytes, st));
+  {
+    dim3 grid((N + 31) / 32, (N + 31) / 32);
+    k_split_transpose<<<grid, dim3(32, 8), 0, st>>>(buf[i1], N, N, op->H_hi, op->H_lo, kpad);
+    NGW_CUDA(cudaGetLastError());
+  }
+  NGW_CUDA(cudaStreamSynchronize(st));
+  NGW_TRY(make_tmap(&op->tHhi, op->H_hi, op->cv_pad, kpad, BM));
+  NGW_TRY(make_tmap(&op->tHlo, op->H_lo, op->cv_pad, kpad, BM));
+  op->dense_g.assign(g, g + n + 1);
+  op->dense_c0 = c0;
+  op->dense_c1 = c1;
+  op->dense_ok = true;
+  return check_status(s);
+}
+
+static int encode_dense_maps(MixedOperator *op, int bn) {
+  if (op->maps_bnd != bn) {
+    NGW_TRY(make_tmap(&op->tVhi, op->S_hi, op->nb_pad, op->cv_pad, bn));
+    NGW_TRY(make_tmap(&op->tVlo, op->S_lo, op->nb_pad, op->cv_pad, bn));
+    op->maps_bnd = bn;
+  }
+  return NGW_OK;
+}
+
+// out64 (ncv x nb, ld ldv) = H S + U p(Lambda) xo, S = the split chain vectors
+static int run_dense_gemm(ngw_session *s, int nb, double *out64, int ldv) {
+  MixedOperator *op = s->mixed;
+  GemmArgs ga;
+  ga.num_kb = op->kpad / BK;
+  ga.nseg = 3;
+  ga.nsplit = 1;
+  EpiParams ep;
+  std::memset(&ep, 0, sizeof(ep));
+  ep.kind = EPI_CLENSHAW;
+  ep.dense = 1;
+  ep.Mv = s->ncv;
+  ep.Nv = nb;
+  ep.s = s->d_sqrtR;
+  ep.ldx = op->cv_pad;
+  ep.ldv = ldv;
+  ep.out64 = out64;
+  if (op->kdef > 0) {
+    ep.Up = op->Up;
+    ep.xo = op->xo;
+    ep.kdef = op->kdef;
+  }
+  const int tiles_m = op->cv_pad / BM;
+  const int tiles_n = (nb + op->BNd - 1) / op->BNd;
+  return dispatch_tc(op->BNd, op->vard, op->tHhi, op->tHlo, op->tVhi, op->tVlo, tiles_m, tiles_n, ga, ep,
+                     s->d_status, s->stream);
+}
+
+// out64 = p(C) v through the dense operator.  Launch-only.
+int mixed_dense_apply(ngw_session *s, int nb, const double *v, int ldv, double *out64) {
+  MixedOperator *op = s->mixed;
+  if (!op || !op->dense_ok || op->nb_cap < nb || op->maps_bnd != op->BNd) {
+    set_error("dense p(C): operator or chain buffers not prepared");
+    return NGW_ERR_STATE;
+  }
+  const int N = s->ncv, k = op->kdef;
+  cudaStream_t st = s->stream;
+  if (k > 0)
+    NGW_CUDA(dgemm(st, true, false, k, nb, N, 1.0, s->eig_U, N, v, ldv, 0.0, op->xo, k,
+                   reinterpret_cast<double *>(op->ws), op->ws_bytes));
+  k_split_cols<<<dim3(std::min(16, (N + 255) / 256), ygrid(nb)), 256, 0, st>>>(v, ldv, N, nb, op->S_hi, op->S_lo,
+                                                                           op->cv_pad);
+  NGW_CUDA(cudaGetLastError());
+  return run_dense_gemm(s, nb, out64, ldv);
+}
+
+// Tile choice of the dense GEMM for nb chains: process-wide cache keyed by
+// the shapes (so a request gives the same bits alone or among others), else
+// every admissible (N tile, variant) timed on a quiet device.
+// NGW_DENSE_TILES="bn,var" fixes it.
+struct DenseKey {
+  int cv_pad, kpad, nb, defl;
+  bool operator<(const DenseKey &o) const {
+    return std::tie(cv_pad, kpad, nb, defl) < std::tie(o.cv_pad, o.kpad, o.nb, o.defl);
+  }
+};
+static std::mutex g_dtune_mu;
+static std::map<DenseKey, std::pair<int, int>> g_dtune;
+
+int mixed_prepare_dense(ngw_session *s, int nb) {
+  MixedOperator *op = s->mixed;
+  if (!op || !op->dense_ok) return NGW_OK;
+  if (op->nb_cap < nb) {
+    set_error("dense p(C): chain buffers not prepared");
+    return NGW_ERR_STATE;
+  }
+  if (op->tuned_nbd == nb && op->maps_bnd == op->BNd) return NGW_OK;
+  if (const char *env = getenv("NGW_DENSE_TILES")) {
+    int bn = 0, var = 0;
+    if (sscanf(env, "%d,%d", &bn, &var) == 2) {
+      op->BNd = bn;
+      op->vard = var;
+      op->tuned_nbd = nb;
+      return encode_dense_maps(op, bn);
+    }
+  }
+  const DenseKey key{op->cv_pad, op->kpad, nb, op->kdef > 0 ? 1 : 0};
+  {
+    std::lock_guard<std::mutex> lk(g_dtune_mu);
+    auto it = g_dtune.find(key);
+    if (it != g_dtune.end()) {
+      op->BNd = it->second.first;
+      op->vard = it->second.second;
+      op->tuned_nbd = nb;
+      return encode_dense_maps(op, op->BNd);
+    }
+  }
+  std::vector<std::pair<int, int>> cand;
+  for (int bn : kBNs) {
+    if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
+    if ((round_up(nb, bn) - nb) * 8 > nb && bn != kBNs[0]) continue;
+    for (int var : {0, 1, 2, 3, 4}) {
+      if (var == 1 && !has_shallow(bn)) continue;
+      if (var == 2 && !has_persistent(bn)) continue;
+      if (var == 3 && !has_fused(bn)) continue;
+      if (var == 4 && !has_fused2(bn)) continue;
+      cand.push_back({bn, var});
+    }
+  }
+  PoolTmp tout(s);
+  NGW_CUDA(pool_alloc(s, &tout.p, (size_t)s->ncv * nb * 8));
+  double *out = static_cast<double *>(tout.p);
+  std::unique_lock<std::shared_mutex> quiet(gpu_quiet_lock(s->device));
+  NGW_CUDA(cudaMemsetAsync(op->xo, 0, (size_t)nb * std::max(op->kdef, 1) * 8, s->stream));
+  cudaEvent_t e0, e1;
+  NGW_CUDA(cudaEventCreate(&e0));
+  NGW_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  std::pair<int, int> pick = cand.empty() ? std::make_pair(128, 3) : cand[0];
+  const bool verbose = getenv("NGW_TUNE_VERBOSE") != nullptr;
+  int rc = NGW_OK;
+  for (const auto &c : cand) {
+    op->BNd = c.first;
+    op->vard = c.second;
+    if ((rc = encode_dense_maps(op, c.first)) != NGW_OK) break;
+    if ((rc = run_dense_gemm(s, nb, out, s->ncv)) != NGW_OK) break;
+    float ms = 0.f;
+    cudaEventRecord(e0, s->stream);
+    for (int r = 0; r < 3 && rc == NGW_OK; ++r) rc = run_dense_gemm(s, nb, out, s->ncv);
+    cudaEventRecord(e1, s->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      set_error("dense GEMM tuning failed");
+      rc = NGW_ERR_CUDA;
+    }
+    if (rc != NGW_OK) break;
+    if (verbose) fprintf(stderr, "tune dense bn=%d var=%d: %.2f us\n", c.first, c.second, 1e3f * ms / 3);
+    if (ms < best) {
+      best = ms;
+      pick = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  NGW_TRY(rc);
+  op->BNd = pick.first;
+  op->vard = pick.second;
+  op->tuned_nbd = nb;
+  NGW_TRY(encode_dense_maps(op, op->BNd));
+  {
+    std::lock_guard<std::mutex> lk(g_dtune_mu);
+    g_dtune[key] = pick;
+  }
+  return check_status(s);
+}
+
+// ---------------------------------------------------------------------------
 // p(C) v for several molecules with the GEMMs grouped: per Clenshaw term one
 // grouped GEMM1 and one grouped GEMM2 over every molecule still running
 // (k_tc_gemm_grouped), the Clenshaw start per molecule.  The tables are
@@ -2233,6 +2586,47 @@ extern "C" int ngw_profile_mixed_gemms(ngw_session *s, int nb, int reps, double 
   cudaEventDestroy(e2);
   *us_gemm1 = 1e3 * t1 / reps;
   *us_gemm2 = 1e3 * t2 / reps;
+  return check_status(s);
+}
+
+// The dense p(C) GEMM of the mixed form (when the session's last plan built
+// it): mean device time of one launch for nb chains and its shape.
+extern "C" int ngw_profile_dense_gemm(ngw_session *s, int nb, int reps, double *us, int *shape) {
+  using namespace ngw;
+  if (!s || nb <= 0 || reps <= 0 || !us || !shape) {
+    set_error("ngw_profile_dense_gemm: bad arguments");
+    return NGW_ERR_ARG;
+  }
+  if (!s->mixed || !s->mixed->dense_ok || !s->mixed->dense_last) {
+    set_error("dense p(C) operator not in use (the last mixed plan used the factored form)");
+    return NGW_ERR_STATE;
+  }
+  NGW_CUDA(cudaSetDevice(s->device));
+  NGW_TRY(mixed_prepare_chains(s, nb, 0, 0, 0));
+  NGW_TRY(mixed_prepare_dense(s, nb));
+  MixedOperator *op = s->mixed;
+  PoolTmp tout(s);
+  NGW_CUDA(pool_alloc(s, &tout.p, (size_t)s->ncv * nb * 8));
+  double *out = static_cast<double *>(tout.p);
+  NGW_CUDA(cudaMemsetAsync(op->xo, 0, (size_t)nb * std::max(op->kdef, 1) * 8, s->stream));
+  cudaEvent_t e0, e1;
+  NGW_CUDA(cudaEventCreate(&e0));
+  NGW_CUDA(cudaEventCreate(&e1));
+  NGW_TRY(run_dense_gemm(s, nb, out, s->ncv));   // warm
+  NGW_CUDA(cudaEventRecord(e0, s->stream));
+  for (int i = 0; i < reps; ++i) NGW_TRY(run_dense_gemm(s, nb, out, s->ncv));
+  NGW_CUDA(cudaEventRecord(e1, s->stream));
+  NGW_CUDA(cudaEventSynchronize(e1));
+  float t = 0;
+  NGW_CUDA(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *us = 1e3 * t / reps;
+  shape[0] = s->ncv;
+  shape[1] = nb;
+  shape[2] = s->ncv;
+  shape[3] = op->BNd;
+  shape[4] = op->vard;
   return check_status(s);
 }
 

@@ -2,7 +2,8 @@
 
 * Branch mode (the default): one graph whose branches are the molecules'
   solves; each entry bit-identical to the same session's single call,
-  through the eager first call, the capture and the replays.
+  through the eager first call, the capture and the replays (these small
+  molecules take the dense p(C) form).
 * Grouped mode (NGW_BATCH_MODE=grouped): the molecules' recurrences in lock
   step, each Clenshaw term one grouped GEMM1 and one grouped GEMM2 launch
   over all of them, one grouped Lanczos-step launch per step.  With the
@@ -52,6 +53,7 @@ def env():
 def test_batch_equals_single_calls(molecules, precision, mode, env):
     if mode == "grouped_pinned":
         env["NGW_BATCH_MODE"] = "grouped"
+        env["NGW_DENSE"] = "0"                # grouped launches run the factored p(C)
         env["NGW_TILES"] = "64,3,1,64,3"      # the grouped launches' tiles for the single calls
     sessions = []
     reqs = []
@@ -97,6 +99,7 @@ def test_grouped_batch_matches_tuned_single_calls(molecules, env):
     arithmetic differs -> QP energies within 1 meV."""
     RYD = 13.60569193
     env["NGW_BATCH_MODE"] = "grouped"
+    env["NGW_DENSE"] = "0"
     sessions, reqs = [], []
     try:
         for op, poly in molecules:

@@ -119,6 +119,39 @@ def test_sigma_lanczos_fp64(sess, small_system, tamm_d):
         assert np.all(np.max(np.abs(ai - ar) / np.abs(ar), axis=1) <= tol)
 
 
+@pytest.mark.parametrize("nbsum", [5, 20])
+def test_sigma_band_subset(sess, small_system, nbsum):
+    """nbands_sum: Sigma_c summed over bands 1..nbsum only, for QP bands below
+    and above nbsum.  FP64 against the oracle's sum over the same bands with
+    both recurrences fully reorthogonalised (stable, so held to 1e-8: the
+    unreorthogonalised one separates two FP64 codes within a few steps on this
+    system), and the mixed form's QP energies against the FP64 ones, both
+    reorthogonalised (within 1 meV)."""
+    S = small_system
+    qp = np.array([S.nval - 1, S.nval + 1, min(nbsum + 3, S.nmem)], dtype=np.int32)
+    nen, deltae, ecuts, niter = 31, 2.0, 0.02, 16
+    got = sess.calculate_sigma_lanczos(S.e1, S.nval, qp, nen, deltae, ecuts, niter, S.poly, nbands_sum=nbsum,
+                                       reorth=True)
+    for i, m in enumerate(qp):
+        args = (S.psi_intp, S.M, S.e1, S.nval, int(m), nen, deltae, ecuts, niter, S.poly)
+        ref = OS.sigma_c_state(*args, bands=np.arange(1, nbsum + 1), reorth=True)
+        full = OS.sigma_c_state(*args, reorth=True)
+        assert np.max(np.abs(ref)) > 1e-6
+        assert _rel(ref, full) > 1e-3          # the subset is a different sum
+        assert _rel(got[:, i], ref) < 1e-8
+    with ngw.Session(0, "mixed") as s:
+        s.set_isdf(S.psi_intp, S.M)
+        s.set_pairs(S.cvpair, S.sqrtR)
+        mixed = s.calculate_sigma_lanczos(S.e1, S.nval, qp, nen, deltae, ecuts, niter, S.poly, nbands_sum=nbsum,
+                                          reorth=True)
+    sigx = np.full(len(qp), -0.4)
+    vxc = np.full(len(qp), -0.6)
+    e64 = OS.qp_energies(got.T, S.e1, S.e1, qp, deltae, sigx, vxc, xacc_ev=1e-7)
+    emx = OS.qp_energies(mixed.T, S.e1, S.e1, qp, deltae, sigx, vxc, xacc_ev=1e-7)
+    err_mev = np.array([abs(a[0] - b[0]) * 1e3 for a, b in zip(emx, e64)])
+    assert np.all(err_mev < 1.0), err_mev
+
+
 def test_sigma_chain_blocking_is_invisible(sess, small_system):
     S = small_system
     qp = np.array([S.nval, S.nval + 1, S.nval + 2], dtype=np.int32)

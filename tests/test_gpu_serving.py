@@ -80,6 +80,8 @@ def test_grouped_small_requests_within_1mev(requests, mode, monkeypatch):
     NGW_BATCH_MODE=grouped; each QP energy within 1 meV of the same request
     served alone on its tuned tiles."""
     monkeypatch.setenv("NGW_BATCH_MODE", mode)
+    if mode == "grouped":
+        monkeypatch.setenv("NGW_DENSE", "0")    # the factored p(C) that grouped launches run
     alone = {}
     for r in requests:
         srv = SigmaServer(workers=1, precision="mixed")
