@@ -223,7 +223,7 @@ int ngw_profile_mixed_gemms(ngw_session *s, int nb, int reps, double *us_gemm1, 
 int ngw_mixed_gemm_shapes(ngw_session *s, int nb, int *shape);
 /* The mixed form's dense p(C) GEMM (built when the last mixed plan chose the
  * dense form, small N_cv): mean device time of one launch for nb chains to
- * *us and shape[5] = {M, N, K, N tile, variant}; NGW_ERR_STATE when the
+ * *us and shape[5] = {M, N, K, N tile, 16 x variant + split-K}; NGW_ERR_STATE when the
  * session's plan used the factored form.  No reference counterpart: used by
  * the benchmark. */
 int ngw_profile_dense_gemm(ngw_session *s, int nb, int reps, double *us, int *shape);

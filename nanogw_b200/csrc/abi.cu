@@ -342,8 +342,9 @@ static double poly_eval(const std::vector<double> &p, double x) {
 // lambda_{k+1}] (the reference's fit leaves that range), so the Clenshaw
 // recurrence only ever sees a spectrum on which p is bounded.
 // Dense or factored p(C) for a solve of `steps` products on nb chains: the
-// dense operator costs 2 p N_cv^3 FP64 multiply-adds to form (unless it is
-// already built for this polynomial) and 2 N_cv^2 split-BF16 ones per chain
+// dense operator costs about 2 sqrt(p) FP64 GEMMs of N_cv^3 multiply-adds to
+// form (Paterson-Stockmeyer; nothing when it is already built for this
+// polynomial) and 2 N_cv^2 split-BF16 ones per chain
 // and product; the factored form 4 p (N_mu + k) N_cv per chain and product in
 // 2 p launches.  Rates: the FP64 tensor-core GEMM ~25 TFLOP/s, the dense
 // split-BF16 GEMM ~0.9 PFLOP/s executed (x3 products), the factored pair
@@ -359,7 +360,9 @@ static bool want_dense(ngw_session *s, const PolyPlan &pp, int steps, int nb) {
   }
   if (steps < 1 || nb < 1) return false;
   const bool built = mixed_dense_ready(s, pp.cheb.data(), pp.npoly, pp.c0, pp.c1);
-  const double form = built ? 0.0 : 2.0 * p * N * N * N / 25e12;
+  const int m = std::max(2, (int)std::ceil(std::sqrt(p + 1.0)));
+  const double products = (m - 1) + pp.npoly / m;
+  const double form = built ? 0.0 : 2.0 * products * N * N * N / 25e12;
   const double dense_step = 3.0 * 2.0 * N * N * nb / 0.9e15 + 10e-6;
   const double fact_step = p * (3.0 * 4.0 * mu * N * nb / 0.6e15 + 10e-6);
   return form + steps * dense_step < steps * fact_step;

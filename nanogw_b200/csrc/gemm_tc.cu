@@ -25,6 +25,7 @@
 #include <cstring>
 #include <cstdio>
 #include <cstdlib>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -1205,6 +1206,12 @@ static int dispatch_tc(int BN, int var, const CUtensorMap &a_hi, const CUtensorM
       case 80: NGW_TCC(80, 4, 1);
       case 96: NGW_TCC(96, 3, 1);
       case 128: NGW_TCC(128, 3, 1);
+      // wide tiles for the dense p(C) GEMM (fewer re-reads of H and of the
+      // chain vectors; the split-K inside the cluster keeps every SM busy)
+      case 160: NGW_TCC(160, 3, 1);
+      case 192: NGW_TCC(192, 2, 1);
+      case 240: NGW_TCC(240, 2, 1);
+      case 256: NGW_TCC(256, 2, 1);
     }
   }
   if (var == 6) {
@@ -1368,7 +1375,7 @@ struct MixedOperator {
   size_t dense_bytes = 0;
   // dense GEMM tiles (N tile, variant), tuned per chain count; S_hi / S_lo
   // as its B operand with that N tile
-  int BNd = 128, vard = 3, tuned_nbd = -1, maps_bnd = -1;
+  int BNd = 128, vard = 3, splitd = 1, tuned_nbd = -1, maps_bnd = -1;
   CUtensorMap tVhi, tVlo;
 };
 
@@ -1435,7 +1442,7 @@ void extern_mixed_tune(ngw_session *s, int *tune) {
   tune[1] = op->split1;
   tune[2] = (op->BN2 * 16 + op->var2) * 16 + op->split2;
   tune[3] = op->nb_cap;
-  tune[4] = op->BNd * 16 + op->vard;
+  tune[4] = (op->BNd * 16 + op->vard) * 16 + op->splitd;
   tune[5] = op->dense_ok ? 1 : 0;
 }
 
@@ -2061,9 +2068,10 @@ int mixed_poly_apply(ngw_session *s, int nb, const double *v, int ldv, const dou
 //   H = P_perp p(Chat_perp),  Chat_perp = (P_perp C P_perp - c0) / c1,
 // P_perp = I - U U^T (the deflated Ritz vectors), is formed once per operator
 // and polynomial in FP64 (C = R^2 + 4 R^1/2 (C_isdf^T M C_isdf) R^1/2, the
-// deflation as rank-k updates, then the Clenshaw recurrence of the vector
-// form with matrices: B_n = g_n P, B_k = g_k P + 2 Chat B_{k+1} - B_{k+2},
-// H = g_0 P + Chat B_1 - B_2, one FP64 tensor-core GEMM per term), split into
+// deflation as rank-k updates, then the Chebyshev series of the vector form
+// in Paterson-Stockmeyer form: T_0..T_m of X = Chat P by the three-term
+// recurrence and a Horner scheme in T_m over the series' base-T_m digits,
+// about 2 sqrt(n) FP64 tensor-core GEMMs for degree n), split into
 // BF16 hi/lo rows, and every p(C) v of the Lanczos recurrence is then ONE
 // tcgen05 GEMM H v (split-BF16, FP32 accumulation) whose epilogue adds the
 // deflated eigenpairs' U p(Lambda) U^T v in FP64 -- the same quantity the
@@ -2081,26 +2089,31 @@ __global__ void k_dense_casida(double *__restrict__ K, const double *__restrict_
   }
 }
 
-// A = (A - c0 I) * f  in place
-__global__ void k_dense_shift(double *__restrict__ A, int n, double c0, double f) {
-  const size_t total = (size_t)n * n;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(e % n), j = (int)(e / n);
-    A[e] = (A[e] - (i == j ? c0 : 0.0)) * f;
-  }
-}
-
 __global__ void k_dense_identity(double *__restrict__ A, int n) {
   const size_t total = (size_t)n * n;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
     A[e] = ((int)(e % n) == (int)(e / n)) ? 1.0 : 0.0;
 }
 
-// out = g P - b2 (b2 nullable)
-__global__ void k_dense_comb(const double *__restrict__ P, const double *__restrict__ b2, double g, size_t total,
-                             double *__restrict__ out) {
+// out = sum_r c_r T_r (up to 16 terms), elementwise
+struct MatCombo {
+  const double *t[16];
+  double c[16];
+  int n;
+};
+__global__ void k_dense_combo(MatCombo mc, size_t total, double *__restrict__ out) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int r = 0; r < mc.n; ++r) acc = fma(mc.c[r], mc.t[r][e], acc);
+    out[e] = acc;
+  }
+}
+
+// X = (C_perp - c0 P) / c1 = Chat P (C_perp P = C_perp)
+__global__ void k_dense_x(const double *__restrict__ Cp, const double *__restrict__ P, double c0, double f,
+                          size_t total, double *__restrict__ X) {
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
-    out[e] = g * P[e] - (b2 ? b2[e] : 0.0);
+    X[e] = (Cp[e] - c0 * P[e]) * f;
 }
 
 // columns of X (ncv x nb, leading dimension ldx, FP64) -> rows [j][cv] of
@@ -2133,6 +2146,34 @@ bool mixed_dense_ready(ngw_session *s, const double *g, int n, double c0, double
   return true;
 }
 
+// Paterson-Stockmeyer digits of a Chebyshev series g[0..n] in base T_m:
+// p = d_0 + T_m (d_1 + T_m (... + T_m d_Q)), deg d_q < m, by repeated
+// division by T_m with T_i = 2 T_m T_{i-m} - T_{|2m-i|} (long double).
+static std::vector<std::vector<double>> cheb_digits(const double *g, int n, int m) {
+  std::vector<long double> cur(g, g + n + 1);
+  std::vector<std::vector<double>> d;
+  while ((int)cur.size() - 1 >= m) {
+    std::vector<long double> a = cur;
+    const int deg = (int)a.size() - 1;
+    std::vector<long double> q(deg - m + 1, 0.0L);
+    for (int i = deg; i >= m; --i) {
+      const long double c = a[i];
+      if (c == 0.0L) continue;
+      a[i] = 0.0L;
+      if (i == m) {
+        q[0] += c;
+      } else {
+        q[i - m] += 2.0L * c;
+        a[std::abs(2 * m - i)] -= c;
+      }
+    }
+    d.emplace_back(a.begin(), a.begin() + m);
+    cur = q;
+  }
+  d.emplace_back(cur.begin(), cur.end());
+  return d;
+}
+
 int mixed_dense_build(ngw_session *s, const double *g, int n, double c0, double c1) {
   MixedOperator *op = s->mixed;
   if (!op || op->tda || n < 1 || c1 == 0.0) {
@@ -2155,15 +2196,32 @@ int mixed_dense_build(ngw_session *s, const double *g, int n, double c0, double 
   op->dense_ok = false;
   cudaStream_t st = s->stream;
   const size_t nn = (size_t)N * N;
-  PoolTmp tC(s), tP(s), tB0(s), tB1(s), tB2(s), tD(s), tG(s);
-  NGW_CUDA(pool_alloc(s, &tC.p, nn * 8));
-  NGW_CUDA(pool_alloc(s, &tP.p, nn * 8));
-  NGW_CUDA(pool_alloc(s, &tB0.p, nn * 8));
-  NGW_CUDA(pool_alloc(s, &tB1.p, nn * 8));
-  NGW_CUDA(pool_alloc(s, &tB2.p, nn * 8));
-  NGW_CUDA(pool_alloc(s, &tD.p, (size_t)ni * N * 8));
-  double *Cm = static_cast<double *>(tC.p), *P = static_cast<double *>(tP.p), *D = static_cast<double *>(tD.p);
-  double *buf[3] = {static_cast<double *>(tB0.p), static_cast<double *>(tB1.p), static_cast<double *>(tB2.p)};
+  // Paterson-Stockmeyer in the Chebyshev basis: T_r P (r <= m) of X = Chat P
+  // by the three-term recurrence, then the Horner form in T_m over the
+  // digits -- (m - 1) + Q FP64 GEMMs instead of the n of the Clenshaw form
+  const int m = std::max(2, (int)std::ceil(std::sqrt((double)n + 1.0)));
+  const std::vector<std::vector<double>> dig = cheb_digits(g, n, m);
+  const int Q = (int)dig.size() - 1;
+  const int rmax = Q > 0 ? m : n;          // highest T_r needed
+  if (m > 16) {
+    set_error("dense p(C): polynomial degree %d too high for the dense form", n);
+    return NGW_ERR_ARG;
+  }
+  std::deque<PoolTmp> tm;   // element addresses stay fixed as it grows
+  auto mat = [&](size_t elems) -> double * {
+    tm.emplace_back(s);
+    if (pool_alloc(s, &tm.back().p, elems * 8) != cudaSuccess) return nullptr;
+    return static_cast<double *>(tm.back().p);
+  };
+  double *Cm = mat(nn), *D = mat((size_t)ni * N);
+  std::vector<double *> T(rmax + 1, nullptr);
+  for (int r = 0; r <= rmax; ++r) T[r] = mat(nn);
+  double *Y0 = mat(nn), *Y1 = mat(nn);
+  if (!Cm || !D || !Y0 || !Y1 || std::find(T.begin(), T.end(), nullptr) != T.end()) {
+    set_error("dense p(C): out of device memory for the FP64 formation (N_cv %d)", N);
+    return NGW_ERR_OOM;
+  }
+  double *P = T[0];
   // C = R^2 + 4 R^1/2 (C_isdf^T (M C_isdf)) R^1/2
   NGW_CUDA(dgemm(st, false, false, ni, N, ni, 1.0, s->d_M, ni, s->d_C, ni, 0.0, D, ni));
   NGW_CUDA(dgemm(st, true, false, N, N, ni, 1.0, s->d_C, ni, D, ni, 0.0, Cm, N));
@@ -2172,36 +2230,57 @@ int mixed_dense_build(ngw_session *s, const double *g, int n, double c0, double 
   NGW_CUDA(cudaGetLastError());
   if (k > 0) {
     // P C P = C - U G^T - Y U^T with G = C U, Y = G - U (U^T G); P = I - U U^T
-    NGW_CUDA(pool_alloc(s, &tG.p, ((size_t)2 * N * k + (size_t)k * k) * 8));
-    double *G = static_cast<double *>(tG.p), *Y = G + (size_t)N * k, *Wk = Y + (size_t)N * k;
+    double *G = mat(((size_t)2 * N * k + (size_t)k * k));
+    if (!G) {
+      set_error("dense p(C): out of device memory");
+      return NGW_ERR_OOM;
+    }
+    double *Yk = G + (size_t)N * k, *Wk = Yk + (size_t)N * k;
     const double *U = s->eig_U;
     NGW_CUDA(dgemm(st, false, false, N, k, N, 1.0, Cm, N, U, N, 0.0, G, N));
     NGW_CUDA(dgemm(st, true, false, k, k, N, 1.0, U, N, G, N, 0.0, Wk, k));
-    NGW_CUDA(cudaMemcpyAsync(Y, G, (size_t)N * k * 8, cudaMemcpyDeviceToDevice, st));
-    NGW_CUDA(dgemm(st, false, false, N, k, k, -1.0, U, N, Wk, k, 1.0, Y, N));
+    NGW_CUDA(cudaMemcpyAsync(Yk, G, (size_t)N * k * 8, cudaMemcpyDeviceToDevice, st));
+    NGW_CUDA(dgemm(st, false, false, N, k, k, -1.0, U, N, Wk, k, 1.0, Yk, N));
     NGW_CUDA(dgemm(st, false, true, N, N, k, -1.0, U, N, G, N, 1.0, Cm, N));
-    NGW_CUDA(dgemm(st, false, true, N, N, k, -1.0, Y, N, U, N, 1.0, Cm, N));
+    NGW_CUDA(dgemm(st, false, true, N, N, k, -1.0, Yk, N, U, N, 1.0, Cm, N));
     NGW_CUDA(dgemm(st, false, true, N, N, k, -1.0, U, N, U, N, 1.0, P, N));
   }
-  k_dense_shift<<<elem_blocks(nn), 256, 0, st>>>(Cm, N, c0, 1.0 / c1);
-  NGW_CUDA(cudaGetLastError());
-  // matrix Clenshaw, the buffer roles rotating as in mixed_poly_apply
-  int i1 = 0, i2 = -1;
-  k_dense_comb<<<elem_blocks(nn), 256, 0, st>>>(P, nullptr, g[n], nn, buf[0]);
-  for (int kk = n - 1; kk >= 0; --kk) {
-    const int io = (i2 < 0) ? 1 : 3 - i1 - i2;
-    k_dense_comb<<<elem_blocks(nn), 256, 0, st>>>(P, i2 < 0 ? nullptr : buf[i2], g[kk], nn, buf[io]);
+  if (rmax >= 1) k_dense_x<<<elem_blocks(nn), 256, 0, st>>>(Cm, P, c0, 1.0 / c1, nn, T[1]);
+  for (int r = 2; r <= rmax; ++r) {
+    // T_r = 2 X T_{r-1} - T_{r-2}
+    MatCombo mc{};
+    mc.t[0] = T[r - 2];
+    mc.c[0] = -1.0;
+    mc.n = 1;
+    k_dense_combo<<<elem_blocks(nn), 256, 0, st>>>(mc, nn, T[r]);
     NGW_CUDA(cudaGetLastError());
-    NGW_CUDA(dgemm(st, false, false, N, N, N, kk > 0 ? 2.0 : 1.0, Cm, N, buf[i1], N, 1.0, buf[io], N));
-    i2 = i1;
-    i1 = io;
+    NGW_CUDA(dgemm(st, false, false, N, N, N, 2.0, T[1], N, T[r - 1], N, 1.0, T[r], N));
   }
-  // H (buf[i1]) -> split BF16 rows H[m][k]; padding rows / columns zero
+  auto digit = [&](int q, double *out) -> int {
+    MatCombo mc{};
+    mc.n = (int)dig[q].size();
+    for (int r = 0; r < mc.n; ++r) {
+      mc.t[r] = T[r];
+      mc.c[r] = dig[q][r];
+    }
+    k_dense_combo<<<elem_blocks(nn), 256, 0, st>>>(mc, nn, out);
+    NGW_CUDA(cudaGetLastError());
+    return NGW_OK;
+  };
+  double *Yc = Y0, *Yn = Y1;
+  NGW_TRY(digit(Q, Yc));
+  for (int q = Q - 1; q >= 0; --q) {
+    NGW_TRY(digit(q, Yn));
+    NGW_CUDA(dgemm(st, false, false, N, N, N, 1.0, T[m], N, Yc, N, 1.0, Yn, N));
+    std::swap(Yc, Yn);
+  }
+  double *Hm = Yc;
+  // H -> split BF16 rows H[m][k]; padding rows / columns zero
   NGW_CUDA(cudaMemsetAsync(op->H_hi, 0, hbytes, st));
   NGW_CUDA(cudaMemsetAsync(op->H_lo, 0, hbytes, st));
   {
     dim3 grid((N + 31) / 32, (N + 31) / 32);
-    k_split_transpose<<<grid, dim3(32, 8), 0, st>>>(buf[i1], N, N, op->H_hi, op->H_lo, kpad);
+    k_split_transpose<<<grid, dim3(32, 8), 0, st>>>(Hm, N, N, op->H_hi, op->H_lo, kpad);
     NGW_CUDA(cudaGetLastError());
   }
   NGW_CUDA(cudaStreamSynchronize(st));
@@ -2229,7 +2308,7 @@ static int run_dense_gemm(ngw_session *s, int nb, double *out64, int ldv) {
   GemmArgs ga;
   ga.num_kb = op->kpad / BK;
   ga.nseg = 3;
-  ga.nsplit = 1;
+  ga.nsplit = op->vard == 5 ? op->splitd : 1;
   EpiParams ep;
   std::memset(&ep, 0, sizeof(ep));
   ep.kind = EPI_CLENSHAW;
@@ -2258,6 +2337,8 @@ int mixed_dense_apply(ngw_session *s, int nb, const double *v, int ldv, double *
     set_error("dense p(C): operator or chain buffers not prepared");
     return NGW_ERR_STATE;
   }
+  // xo = U^T v (FP64 tensor-core GEMM: U is re-read once per tile, not per
+  // chain) and the split B operand
   const int N = s->ncv, k = op->kdef;
   cudaStream_t st = s->stream;
   if (k > 0)
@@ -2280,7 +2361,7 @@ struct DenseKey {
   }
 };
 static std::mutex g_dtune_mu;
-static std::map<DenseKey, std::pair<int, int>> g_dtune;
+static std::map<DenseKey, TileC> g_dtune;
 
 int mixed_prepare_dense(ngw_session *s, int nb) {
   MixedOperator *op = s->mixed;
@@ -2291,10 +2372,11 @@ int mixed_prepare_dense(ngw_session *s, int nb) {
   }
   if (op->tuned_nbd == nb && op->maps_bnd == op->BNd) return NGW_OK;
   if (const char *env = getenv("NGW_DENSE_TILES")) {
-    int bn = 0, var = 0;
-    if (sscanf(env, "%d,%d", &bn, &var) == 2) {
+    int bn = 0, var = 0, sp = 1;
+    if (sscanf(env, "%d,%d,%d", &bn, &var, &sp) >= 2) {
       op->BNd = bn;
       op->vard = var;
+      op->splitd = var == 5 ? std::max(2, sp) : 1;
       op->tuned_nbd = nb;
       return encode_dense_maps(op, bn);
     }
@@ -2304,13 +2386,14 @@ int mixed_prepare_dense(ngw_session *s, int nb) {
     std::lock_guard<std::mutex> lk(g_dtune_mu);
     auto it = g_dtune.find(key);
     if (it != g_dtune.end()) {
-      op->BNd = it->second.first;
-      op->vard = it->second.second;
+      op->BNd = it->second.bn;
+      op->vard = it->second.var;
+      op->splitd = it->second.sp;
       op->tuned_nbd = nb;
       return encode_dense_maps(op, op->BNd);
     }
   }
-  std::vector<std::pair<int, int>> cand;
+  std::vector<TileC> cand;
   for (int bn : kBNs) {
     if (bn > round_up(nb, 16) && bn != kBNs[0]) continue;
     if ((round_up(nb, bn) - nb) * 8 > nb && bn != kBNs[0]) continue;
@@ -2319,7 +2402,13 @@ int mixed_prepare_dense(ngw_session *s, int nb) {
       if (var == 2 && !has_persistent(bn)) continue;
       if (var == 3 && !has_fused(bn)) continue;
       if (var == 4 && !has_fused2(bn)) continue;
-      cand.push_back({bn, var});
+      cand.push_back({bn, var, 1});
+    }
+    // cluster split-K (variant 5) with the wide tiles too
+    if (bn >= 64) {
+      const int tiles = (op->cv_pad / BM) * ((nb + bn - 1) / bn);
+      for (int sp : {2, 3, 4})
+        if (op->kpad / BK / sp >= 4 && tiles * sp <= 2 * 148) cand.push_back({bn, 5, sp});
     }
   }
   PoolTmp tout(s);
@@ -2331,13 +2420,14 @@ int mixed_prepare_dense(ngw_session *s, int nb) {
   NGW_CUDA(cudaEventCreate(&e0));
   NGW_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
-  std::pair<int, int> pick = cand.empty() ? std::make_pair(128, 3) : cand[0];
+  TileC pick = cand.empty() ? TileC{128, 3, 1} : cand[0];
   const bool verbose = getenv("NGW_TUNE_VERBOSE") != nullptr;
   int rc = NGW_OK;
   for (const auto &c : cand) {
-    op->BNd = c.first;
-    op->vard = c.second;
-    if ((rc = encode_dense_maps(op, c.first)) != NGW_OK) break;
+    op->BNd = c.bn;
+    op->vard = c.var;
+    op->splitd = c.sp;
+    if ((rc = encode_dense_maps(op, c.bn)) != NGW_OK) break;
     if ((rc = run_dense_gemm(s, nb, out, s->ncv)) != NGW_OK) break;
     float ms = 0.f;
     cudaEventRecord(e0, s->stream);
@@ -2348,7 +2438,7 @@ int mixed_prepare_dense(ngw_session *s, int nb) {
       rc = NGW_ERR_CUDA;
     }
     if (rc != NGW_OK) break;
-    if (verbose) fprintf(stderr, "tune dense bn=%d var=%d: %.2f us\n", c.first, c.second, 1e3f * ms / 3);
+    if (verbose) fprintf(stderr, "tune dense bn=%d var=%d split=%d: %.2f us\n", c.bn, c.var, c.sp, 1e3f * ms / 3);
     if (ms < best) {
       best = ms;
       pick = c;
@@ -2357,8 +2447,9 @@ int mixed_prepare_dense(ngw_session *s, int nb) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   NGW_TRY(rc);
-  op->BNd = pick.first;
-  op->vard = pick.second;
+  op->BNd = pick.bn;
+  op->vard = pick.var;
+  op->splitd = pick.sp;
   op->tuned_nbd = nb;
   NGW_TRY(encode_dense_maps(op, op->BNd));
   {
@@ -2626,7 +2717,7 @@ extern "C" int ngw_profile_dense_gemm(ngw_session *s, int nb, int reps, double *
   shape[1] = nb;
   shape[2] = s->ncv;
   shape[3] = op->BNd;
-  shape[4] = op->vard;
+  shape[4] = op->vard * 16 + op->splitd;
   return check_status(s);
 }
 
