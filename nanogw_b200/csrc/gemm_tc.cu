@@ -1376,6 +1376,12 @@ struct MixedOperator {
   // dense GEMM tiles (N tile, variant), tuned per chain count; S_hi / S_lo
   // as its B operand with that N tile
   int BNd = 128, vard = 3, splitd = 1, tuned_nbd = -1, maps_bnd = -1;
+  // k_dense_prep's chunk partials and per-group counters (zeroed once; the
+  // last CTA of a group resets its counter), sized for dws_nb chains
+  double *dws = nullptr;
+  unsigned *dcnt = nullptr;
+  int dws_nb = 0;
+  size_t dws_bytes = 0;
   CUtensorMap tVhi, tVlo;
 };
 
@@ -1414,9 +1420,14 @@ static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
 static void free_dense(ngw_session *s, MixedOperator *op) {
   pool_free(s, op->H_hi);
   pool_free(s, op->H_lo);
+  pool_free(s, op->dws);
   op->H_hi = op->H_lo = nullptr;
-  s->bytes -= op->dense_bytes;
+  op->dws = nullptr;
+  op->dcnt = nullptr;
+  op->dws_nb = 0;
+  s->bytes -= op->dense_bytes + op->dws_bytes;
   op->dense_bytes = 0;
+  op->dws_bytes = 0;
   op->dense_ok = false;
 }
 
@@ -2116,17 +2127,99 @@ __global__ void k_dense_x(const double *__restrict__ Cp, const double *__restric
     X[e] = (Cp[e] - c0 * P[e]) * f;
 }
 
-// columns of X (ncv x nb, leading dimension ldx, FP64) -> rows [j][cv] of
-// the split-BF16 pair (row length lds)
-__global__ void k_split_cols(const double *__restrict__ X, int ldx, int ncv, int nb, bf16 *__restrict__ hi,
-                             bf16 *__restrict__ lo, int lds) {
-  for (int j = blockIdx.y; j < nb; j += gridDim.y)
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x) {
-      const double x = X[(size_t)j * ldx + i];
-      const bf16 h = __double2bfloat16(x);
-      hi[(size_t)j * lds + i] = h;
-      lo[(size_t)j * lds + i] = __double2bfloat16(x - (double)__bfloat162float(h));
+// The split-BF16 rows [j][cv] of the chain vectors and xo(:, j) = U^T v_j in
+// FP64, one launch: CTA (c, g) takes elements [c*DP_IC, (c+1)*DP_IC) of the
+// DP_TJ chains of group g (two elements per thread), writes their split and
+// its partial sums of U^T v (warp shuffles, then the eight warps in order)
+// to ws[(j*k + q)*C + c]; the last CTA of the group to finish (counter in
+// cnt[g], reset by it) sums the C partials in order into xo.  Deterministic;
+// U is read once per chunk and group.  256 threads.
+constexpr int DP_TJ = 4, DP_IC = 512;
+__global__ void __launch_bounds__(256) k_dense_prep(const double *__restrict__ V, int ldv, int ncv, int nb,
+                                                    const double *__restrict__ U, int k, bf16 *__restrict__ hi,
+                                                    bf16 *__restrict__ lo, int lds, double *__restrict__ ws,
+                                                    unsigned *__restrict__ cnt, double *__restrict__ xo) {
+  __shared__ double red[8][8 * DP_TJ];
+  __shared__ bool last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int c = blockIdx.x, C = gridDim.x, g = blockIdx.y;
+  const int j0 = g * DP_TJ, nj = min(DP_TJ, nb - j0);
+  double x[2][DP_TJ];
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const int i = c * DP_IC + e * 256 + tid;
+#pragma unroll
+    for (int jj = 0; jj < DP_TJ; ++jj) {
+      x[e][jj] = 0.0;
+      if (i < ncv && jj < nj) {
+        const double v = V[(size_t)(j0 + jj) * ldv + i];
+        x[e][jj] = v;
+        const bf16 h = __double2bfloat16(v);
+        hi[(size_t)(j0 + jj) * lds + i] = h;
+        lo[(size_t)(j0 + jj) * lds + i] = __double2bfloat16(v - (double)__bfloat162float(h));
+      }
     }
+  }
+  if (k == 0) return;
+  for (int q0 = 0; q0 < k; q0 += 8) {
+    const int nq = min(8, k - q0);
+    double acc[8][DP_TJ];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+#pragma unroll
+      for (int jj = 0; jj < DP_TJ; ++jj) acc[q][jj] = 0.0;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int i = c * DP_IC + e * 256 + tid;
+      if (i >= ncv) continue;
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (q < nq) {
+          const double u = U[(size_t)(q0 + q) * ncv + i];
+#pragma unroll
+          for (int jj = 0; jj < DP_TJ; ++jj) acc[q][jj] = fma(u, x[e][jj], acc[q][jj]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+#pragma unroll
+      for (int jj = 0; jj < DP_TJ; ++jj) {
+        double v = acc[q][jj];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[q][jj] = v;
+      }
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int jj = 0; jj < DP_TJ; ++jj) red[warp][q * DP_TJ + jj] = acc[q][jj];
+    __syncthreads();
+    if (tid < 8 * DP_TJ) {
+      const int q = tid / DP_TJ, jj = tid % DP_TJ;
+      if (q < nq && jj < nj) {
+        double sum = 0.0;
+        for (int w = 0; w < 8; ++w) sum += red[w][tid];
+        ws[((size_t)(j0 + jj) * k + q0 + q) * C + c] = sum;
+      }
+    }
+    __syncthreads();
+  }
+  // the last CTA of the group sums the chunks' partials in chunk order
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = atomicAdd(&cnt[g], 1u) == (unsigned)(C - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int t = tid; t < nj * k; t += 256) {
+    const int jj = t / k, q = t % k;
+    const double *p = ws + ((size_t)(j0 + jj) * k + q) * C;
+    double sum = 0.0;
+    for (int cc = 0; cc < C; ++cc) sum += __ldcg(p + cc);
+    xo[(size_t)(j0 + jj) * k + q] = sum;
+  }
+  if (tid == 0) cnt[g] = 0u;
 }
 
 static unsigned elem_blocks(size_t total) {
@@ -2333,19 +2426,14 @@ static int run_dense_gemm(ngw_session *s, int nb, double *out64, int ldv) {
 // out64 = p(C) v through the dense operator.  Launch-only.
 int mixed_dense_apply(ngw_session *s, int nb, const double *v, int ldv, double *out64) {
   MixedOperator *op = s->mixed;
-  if (!op || !op->dense_ok || op->nb_cap < nb || op->maps_bnd != op->BNd) {
+  if (!op || !op->dense_ok || op->nb_cap < nb || op->maps_bnd != op->BNd || op->dws_nb < nb) {
     set_error("dense p(C): operator or chain buffers not prepared");
     return NGW_ERR_STATE;
   }
-  // xo = U^T v (FP64 tensor-core GEMM: U is re-read once per tile, not per
-  // chain) and the split B operand
-  const int N = s->ncv, k = op->kdef;
-  cudaStream_t st = s->stream;
-  if (k > 0)
-    NGW_CUDA(dgemm(st, true, false, k, nb, N, 1.0, s->eig_U, N, v, ldv, 0.0, op->xo, k,
-                   reinterpret_cast<double *>(op->ws), op->ws_bytes));
-  k_split_cols<<<dim3(std::min(16, (N + 255) / 256), ygrid(nb)), 256, 0, st>>>(v, ldv, N, nb, op->S_hi, op->S_lo,
-                                                                           op->cv_pad);
+  // the split B operand and xo = U^T v (FP64) in one launch
+  const dim3 grid((s->ncv + DP_IC - 1) / DP_IC, (nb + DP_TJ - 1) / DP_TJ);
+  k_dense_prep<<<grid, 256, 0, s->stream>>>(v, ldv, s->ncv, nb, s->eig_U, op->kdef, op->S_hi, op->S_lo, op->cv_pad,
+                                           op->dws, op->dcnt, op->xo);
   NGW_CUDA(cudaGetLastError());
   return run_dense_gemm(s, nb, out64, ldv);
 }
@@ -2369,6 +2457,21 @@ int mixed_prepare_dense(ngw_session *s, int nb) {
   if (op->nb_cap < nb) {
     set_error("dense p(C): chain buffers not prepared");
     return NGW_ERR_STATE;
+  }
+  if (op->dws_nb < op->nb_cap) {
+    // chunk partials (nb_cap x k x chunks) and one counter per chain group
+    bump_generation(s);
+    pool_free(s, op->dws);
+    s->bytes -= op->dws_bytes;
+    const size_t chunks = (size_t)(s->ncv + DP_IC - 1) / DP_IC;
+    const size_t groups = (size_t)(op->nb_cap + DP_TJ - 1) / DP_TJ;
+    const size_t wb = (size_t)op->nb_cap * std::max(op->kdef, 1) * chunks * 8;
+    op->dws_bytes = wb + groups * sizeof(unsigned);
+    NGW_CUDA(pool_alloc(s, (void **)&op->dws, op->dws_bytes));
+    op->dcnt = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(op->dws) + wb);
+    NGW_CUDA(cudaMemsetAsync(op->dcnt, 0, groups * sizeof(unsigned), s->stream));
+    s->bytes += op->dws_bytes;
+    op->dws_nb = op->nb_cap;
   }
   if (op->tuned_nbd == nb && op->maps_bnd == op->BNd) return NGW_OK;
   if (const char *env = getenv("NGW_DENSE_TILES")) {

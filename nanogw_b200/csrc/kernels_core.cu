@@ -417,16 +417,17 @@ void launch_lanczos_step(double *w, double *v, const double *t, int ncv, int nb,
                          double *b, int niter, const double *s, double *hs, int tamm_d,
                          int prescale_next, int *clen, double eps, cudaStream_t st) {
   if (nb <= 0) return;
-  // The register form pays off from ncv > 4096 (at ncv = 2700 its 128
-  // registers per thread cost more occupancy than its single pass saves).
-  // NGW_LSTEP=3 keeps the three-pass form at every size, NGW_LSTEP=r takes the
-  // register form at every size it covers (comparison runs; both forms give
-  // identical results).
+  // The register form reads t, w, v once and writes w, v once; measured
+  // (warm launch list, 720 chains): 15.8 us against 21.9 us for the three
+  // passes at ncv = 2700, 81 against 98 us at ncv = 5776.  Below ncv = 1024
+  // the three-pass form.  NGW_LSTEP=3 keeps the three-pass form at every
+  // size, NGW_LSTEP=r takes the register form at every size it covers
+  // (comparison runs; both forms give identical results).
   static const int mode = [] {
     const char *e = getenv("NGW_LSTEP");
     return (e && e[0] == '3') ? 3 : ((e && e[0] == 'r') ? 1 : 0);
   }();
-  const bool three_pass = mode == 3 || (mode == 0 && ncv <= 16 * LNT);
+  const bool three_pass = mode == 3 || (mode == 0 && ncv <= 4 * LNT);
 #define NGW_LSR(E)                                                                                       \
   k_lanczos_step_reg<E><<<nb, LNT, 0, st>>>(w, v, t, ncv, k, a, b, niter, s, hs, tamm_d, prescale_next, \
                                             clen, eps)
