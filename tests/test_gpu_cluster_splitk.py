@@ -32,7 +32,7 @@ np.save({out!r}, sig)
 
 def _run(tmp_path, tiles, **extra_env):
     out = str(tmp_path / ("sig_" + tiles.replace(",", "_") + "_".join(extra_env) + ".npy"))
-    env = dict(os.environ, NGW_TILES=tiles, **extra_env)
+    env = dict(os.environ, NGW_TILES=tiles, NGW_DENSE="0", **extra_env)   # the factored p(C) these tiles run
     subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT, out=out)], env=env, check=True,
                    timeout=600)
     return np.load(out)
@@ -70,7 +70,7 @@ np.save({out!r}, np.array([abs(a[0] - b[0]) * 1e3 for a, b in zip(eg, er)] + [sh
 
 def _qp(tmp_path, tiles):
     out = str(tmp_path / ("qp_" + tiles.replace(",", "_") + ".npy"))
-    env = dict(os.environ, NGW_TILES=tiles)
+    env = dict(os.environ, NGW_TILES=tiles, NGW_DENSE="0")
     subprocess.run([sys.executable, "-c", QP_SCRIPT.format(root=ROOT, out=out)], env=env, check=True,
                    timeout=600)
     return np.load(out)

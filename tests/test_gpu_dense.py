@@ -96,3 +96,37 @@ def test_dense_plain_recurrence_qp(small_system, env):
     err = np.array([abs(a[0] - b[0]) * 1e3 for a, b in zip(e_got, e_ref)])
     print("dense plain recurrence QP error (meV):", err)
     assert np.all(err < 1.0)
+
+
+DENSE_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, {root!r})
+import nanogw_b200 as ngw
+from tests._system import make_small_system
+S = make_small_system()
+with ngw.Session(0, "mixed") as s:
+    s.set_isdf(S.psi_intp, S.M)
+    s.set_pairs(S.cvpair, S.sqrtR)
+    qp = np.array([S.nval - 1, S.nval, S.nval + 1, S.nval + 2], dtype=np.int32)
+    sig = s.calculate_sigma_lanczos(S.e1, S.nval, qp, 41, 3.0, 0.02, 20, S.poly)
+    shape = s.profile_dense_gemm(len(qp) * S.nmem, reps=2)[1]
+np.save({out!r}, np.concatenate([sig.ravel().view(np.float64), np.array(shape, dtype=np.float64)]))
+"""
+
+
+def test_dense_occupancy_forms_bit_identical(tmp_path):
+    """The dense GEMM fused at one and at two CTAs per SM (NGW_DENSE_TILES
+    64,3 and 64,4) runs the same MMAs and epilogue: identical Sigma_c."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for tiles in ("64,3", "64,4"):
+        f = str(tmp_path / ("dense_" + tiles.replace(",", "_") + ".npy"))
+        env = dict(os.environ, NGW_DENSE="1", NGW_DENSE_TILES=tiles)
+        subprocess.run([sys.executable, "-c", DENSE_SCRIPT.format(root=root, out=f)], env=env, check=True,
+                       timeout=600)
+        out[tiles] = np.load(f)
+    assert out["64,3"][-2] == 64 and out["64,4"][-2] == 64
+    assert out["64,3"][-1] == 3 * 16 + 1 and out["64,4"][-1] == 4 * 16 + 1
+    assert np.array_equal(out["64,3"][:-5], out["64,4"][:-5])

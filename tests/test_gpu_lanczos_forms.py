@@ -33,7 +33,7 @@ np.save({out!r}, np.concatenate(out))
 
 def _run(tmp_path, name, **env_extra):
     out = str(tmp_path / (name + ".npy"))
-    env = dict(os.environ, NGW_TILES="64,3,2,64,4", **env_extra)   # same GEMM tiles in both runs
+    env = dict(os.environ, NGW_TILES="64,3,2,64,4", NGW_DENSE="0", **env_extra)   # same GEMM tiles in both runs
     subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT, out=out)], env=env, check=True,
                    timeout=600)
     return np.load(out)
@@ -81,7 +81,7 @@ def test_register_forms_of_production_sizes(tmp_path, nocc, nemp):
     res = []
     for mode in ("r", "3"):
         out = str(tmp_path / f"{mode}.npy")
-        env = dict(os.environ, NGW_TILES="64,3,2,64,4", NGW_LSTEP=mode)
+        env = dict(os.environ, NGW_TILES="64,3,2,64,4", NGW_DENSE="0", NGW_LSTEP=mode)
         code = SCRIPT_RANDOM.format(root=ROOT, out=out, nocc=nocc, nemp=nemp, n_isdf=200)
         subprocess.run([sys.executable, "-c", code], env=env, check=True, timeout=600)
         res.append(np.load(out))

@@ -38,7 +38,7 @@ np.save({out!r}, np.array([e[0] for e in eq]))
 
 def _run(tmp_path, name, **extra):
     out = str(tmp_path / (name + ".npy"))
-    env = dict(os.environ, NGW_TUNE_VERBOSE="1", **extra)
+    env = dict(os.environ, NGW_TUNE_VERBOSE="1", NGW_DENSE="0", **extra)   # the factored GEMMs' tuner
     env.pop("NGW_TILES", None)
     r = subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT, out=out)], env=env, check=True,
                        timeout=600, capture_output=True, text=True)
