@@ -1376,12 +1376,9 @@ struct MixedOperator {
   // dense GEMM tiles (N tile, variant), tuned per chain count; S_hi / S_lo
   // as its B operand with that N tile
   int BNd = 128, vard = 3, splitd = 1, tuned_nbd = -1, maps_bnd = -1;
-  // k_dense_prep's chunk partials and per-group counters (zeroed once; the
-  // last CTA of a group resets its counter), sized for dws_nb chains
-  double *dws = nullptr;
-  unsigned *dcnt = nullptr;
-  int dws_nb = 0;
-  size_t dws_bytes = 0;
+  // side stream of the dense step: xo = U^T v runs beside the split
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   CUtensorMap tVhi, tVlo;
 };
 
@@ -1420,14 +1417,9 @@ static void free_chain_buffers(ngw_session *s, MixedOperator *op) {
 static void free_dense(ngw_session *s, MixedOperator *op) {
   pool_free(s, op->H_hi);
   pool_free(s, op->H_lo);
-  pool_free(s, op->dws);
   op->H_hi = op->H_lo = nullptr;
-  op->dws = nullptr;
-  op->dcnt = nullptr;
-  op->dws_nb = 0;
-  s->bytes -= op->dense_bytes + op->dws_bytes;
+  s->bytes -= op->dense_bytes;
   op->dense_bytes = 0;
-  op->dws_bytes = 0;
   op->dense_ok = false;
 }
 
@@ -1436,6 +1428,9 @@ void mixed_free(ngw_session *s) {
   if (!op) return;
   free_chain_buffers(s, op);
   free_dense(s, op);
+  if (op->ev_fork) cudaEventDestroy(op->ev_fork);
+  if (op->ev_join) cudaEventDestroy(op->ev_join);
+  if (op->aux) cudaStreamDestroy(op->aux);
   void *ptrs[] = {op->A1_hi, op->A1_lo, op->A3_hi, op->A3_lo, op->Up};
   for (void *p : ptrs)
     pool_free(s, p);
@@ -2127,99 +2122,75 @@ __global__ void k_dense_x(const double *__restrict__ Cp, const double *__restric
     X[e] = (Cp[e] - c0 * P[e]) * f;
 }
 
-// The split-BF16 rows [j][cv] of the chain vectors and xo(:, j) = U^T v_j in
-// FP64, one launch: CTA (c, g) takes elements [c*DP_IC, (c+1)*DP_IC) of the
-// DP_TJ chains of group g (two elements per thread), writes their split and
-// its partial sums of U^T v (warp shuffles, then the eight warps in order)
-// to ws[(j*k + q)*C + c]; the last CTA of the group to finish (counter in
-// cnt[g], reset by it) sums the C partials in order into xo.  Deterministic;
-// U is read once per chunk and group.  256 threads.
-constexpr int DP_TJ = 4, DP_IC = 512;
-__global__ void __launch_bounds__(256) k_dense_prep(const double *__restrict__ V, int ldv, int ncv, int nb,
-                                                    const double *__restrict__ U, int k, bf16 *__restrict__ hi,
-                                                    bf16 *__restrict__ lo, int lds, double *__restrict__ ws,
-                                                    unsigned *__restrict__ cnt, double *__restrict__ xo) {
-  __shared__ double red[8][8 * DP_TJ];
-  __shared__ bool last;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int c = blockIdx.x, C = gridDim.x, g = blockIdx.y;
-  const int j0 = g * DP_TJ, nj = min(DP_TJ, nb - j0);
-  double x[2][DP_TJ];
-#pragma unroll
-  for (int e = 0; e < 2; ++e) {
-    const int i = c * DP_IC + e * 256 + tid;
-#pragma unroll
-    for (int jj = 0; jj < DP_TJ; ++jj) {
-      x[e][jj] = 0.0;
-      if (i < ncv && jj < nj) {
-        const double v = V[(size_t)(j0 + jj) * ldv + i];
-        x[e][jj] = v;
-        const bf16 h = __double2bfloat16(v);
-        hi[(size_t)(j0 + jj) * lds + i] = h;
-        lo[(size_t)(j0 + jj) * lds + i] = __double2bfloat16(v - (double)__bfloat162float(h));
-      }
-    }
-  }
-  if (k == 0) return;
+// xo(:, j) = U^T v_j in FP64 on the FP64 tensor cores: a CTA takes eight
+// chains, each of its DP_W warps a K slice of ncv and runs mma.sync m8n8k4
+// f64 over it per eight eigenpairs (A = U^T: q x k, B = v: k x chain; lane
+// (g, t) = (lane / 4, lane % 4) holds A[g][t], B[t][g] and C[g][2t],
+// C[g][2t+1]); the warps' 8 x 8 tiles are summed in warp order
+// (deterministic).  U is read once per eight chains.
+constexpr int DP_W = 32;
+__device__ __forceinline__ void dmma_f64(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+__global__ void __launch_bounds__(DP_W * 32) k_dense_xo(const double *__restrict__ V, int ldv, int ncv, int nb,
+                                                       const double *__restrict__ U, int k,
+                                                       double *__restrict__ xo) {
+  __shared__ double red[DP_W][64];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, grp = lane >> 2, tig = lane & 3;
+  const int j0 = blockIdx.x * 8;
+  const int nj = min(8, nb - j0);
+  const int kc = (((ncv + DP_W - 1) / DP_W) + 3) & ~3;
+  const int kb = w * kc, ke = min(ncv, kb + kc);
+  const bool jv = grp < nj;
+  const double *vj = V + (size_t)(j0 + (jv ? grp : 0)) * ldv;
   for (int q0 = 0; q0 < k; q0 += 8) {
-    const int nq = min(8, k - q0);
-    double acc[8][DP_TJ];
+    const bool qv = q0 + grp < k;
+    const double *uq = U + (size_t)(qv ? q0 + grp : 0) * ncv;
+    double c0 = 0.0, c1 = 0.0;
+    for (int kbase = kb; kbase < ke; kbase += 32) {
+      double bv[8], av[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
+      for (int u = 0; u < 8; ++u) {
+        const int kx = kbase + 4 * u + tig;
+        const bool in = kx < ke;
+        bv[u] = (jv && in) ? vj[kx] : 0.0;
+        av[u] = (qv && in) ? uq[kx] : 0.0;
+      }
 #pragma unroll
-      for (int jj = 0; jj < DP_TJ; ++jj) acc[q][jj] = 0.0;
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int i = c * DP_IC + e * 256 + tid;
-      if (i >= ncv) continue;
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-        if (q < nq) {
-          const double u = U[(size_t)(q0 + q) * ncv + i];
-#pragma unroll
-          for (int jj = 0; jj < DP_TJ; ++jj) acc[q][jj] = fma(u, x[e][jj], acc[q][jj]);
-        }
+      for (int u = 0; u < 8; ++u) dmma_f64(c0, c1, av[u], bv[u]);
     }
-#pragma unroll
-    for (int q = 0; q < 8; ++q)
-#pragma unroll
-      for (int jj = 0; jj < DP_TJ; ++jj) {
-        double v = acc[q][jj];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        acc[q][jj] = v;
-      }
-    if (lane == 0)
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-#pragma unroll
-        for (int jj = 0; jj < DP_TJ; ++jj) red[warp][q * DP_TJ + jj] = acc[q][jj];
+    red[w][grp * 8 + 2 * tig] = c0;
+    red[w][grp * 8 + 2 * tig + 1] = c1;
     __syncthreads();
-    if (tid < 8 * DP_TJ) {
-      const int q = tid / DP_TJ, jj = tid % DP_TJ;
-      if (q < nq && jj < nj) {
-        double sum = 0.0;
-        for (int w = 0; w < 8; ++w) sum += red[w][tid];
-        ws[((size_t)(j0 + jj) * k + q0 + q) * C + c] = sum;
-      }
+    if (tid < 64) {
+      const int q = tid >> 3, n = tid & 7;
+      double sum = 0.0;
+      for (int ww = 0; ww < DP_W; ++ww) sum += red[ww][tid];
+      if (q0 + q < k && n < nj) xo[(size_t)(j0 + n) * k + q0 + q] = sum;
     }
     __syncthreads();
   }
-  // the last CTA of the group sums the chunks' partials in chunk order
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) last = atomicAdd(&cnt[g], 1u) == (unsigned)(C - 1);
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  for (int t = tid; t < nj * k; t += 256) {
-    const int jj = t / k, q = t % k;
-    const double *p = ws + ((size_t)(j0 + jj) * k + q) * C;
-    double sum = 0.0;
-    for (int cc = 0; cc < C; ++cc) sum += __ldcg(p + cc);
-    xo[(size_t)(j0 + jj) * k + q] = sum;
-  }
-  if (tid == 0) cnt[g] = 0u;
+}
+
+// the split-BF16 rows [j][cv] of the chain vectors: four consecutive
+// elements per thread (hi through FP32, lo the FP64 remainder)
+__global__ void k_split_chains(const double *__restrict__ V, int ldv, int ncv, int nb, bf16 *__restrict__ hi,
+                               bf16 *__restrict__ lo, int lds) {
+  const int j = blockIdx.y;
+  const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (j >= nb || i0 >= ncv) return;
+  double x[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) x[u] = i0 + u < ncv ? V[(size_t)j * ldv + i0 + u] : 0.0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+    if (i0 + u < ncv) {
+      const bf16 h = __float2bfloat16_rn((float)x[u]);
+      hi[(size_t)j * lds + i0 + u] = h;
+      lo[(size_t)j * lds + i0 + u] = __float2bfloat16_rn((float)(x[u] - (double)__bfloat162float(h)));
+    }
 }
 
 static unsigned elem_blocks(size_t total) {
@@ -2274,6 +2245,11 @@ int mixed_dense_build(ngw_session *s, const double *g, int n, double c0, double 
     return NGW_ERR_STATE;
   }
   if (mixed_dense_ready(s, g, n, c0, c1)) return NGW_OK;
+  if (!op->aux) {
+    NGW_CUDA(cudaStreamCreateWithFlags(&op->aux, cudaStreamNonBlocking));
+    NGW_CUDA(cudaEventCreateWithFlags(&op->ev_fork, cudaEventDisableTiming));
+    NGW_CUDA(cudaEventCreateWithFlags(&op->ev_join, cudaEventDisableTiming));
+  }
   const int N = s->ncv, ni = s->n_isdf, k = op->kdef;
   const int kpad = round_up(N, BK);
   const size_t hbytes = (size_t)op->cv_pad * kpad * sizeof(bf16);
@@ -2426,14 +2402,22 @@ static int run_dense_gemm(ngw_session *s, int nb, double *out64, int ldv) {
 // out64 = p(C) v through the dense operator.  Launch-only.
 int mixed_dense_apply(ngw_session *s, int nb, const double *v, int ldv, double *out64) {
   MixedOperator *op = s->mixed;
-  if (!op || !op->dense_ok || op->nb_cap < nb || op->maps_bnd != op->BNd || op->dws_nb < nb) {
+  if (!op || !op->dense_ok || op->nb_cap < nb || op->maps_bnd != op->BNd || !op->aux) {
     set_error("dense p(C): operator or chain buffers not prepared");
     return NGW_ERR_STATE;
   }
-  // the split B operand and xo = U^T v (FP64) in one launch
-  const dim3 grid((s->ncv + DP_IC - 1) / DP_IC, (nb + DP_TJ - 1) / DP_TJ);
-  k_dense_prep<<<grid, 256, 0, s->stream>>>(v, ldv, s->ncv, nb, s->eig_U, op->kdef, op->S_hi, op->S_lo, op->cv_pad,
-                                           op->dws, op->dcnt, op->xo);
+  // xo = U^T v (FP64 tensor cores) on the side stream beside the split B
+  // operand on the session stream (two branches of a captured graph)
+  cudaStream_t st = s->stream;
+  if (op->kdef > 0) {
+    NGW_CUDA(cudaEventRecord(op->ev_fork, st));
+    NGW_CUDA(cudaStreamWaitEvent(op->aux, op->ev_fork, 0));
+    k_dense_xo<<<(nb + 7) / 8, DP_W * 32, 0, op->aux>>>(v, ldv, s->ncv, nb, s->eig_U, op->kdef, op->xo);
+    NGW_CUDA(cudaEventRecord(op->ev_join, op->aux));
+  }
+  k_split_chains<<<dim3((s->ncv + 1023) / 1024, nb), 256, 0, st>>>(v, ldv, s->ncv, nb, op->S_hi, op->S_lo,
+                                                                  op->cv_pad);
+  if (op->kdef > 0) NGW_CUDA(cudaStreamWaitEvent(st, op->ev_join, 0));
   NGW_CUDA(cudaGetLastError());
   return run_dense_gemm(s, nb, out64, ldv);
 }
@@ -2458,21 +2442,7 @@ int mixed_prepare_dense(ngw_session *s, int nb) {
     set_error("dense p(C): chain buffers not prepared");
     return NGW_ERR_STATE;
   }
-  if (op->dws_nb < op->nb_cap) {
-    // chunk partials (nb_cap x k x chunks) and one counter per chain group
-    bump_generation(s);
-    pool_free(s, op->dws);
-    s->bytes -= op->dws_bytes;
-    const size_t chunks = (size_t)(s->ncv + DP_IC - 1) / DP_IC;
-    const size_t groups = (size_t)(op->nb_cap + DP_TJ - 1) / DP_TJ;
-    const size_t wb = (size_t)op->nb_cap * std::max(op->kdef, 1) * chunks * 8;
-    op->dws_bytes = wb + groups * sizeof(unsigned);
-    NGW_CUDA(pool_alloc(s, (void **)&op->dws, op->dws_bytes));
-    op->dcnt = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(op->dws) + wb);
-    NGW_CUDA(cudaMemsetAsync(op->dcnt, 0, groups * sizeof(unsigned), s->stream));
-    s->bytes += op->dws_bytes;
-    op->dws_nb = op->nb_cap;
-  }
+
   if (op->tuned_nbd == nb && op->maps_bnd == op->BNd) return NGW_OK;
   if (const char *env = getenv("NGW_DENSE_TILES")) {
     int bn = 0, var = 0, sp = 1;
