@@ -1314,6 +1314,21 @@ __global__ void k_split_rows(const double *__restrict__ D, int n_isdf, int ncv,
     }
 }
 
+// Up(:, j) = U(:, j) * p(lambda_j) for the deflated Ritz vectors (ncv x k,
+// column-major); the mixed plan deflates at most kMaxDeflation pairs (it
+// asks the eigen-solver for 64).
+constexpr int kMaxDeflation = 64;
+struct DeflationValues {
+  double v[kMaxDeflation];
+};
+__global__ void k_scale_cols(const double *__restrict__ U, int ncv, DeflationValues pv,
+                             double *__restrict__ Up) {
+  const int j = blockIdx.y;
+  const double f = pv.v[j];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncv; i += gridDim.x * blockDim.x)
+    Up[(size_t)j * ncv + i] = U[(size_t)j * ncv + i] * f;
+}
+
 // Clenshaw start: v_perp = v - U xo (deflated part, stored FP32), b_n = g v_perp
 // (FP32) and split((R^1/2 or 1) * b_n) for the first GEMM1.
 __global__ void k_cheb_start(const double *__restrict__ v, int ldv, const double *__restrict__ U,
@@ -1452,8 +1467,6 @@ void extern_mixed_tune(ngw_session *s, int *tune) {
   tune[5] = op->dense_ok ? 1 : 0;
 }
 
-int matvec_f64_dev_pub(ngw_session *s, int nb, double *hs, double *y, int tamm_d);
-
 // Build A1 = [C_isdf ; G^T] (G = (C U) / R^1/2, k rows) and
 // A3 = [(M C_isdf)^T | -U / (4 R^1/2)] in split-BF16 from the FP64 operator;
 // U = the first kdef Ritz vectors in s->eig_U (kdef = 0: no deflation).
@@ -1503,22 +1516,33 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
   }
   const double one = 1.0, zero = 0.0;
   if (kdef > 0) {
-    // G = (C U) / s  in FP64: C applied to the Ritz vectors with the FP64 matvec
-    PoolTmp ths(s), tcu(s);
-    NGW_CUDA(pool_alloc(s, &ths.p, (size_t)s->ncv * kdef * 8));
-    NGW_CUDA(pool_alloc(s, &tcu.p, (size_t)s->ncv * kdef * 8));
+    // G = (C U) / s  in FP64: C applied to the Ritz vectors as the matvec's
+    // three products (C_isdf hs, M t1, C_isdf^T t2) on the FP64 tensor-core
+    // GEMM, then the same combine (R^2 x + 4 R^1/2 z; TDA R x + 2 z)
+    const int ni = s->n_isdf, nc = s->ncv;
+    PoolTmp ths(s), tcu(s), tt1(s), tt2(s), tz(s), tws(s);
+    const size_t wsb = std::min(dgemm_ws_bytes(std::max(ni, nc), kdef, 0), (size_t)64 << 20);
+    NGW_CUDA(pool_alloc(s, &ths.p, (size_t)nc * kdef * 8));
+    NGW_CUDA(pool_alloc(s, &tcu.p, (size_t)nc * kdef * 8));
+    NGW_CUDA(pool_alloc(s, &tt1.p, (size_t)ni * kdef * 8));
+    NGW_CUDA(pool_alloc(s, &tt2.p, (size_t)ni * kdef * 8));
+    NGW_CUDA(pool_alloc(s, &tz.p, (size_t)nc * kdef * 8));
+    NGW_CUDA(pool_alloc(s, &tws.p, wsb));
     double *hs = static_cast<double *>(ths.p), *CU = static_cast<double *>(tcu.p);
-    launch_scale_rows(s->d_sqrtR, s->eig_U, s->ncv, hs, s->ncv, s->ncv, kdef, tda, st);
-    int rc = matvec_f64_dev_pub(s, kdef, hs, CU, tda);
-    if (rc == NGW_OK) {
-      int bx = std::min(64, (s->ncv + 255) / 256);
-      // TDA: the pair scaling is 1 (A x uses x, not R^1/2 x)
-      k_split_cols_to_rows<<<dim3(bx, kdef), 256, 0, st>>>(CU, s->ncv, kdef, tda ? nullptr : s->d_sqrtR,
-                                                          1.0, op->A1_hi, op->A1_lo, op->cv_pad,
-                                                          s->n_isdf);
-    }
-    NGW_TRY(rc);
+    double *t1 = static_cast<double *>(tt1.p), *t2 = static_cast<double *>(tt2.p);
+    double *z = static_cast<double *>(tz.p), *ws = static_cast<double *>(tws.p);
+    launch_scale_rows(s->d_sqrtR, s->eig_U, nc, hs, nc, nc, kdef, tda, st);
+    NGW_CUDA(dgemm(st, false, false, ni, kdef, nc, one, s->d_C, ni, hs, nc, zero, t1, ni, ws, wsb));
+    NGW_CUDA(dgemm(st, false, false, ni, kdef, ni, one, s->d_M, ni, t1, ni, zero, t2, ni, ws, wsb));
+    NGW_CUDA(dgemm(st, true, false, nc, kdef, ni, one, s->d_C, ni, t2, ni, zero, z, nc, ws, wsb));
+    launch_matvec_combine(s->d_sqrtR, hs, z, CU, nullptr, nc, kdef, tda, 0, 0.0, 0.0, nullptr, st);
+    int bx = std::min(64, (nc + 255) / 256);
+    // TDA: the pair scaling is 1 (A x uses x, not R^1/2 x)
+    k_split_cols_to_rows<<<dim3(bx, kdef), 256, 0, st>>>(CU, nc, kdef, tda ? nullptr : s->d_sqrtR, 1.0,
+                                                        op->A1_hi, op->A1_lo, op->cv_pad, ni);
     NGW_CUDA(cudaGetLastError());
+    // the temporaries go back to the pool in stream order (PoolTmp), after
+    // the kernels above on the session stream
   }
   // D = M * C (FP64 tensor-core GEMM), then split into A3[cv][mu] with the -U/(4s) columns
   PoolTmp td(s);
@@ -1544,12 +1568,15 @@ int mixed_build_operator(ngw_session *s, int kdef, int tda) {
 int mixed_set_deflation_values(ngw_session *s, const double *pvals) {
   MixedOperator *op = s->mixed;
   if (!op || op->kdef == 0) return NGW_OK;
-  NGW_CUDA(cudaMemcpyAsync(op->Up, s->eig_U, (size_t)s->ncv * op->kdef * 8, cudaMemcpyDeviceToDevice,
-                           s->stream));
-  for (int j = 0; j < op->kdef; ++j) {
-    const double pv = pvals[j];
-    NGW_CUBLAS(cublasDscal(s->cublas, s->ncv, &pv, op->Up + (size_t)j * s->ncv, 1));
+  if (op->kdef > kMaxDeflation) {
+    set_error("deflation: more eigenpairs than the column scaling holds");
+    return NGW_ERR_ARG;
   }
+  DeflationValues pv;
+  for (int j = 0; j < op->kdef; ++j) pv.v[j] = pvals[j];
+  const int bx = std::min(64, (s->ncv + 255) / 256);
+  k_scale_cols<<<dim3(bx, op->kdef), 256, 0, s->stream>>>(s->eig_U, s->ncv, pv, op->Up);
+  NGW_CUDA(cudaGetLastError());
   return NGW_OK;
 }
 
