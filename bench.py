@@ -37,8 +37,10 @@ WORKLOAD = dict(name="12-atom molecule, 30 occ + 90 empty, 600 ISDF points, 150 
                 deltae=4.0, ecuts=0.02, npoly=12, seed=11)
 METRIC = "Sigma_c solves/s"
 # DRAM bytes (read + write) of one in-situ dense p(C) GEMM of the 12-atom
-# workload from an ncu capture, by tile choice "bn,variant"
-MEASURED_TRAFFIC_DENSE = {}
+# workload from an ncu capture, by tile choice "bn,variant[,split]" (the
+# NGW_DENSE_TILES form): 300 launches of two requests of 150 Lanczos steps,
+# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum, mean per launch
+MEASURED_TRAFFIC_DENSE = {"128,3": 39.99e6}
 # DRAM bytes (read + write) of one in-situ GEMM1 + GEMM2 pair of the 12-atom
 # workload from an ncu capture, by tile choice "bn1,var1,split1,bn2,var2"
 # (GEMM1 [+ split-K reduce] + GEMM2, current kernels; ncu --metrics
@@ -835,6 +837,9 @@ def main():
     dense = sess.profile_dense_gemm(nb, reps=50) if args.precision == "mixed" else None
     if dense is not None:
         us_d, (Md, Nd, Kd, BNd, vd) = dense
+        # the library reports the variant and split-K as 16 x variant + split
+        var_d, split_d = vd // 16, vd % 16
+        tiles_d = f"{BNd},{var_d}" + (f",{split_d}" if var_d == 5 else "")
         flops = 2.0 * Md * Nd * Kd
         achieved = flops / (us_d * 1e-6) / 1e12
         hbm, bf16, bf16s, src = load_peaks()
@@ -842,12 +847,14 @@ def main():
         # split chain vectors (4 B), the FP64 output (8 B)
         alg_bytes = 4.0 * Md * Kd + 4.0 * Nd * Kd + 8.0 * Md * Nd
         roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                "frac": achieved / bf16, "traffic": MEASURED_TRAFFIC_DENSE.get(f"{BNd},{vd}"),
-                "traffic_note": "ncu dram__bytes_read+write of one dense GEMM in situ (--ncu-case); null "
-                                "when the tuned tiles differ from the profiled ones",
+                "frac": achieved / bf16, "traffic": MEASURED_TRAFFIC_DENSE.get(tiles_d),
+                "traffic_note": "ncu dram__bytes_read+write per launch of the dense GEMM in situ, from a "
+                                "separate capture (bench.py --ncu-case --ncu-niter 150 with the tiles pinned "
+                                "by NGW_DENSE_TILES); null when the tuned tiles differ from the profiled ones",
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "kernel": "k_tc_gemm (dense p(C) GEMM: H v, one per Lanczos step)",
-                "form": "dense", "us_per_launch": us_d, "shape": [Md, Nd, Kd, BNd, vd],
+                "form": "dense", "us_per_launch": us_d, "shape": [Md, Nd, Kd, BNd, var_d, split_d],
+                "tiles_env": tiles_d,
                 "peak_source": f"{src} (bf16 dense, burst)", "executed_bf16_frac": 3.0 * achieved / bf16}
     elif args.precision == "mixed":
         us1, us2 = sess.profile_mixed_gemms(nb, reps=50)
@@ -974,18 +981,24 @@ def main():
     # the Sigma_c spectra / reduction
     per_mv = 2
     per_step = 2
+    per_request = 10
     if args.precision == "mixed" and roof is not None and roof["form"] == "dense":
-        # dense form: per Lanczos step U^T v (FP64 GEMM + its K-slice sum), the
-        # split of the chain vectors, the dense GEMM and the Lanczos update
+        # dense form (ncu launch list of the request): per Lanczos step U^T v
+        # (k_dense_xo), the split of the chain vectors, the dense GEMM and the
+        # Lanczos update (the first step's update is k_lanczos_first); per
+        # request the start vectors (pair gather, two FP64 GEMMs, K-slice sum,
+        # norms, square root, init), the prescale, the Sigma_c spectra and
+        # reduction, the deflation scaling and the QP Newton solve
         per_mv = 0
-        per_step = 5
+        per_step = 4
+        per_request = 12
     elif args.precision == "mixed" and roof is not None:
         g1 = roof["shapes"][0]
         per_mv += 1 if (g1[4] > 1 and g1[5] not in (5, 6)) else 0
         per_step += 2
     elif args.precision != "mixed":
         per_mv = 2        # FP64 (library DGEMMs not counted): combine kernel + (next matvec's) scaling
-    launches_per_step = wl["niter"] * (wl["npoly"] * per_mv + per_step) + 10
+    launches_per_step = wl["niter"] * (wl["npoly"] * per_mv + per_step) + per_request
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": K,
                 "warmup": W, "ms_per_step": tot_ms / K, "higher_is_better": True, "scaling": "weak",
