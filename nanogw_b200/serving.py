@@ -73,13 +73,47 @@ class SigmaRequest:
         n = self.psi_intp.shape[0]
         return float(len(self.qp_bands)) * self.nmem * self.niter * n * (2.0 * self.ncv + n)
 
-    def footprint_bytes(self):
+    def footprint_bytes(self, mixed=True):
         """Device memory the request needs: operator (FP64 + split-BF16 +
-        pair products) and Lanczos / Clenshaw state of all its chains."""
+        pair products), Lanczos / Clenshaw state of all its chains and, in
+        mixed precision where the library may take the dense p(C) form, that
+        form's memory."""
         n, ncv, nb = self.psi_intp.shape[0], self.ncv, len(self.qp_bands) * self.nmem
         op = 8 * (n * self.nmem + n * n + n * ncv) + 2 * 2 * 2 * (n + 64) * (ncv + 128)
         chains = nb * ncv * (8 * 6 + 4 * 3 + 2 * 2) + nb * self.niter * 16 + nb * (self.nen + 1) * 16
-        return int(op + chains + (96 << 20))
+        dense = self.dense_bytes() if mixed else 0
+        return int(op + chains + dense + (96 << 20))
+
+    def dense_bytes(self):
+        """Peak device memory of the dense p(C) form when the library may
+        choose it for this request (mixed precision), else 0.
+
+        The library (``want_dense`` in csrc/abi.cu) takes the dense form for
+        N_cv <= 16384 when forming H = p(C) once plus one N_cv x N_cv product
+        per Lanczos step costs less than the factored form's 2p GEMMs per
+        step.  Here the test runs with the formation already paid and the
+        most deflated pairs the plan asks for (64), the case that favours
+        the dense form most, so the estimate stays an upper bound.  Memory:
+        H in split BF16 (kept in the session, 4 B per padded element) and
+        the FP64 formation's temporaries, freed after it (the Casida matrix,
+        the Paterson-Stockmeyer powers T_0 .. T_m, two Horner accumulators,
+        M C_isdf and the rank-k deflation products)."""
+        n, ncv, nb = self.psi_intp.shape[0], self.ncv, len(self.qp_bands) * self.nmem
+        p = len(self.polynomial) - 1
+        if ncv > 16384 or p < 2:
+            return 0
+        kdef = 64
+        dense_step = 3.0 * 2.0 * ncv * ncv * nb / 0.9e15 + 10e-6
+        fact_step = p * (3.0 * 4.0 * (n + kdef) * ncv * nb / 0.6e15 + 10e-6)
+        if dense_step >= fact_step:
+            return 0
+        m = max(2, int(np.ceil(np.sqrt(p + 1.0))))
+        powers = m + 1
+        cv_pad = -(-ncv // 128) * 128
+        kpad = -(-ncv // 64) * 64
+        resident = 2 * 2 * cv_pad * kpad
+        formation = 8 * ncv * ncv * (1 + powers + 2) + 8 * n * ncv + 8 * (2 * ncv * kdef + kdef * kdef)
+        return int(resident + formation)
 
 
 class SigmaServer:
@@ -183,6 +217,7 @@ class SigmaServer:
         if policy not in ("fifo", "largest"):
             raise ValueError("policy must be 'fifo' or 'largest'")
         reqs = sorted(requests, key=lambda r: r.arrival)
+        mixed = self.precision == "mixed"     # the dense p(C) form's memory counts in mixed precision
         lock = threading.Condition()
         free = list(range(self.nworkers))
         inflight = {}
@@ -235,7 +270,7 @@ class SigmaServer:
                 admitted = False
                 while pending and free:
                     _, _, req = pending[0]
-                    need = req.footprint_bytes()
+                    need = req.footprint_bytes(mixed)
                     if need > self.budget:
                         heapq.heappop(pending)
                         req.error = NGWError(NGW_ERR_BUDGET, f"request {req.rid} needs {need} bytes, more "
@@ -263,11 +298,12 @@ class SigmaServer:
                         while pending and free and len(group_r) < self.group_max:
                             item = heapq.heappop(pending)
                             r2 = item[2]
-                            if r2.work() > self.group_work or r2.footprint_bytes() > self.budget:
+                            need2 = r2.footprint_bytes(mixed)
+                            if r2.work() > self.group_work or need2 > self.budget:
                                 aside.append(item)
                                 continue
                             w2 = next((x for x in free if self.resident[x] == r2.mol_id), free[0])
-                            reserved[w2] = r2.footprint_bytes()
+                            reserved[w2] = need2
                             if used() > self.budget:
                                 reserved[w2] = 0
                                 aside.append(item)

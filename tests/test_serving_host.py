@@ -137,3 +137,44 @@ def test_small_requests_grouped():
     assert len({w for _, w in seen}) == 4          # every request on its own worker
     grouped = [r for r in reqs if r.rid in (0, 1, 3)]
     assert len({round(r.start, 3) for r in grouped}) == 1   # admitted together
+
+
+def _req_sized(nval, nmem, n, nqp, npoly=12):
+    return SigmaRequest(rid=0, mol_id=0, psi_intp=np.zeros((n, nmem)), mmtrx=np.zeros((n, n)),
+                        e1=np.arange(nmem, dtype=float), nval=nval,
+                        qp_bands=np.arange(nval - nqp // 2, nval - nqp // 2 + nqp) + 1,
+                        polynomial=np.ones(npoly + 1), niter=150, nen=400)
+
+
+def test_dense_form_memory_counts_in_mixed_footprint():
+    # 12-atom class (N_cv = 2700, 600 ISDF points, 720 chains): the library
+    # forms H = p(C) here, so the mixed footprint holds H in split BF16 and
+    # the FP64 formation's eight N_cv^2 matrices
+    small = _req_sized(30, 120, 600, 6)
+    dense = small.dense_bytes()
+    n2 = small.ncv ** 2
+    assert dense >= 4 * n2 + 8 * 8 * n2
+    assert small.footprint_bytes(mixed=True) - small.footprint_bytes(mixed=False) == dense
+    # above N_cv = 16384 the library never takes the dense form
+    big = _req_sized(80, 400, 640, 4)
+    assert big.ncv > 16384 and big.dense_bytes() == 0
+    # a degree-1 polynomial (TDA-like) has no dense form either
+    assert _req_sized(30, 120, 600, 6, npoly=1).dense_bytes() == 0
+
+
+def test_fp64_server_admits_without_dense_memory():
+    req = _req_sized(30, 120, 600, 6)
+    budget_gb = (req.footprint_bytes(mixed=False) + (1 << 20)) / (1 << 30)
+    assert req.footprint_bytes(mixed=True) > budget_gb * (1 << 30)
+    ran = []
+
+    def solver(w, r):
+        ran.append(r.rid)
+        r.eqp = np.zeros(len(r.qp_bands))
+
+    st = SigmaServer(workers=1, precision="fp64", hbm_budget_gb=budget_gb, solver=solver).run([req],
+                                                                                                realtime=False)
+    assert ran == [0] and st["refused"] == 0
+    st = SigmaServer(workers=1, precision="mixed", hbm_budget_gb=budget_gb, solver=solver).run([req],
+                                                                                                 realtime=False)
+    assert st["refused"] == 1
