@@ -57,3 +57,17 @@ def test_two_rank_gather_matches_single(tmp_path):
     ref = np.stack([OS.sigma_c_state(S.psi_intp, S.M, S.e1, S.nval, int(m), 21, 2.0, 0.02, 6, S.poly)
                     for m in qp], axis=1)
     assert np.array_equal(full, ref)
+
+
+def test_two_rank_gather_with_an_empty_shard(tmp_path):
+    # one QP state on two ranks: rank 1 holds none and still takes part in
+    # the gather with an empty table
+    from oracle import sigma as OS
+    from tests._system import make_small_system
+    S = make_small_system()
+    qp = np.array([S.nval], dtype=np.int32)
+    out = str(tmp_path / "full.npy")
+    mp.start_processes(_worker, args=(2, _free_port(), qp, out), nprocs=2, join=True, start_method="spawn")
+    full = np.load(out)
+    ref = OS.sigma_c_state(S.psi_intp, S.M, S.e1, S.nval, int(qp[0]), 21, 2.0, 0.02, 6, S.poly)[:, None]
+    assert full.shape == (21, 1) and np.array_equal(full, ref)
